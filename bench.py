@@ -1,0 +1,299 @@
+"""Benchmark of the B200 DUGKS step (dugksFoam fvDVM::evolution).
+
+Default workload: flow past a sphere on a cubed-sphere mesh (6 x 24 x 24 x
+32 cells = 110,592, radial stretch 1.12, r in [1, 10]), 16^3 Gauss-Hermite
+DVs (4,096), far field at Ma 0.5, Kn 0.1 on the diameter, isothermal diffuse
+wall; FP64.  Synthetic mesh and initial state (uniform free stream).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Multi-GPU: replicas only (every rank advances
+its own copy of the workload; the step has no cross-rank exchange), so
+value = all ranks' cell-DV updates / the slowest rank's time, weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "psp-vst_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "cell·DV updates/s: FP32-comp vs FP64 at ≤1e-6 macro rel-L2; % HBM peak; adjoint"
+UNIT = "cell·DV updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["ball", "cavity", "cube"], default="ball")
+    p.add_argument("--precision", choices=["fp64", "fp32c"], default="fp64")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp32c", action="store_true")
+    p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
+    return p.parse_args()
+
+
+def build_case(name):
+    from dugks_b200 import case as cs
+    if name == "ball":
+        c = cs.ball_case(24, 32, 1.12, 16, kn=0.1, mach=0.5)
+        cfg = {"workload": "ball: cubed sphere 6x24x24x32 (110592 cells), stretch 1.12, r 1..10, 16^3 GH DVs, "
+                           "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall",
+               "cells": c.n_cells, "n_dv": c.n_dv}
+    elif name == "cube":
+        c = cs.cube_case(64, 20, kn=0.1)
+        cfg = {"workload": "cube: 64^3 lid-driven cube, 20^3 GH DVs, Kn 0.1, lid 50 m/s", "cells": c.n_cells,
+               "n_dv": c.n_dv}
+    else:
+        c = cs.cavity_case(61, 28)
+        cfg = {"workload": "cavity: 61x61 lid-driven cavity, 28^2 GH DVs, Kn 0.075, lid 50 m/s", "cells": c.n_cells,
+               "n_dv": c.n_dv}
+    cfg["dt"] = c.dt
+    cfg["cfl"] = 0.5
+    return c, cfg
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_uuid(dev: int):
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+def cpu_baseline(case_name: str, n1d: int, steps: int, warmup: int):
+    """The CPU restatement of the step (the reference itself cannot be built
+    here: it needs OpenFOAM, MPI and legacy TBB) on all host cores, on a
+    bounded sample of the workload: the same mesh with an n1d^D DV set."""
+    import oracle_bind as ob
+    from dugks_b200 import case as cs
+    from dugks_b200 import quadrature
+    c, _ = build_case(case_name)
+    C = math.sqrt(2.0 * c.gas["R"] * c.gas["Tref"])
+    xis, w = quadrature.gauss_hermite_half_range(C, n1d)
+    xi, ww = quadrature.tensor_product(xis, w, c.D)
+    cores = os.cpu_count() or 1
+    o = ob.Oracle(c, threads=cores, xi=xi, w=ww)
+    for _ in range(warmup):
+        o.evolution(c.dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.evolution(c.dt)
+    t = time.perf_counter() - t0
+    n = c.n_cells * len(ww) * steps
+    o.close()
+    return {"value": n / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"same mesh ({c.n_cells} cells) with a {n1d}^{c.D} = {len(ww)}-DV Gauss-Hermite set, "
+                      f"{steps} steps after {warmup} warm-up, OpenMP over DVs/faces/cells ({cores} threads)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, cfg = build_case(args.workload)
+    steps = max(1, min(args.steps, 5))
+    warm = 1
+    cb = cpu_baseline(args.workload, args.cpu_sample_ndv, steps, warm)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from dugks_b200 import lib as dl
+    case, cfg = build_case(args.workload)
+    prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
+    solver = dl.Solver(case, precision=prec, device=local)
+    nv, nc = solver.n_dv, case.n_cells
+    K, W = args.steps, max(3, args.warmup)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    solver.step(W, case.dt)
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_uuid(local)) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    l0 = solver.kernel_launches()
+    stage = solver.step_timed(K, case.dt)            # CUDA events on the library's stream
+    launches = solver.kernel_launches() - l0
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    t_ms = max_over_ranks(float(stage[4]))
+    value = world * nc * nv * K / (t_ms / 1e3)
+
+    # end to end through the public API with host buffers: each step is
+    # fvDVM::evolution (dt passed by value) followed by the copy of the
+    # cell macros rho, U, T, q (and tau) back into host fields
+    barrier()
+    te0 = time.perf_counter()
+    for _ in range(K):
+        solver.step(1, case.dt)
+        solver.macros()
+    te = max_over_ranks(time.perf_counter() - te0)
+    e2e = world * nc * nv * K / te
+
+    rs = 8 if prec == dl.FP64 else 4
+    peak, peak_kind = measured_peaks()
+    a_ms, b_ms = stage[0] / K, stage[2] / K
+    if b_ms >= a_ms:
+        kname, kbytes, kms = "pass B (face relaxation, flux, update, cell moments)", 4 * rs * nc * nv, b_ms
+    else:
+        kname, kbytes, kms = "pass A (reconstruction, face moments)", 2 * rs * nc * nv, a_ms
+    achieved = kbytes / (kms / 1e3) / 1e9
+    step_bytes = 6 * rs * nc * nv
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == dl.FP64 else "f32 storage / f64 moments", "data": "synthetic",
+        "config": dict(cfg, precision=args.precision, parallelism=f"replicas x{world}",
+                       l2="inputs larger than L2 (state %.2f GB)" % (4 * rs * nc * nv / 1e9)),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 72 * nc + 16},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": kbytes},
+        "step_roofline": {"bytes_per_update": 6 * rs, "achieved": step_bytes / (t_ms / K / 1e3) / 1e9,
+                          "frac": step_bytes / (t_ms / K / 1e3) / 1e9 / peak},
+        "stage_ms_per_step": {"pass_a": a_ms, "face_combine": stage[1] / K, "pass_b": b_ms,
+                              "cell_combine": stage[3] / K},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_fp32c and prec == dl.FP64:
+        # the FP32-compensated path on the same workload, and its macros'
+        # rel-L2 against this FP64 run after the same steps
+        import numpy as np
+        ref = solver.macros()
+        steps_done = W + 2 * K
+        del solver
+        s32 = dl.Solver(case, precision=dl.FP32C, device=local)
+        s32.step(W, case.dt)
+        st32 = s32.step_timed(K, case.dt)
+        s32.step(steps_done - W - K, case.dt)
+        m32 = s32.macros()
+        rel = {k: float(np.linalg.norm(m32[k] - ref[k]) / np.linalg.norm(ref[k])) for k in ("rho", "U", "T", "q")}
+        v32 = nc * nv * K / (st32[4] / 1e3)
+        line["fp32c"] = {"value": v32, "ms_per_step": st32[4] / K, "speedup_vs_fp64": v32 / value,
+                         "rel_l2_vs_fp64_after_%d_steps" % steps_done: rel,
+                         "step_roofline_frac": 3 * 4 * 2 * nc * nv / (st32[4] / K / 1e3) / 1e9 / peak}
+        del s32
+    else:
+        del solver
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_sample_ndv, 2, 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * dugks_b200 -- C ABI of the B200-native DUGKS step.
+ *
+ * This ABI replaces the step of dugksFoam's Foam::fvDVM class
+ * (src/fvDVM/fvDVM/fvDVM.H:80-409).  A thin fvDVM shim keeps that class's
+ * public interface and calls into this library:
+ *
+ *   fvDVM::fvDVM(rho, U, T, argc, argv, args)   fvDVM.C:1901-2117
+ *       -> dugks_create + dugks_set_macros
+ *   fvDVM::evolution()                          fvDVM.C:2128-2174
+ *       -> dugks_step, then dugks_get_macros into the app's rho/U/T fields
+ *   fvDVM::getCoNum(maxCo, meanCo)              fvDVM.C:2177-2185
+ *       -> dugks_co_num
+ *   fvDVM::writeDFonCells()                     fvDVM.C:1835-1897
+ *       -> dugks_get_df
+ *   qVol()/qSurf() accessors (fvDVM.H:330-396)  -> dugks_get_macros,
+ *                                                  dugks_get_face_macros
+ *
+ * Conventions.  Plain pointers and sizes only.  Host buffers are owned by
+ * the caller and copied; the distribution functions live in device memory
+ * owned by the handle.  Every function returns a dugks_status; no function
+ * aborts the process.  dugks_last_error() returns the text of the last
+ * error on a handle.  One handle is used by one host thread at a time.
+ *
+ * Mesh convention: OpenFOAM fvMesh addressing.  Faces are the internal
+ * faces (owner < neighbour, any order) followed by the boundary faces of the
+ * non-empty patches, grouped by patch (empty patches have no fv faces).
+ * Vectors are stored xyz-interleaved.  Cell and face geometry is what
+ * fvMesh provides (C, V, Cf, Sf); dugks_mesh_geometry computes it from a
+ * polyMesh when OpenFOAM is not present.
+ */
+#ifndef DUGKS_B200_H
+#define DUGKS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DUGKS_ABI_VERSION 1
+
+typedef enum dugks_status {
+    DUGKS_OK = 0,
+    DUGKS_ERR_ARG = 1,       /* invalid argument (null pointer, bad size, bad mesh) */
+    DUGKS_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    DUGKS_ERR_OOM = 3,       /* device or host allocation failed */
+    DUGKS_ERR_TIMEOUT = 4,   /* a bounded device wait ran out */
+    DUGKS_ERR_NAN = 5,       /* non-finite macroscopic state detected */
+    DUGKS_ERR_STATE = 6,     /* call out of order (e.g. step before set_macros) */
+    DUGKS_ERR_UNSUPPORTED = 7
+} dugks_status;
+
+/* Boundary patch types.  The reference selects the g/h surface patch type
+ * from the rho patch type (discreteVelocity::setBCtype,
+ * src/fvDVM/discreteVelocity/discreteVelocity.C:188-195):
+ *   rho calculatedMaxwell -> maxwellWall  (diffuse Maxwell wall)
+ *   rho farField          -> farField     (equilibrium inflow, upwind outflow) */
+typedef enum dugks_patch_type {
+    DUGKS_PATCH_MAXWELL_WALL = 1,
+    DUGKS_PATCH_FAR_FIELD = 2
+} dugks_patch_type;
+
+typedef enum dugks_precision {
+    DUGKS_FP64 = 0,   /* FP64 storage and arithmetic, the plain path */
+    DUGKS_FP32C = 1   /* FP32 g/h storage and flux arithmetic; FP64 moment accumulation,
+                         conserved update, heat-flux term and quadrature weights */
+} dugks_precision;
+
+/* Least-squares weighting (the stock leastSquares scheme as written in
+ * src/fvDVM/zeroBoundaryGrad/zeroBoundaryVectors.C:110-123 is the default;
+ * the two variants are invDistLeastSquaresVectors.C:109-167 and
+ * unweightedLeastSquaresVectors.C:108-162 of the same directory). */
+typedef enum dugks_ls_weighting {
+    DUGKS_LS_MAGSF = 0,
+    DUGKS_LS_INVDIST = 1,
+    DUGKS_LS_UNWEIGHTED = 2
+} dugks_ls_weighting;
+
+typedef struct dugks_mesh {
+    int32_t n_cells;
+    int32_t n_internal_faces;
+    int32_t n_boundary_faces;       /* faces of non-empty patches */
+    int32_t n_solution_dims;        /* fvMesh::nSolutionD(): 2 (z empty) or 3 */
+    const int64_t* owner;           /* [n_internal_faces + n_boundary_faces] */
+    const int64_t* neighbour;       /* [n_internal_faces] */
+    const double* cell_centres;     /* [n_cells*3]  fvMesh::C() */
+    const double* cell_volumes;     /* [n_cells]    fvMesh::V() */
+    const double* face_centres;     /* [n_faces*3]  fvMesh::Cf() */
+    const double* face_areas;       /* [n_faces*3]  fvMesh::Sf() */
+    int32_t n_patches;              /* non-empty patches */
+    const int32_t* patch_start;     /* [n_patches+1] offsets into the boundary faces */
+} dugks_mesh;
+
+/* constant/Xis, constant/weights and DVMProperties fvDVMparas
+ * (fvDVM.C:62-123, :1928-1933); the D-dimensional tensor product is built
+ * as fvDVM::initialiseDV does (fvDVM.C:293-374). */
+typedef struct dugks_dv_set {
+    int32_t n_per_dim;              /* nDV */
+    const double* xis;              /* [n_per_dim] */
+    const double* weights;          /* [n_per_dim] */
+    double xi_max;                  /* xiMax, used by the Courant number only */
+} dugks_dv_set;
+
+/* DVMProperties gasProperties (fvDVM.C:1943-1948) */
+typedef struct dugks_gas {
+    double R;
+    double omega;
+    double Tref;
+    double mu_ref;
+    double Pr;
+    int32_t K_inner;
+} dugks_gas;
+
+/* Boundary conditions of the non-empty patches.  Per boundary face values
+ * are the patch values of the app's rho, U and T fields.  For maxwellWall
+ * faces rho is ignored (computed each step from the outgoing flux,
+ * calculatedMaxwellFvPatchField.C:140-164); for farField faces rho and T
+ * stay at these values (farFieldFvPatchField.H assignment operators are
+ * no-ops) and U is not used (the owner-cell velocity is, fvDVM.C:929-934). */
+typedef struct dugks_bc {
+    const int32_t* patch_type;      /* [n_patches] dugks_patch_type */
+    const double* rho;              /* [n_boundary_faces] */
+    const double* U;                /* [n_boundary_faces*3] */
+    const double* T;                /* [n_boundary_faces] */
+} dugks_bc;
+
+typedef struct dugks_options {
+    int32_t precision;              /* dugks_precision */
+    int32_t ls_weighting;           /* dugks_ls_weighting */
+    int32_t device;                 /* CUDA device ordinal */
+    int32_t tile_cells;             /* cells per tile; 0 = automatic */
+    int32_t dv_chunks;              /* DV chunks per tile; 0 = automatic */
+    int32_t reserved[11];
+} dugks_options;
+
+typedef struct dugks_handle dugks_handle;
+
+int dugks_abi_version(void);
+
+/* Default options (FP64, magSf-weighted least squares, device 0, automatic tiling). */
+void dugks_default_options(dugks_options* opt);
+
+/* Host-only: OpenFOAM primitiveMesh geometry from a polyMesh (all faces,
+ * empty patches included).  Face centres/area vectors by the triangle fan
+ * about the point average; cell centres/volumes by face pyramids about the
+ * average of the face centres. */
+int dugks_mesh_geometry(int32_t n_points, const double* points, int32_t n_faces,
+                        const int64_t* face_offsets, const int64_t* face_points,
+                        const int64_t* owner, int32_t n_internal, const int64_t* neighbour,
+                        int32_t n_cells, double* face_centres, double* face_areas,
+                        double* cell_centres, double* cell_volumes);
+
+/* fvDVM::fvDVM, first half: mesh, DV set, gas, boundary conditions; builds
+ * the least-squares vectors and the device layout.  fvDVM.C:1901-2110 */
+int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas,
+                 const dugks_bc* bc, const dugks_options* opt, dugks_handle** out);
+
+/* fvDVM::fvDVM, second half: g~ = Maxwellian(rho,U,T), h~ = (K+3-D)RT g~,
+ * wall inComingByRho, tau, q = 0, linear face velocity.
+ * fvDVM.C:414-426, :578-624, :2115-2116.  U is [n_cells*3]. */
+int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const double* T);
+
+/* n_steps calls of fvDVM::evolution() (fvDVM.C:2128-2174) with time steps
+ * dt[0..n_steps-1]. */
+int dugks_step(dugks_handle* h, int32_t n_steps, const double* dt);
+
+/* fvDVM::getCoNum (fvDVM.C:2177-2185) for time step dt, from the current
+ * face velocities. */
+int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean);
+
+/* Cell macros rho [n], U [n*3], T [n], q [n*3]; any pointer may be NULL. */
+int dugks_get_macros(dugks_handle* h, double* rho, double* U, double* T, double* q);
+
+/* Face macros of the last step (internal faces then boundary faces):
+ * rhoSurf, Usurf, Tsurf, qSurf (fvDVM.C:1181-1300); any pointer may be NULL. */
+int dugks_get_face_macros(dugks_handle* h, double* rho, double* U, double* T, double* q);
+
+/* Boundary rho patch values: wall density of the last step on maxwellWall
+ * faces, the fixed value on farField faces. [n_boundary_faces] */
+int dugks_get_boundary_rho(dugks_handle* h, double* rho_b);
+
+/* g~ (and h~) at the given cells for all DVs, [n][n_dv] row per cell
+ * (fvDVM::writeDFonCell, fvDVM.C:1835-1890). h_out may be NULL. */
+int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out, double* h_out);
+
+/* Whole state g~, h~ as DV-major [n_dv][n_cells] doubles, for exact
+ * restart (the reference writes only macros and re-initialises the DFs to
+ * the Maxwellian on restart, fvDVM.C:414-426).  dugks_set_state (after
+ * dugks_set_macros) recomputes the cell macros from the given DFs as
+ * fvDVM::updateMacroVol does (fvDVM.C:1528-1554, :1682-1742); dt_prev is
+ * the time step that produced them (it enters the heat-flux correction). */
+int dugks_get_state(dugks_handle* h, double* g, double* hh);
+int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double dt_prev);
+
+/* Number of discrete velocities (nDV^D). */
+int32_t dugks_n_dv(const dugks_handle* h);
+
+/* Wall-clock of the kernels of the last dugks_step call, in milliseconds,
+ * measured with CUDA events on the handle's stream. */
+int dugks_last_step_ms(dugks_handle* h, double* ms);
+
+/* dugks_step with CUDA events around every kernel stage on the handle's
+ * stream; stage_ms[0..4] receive the summed milliseconds of pass A (face
+ * reconstruction and moments), the face combine, pass B (relaxation, flux,
+ * update, cell moments), the cell combine, and the whole call. */
+int dugks_step_timed(dugks_handle* h, int32_t n_steps, const double* dt, double* stage_ms);
+
+/* Number of kernels this handle has launched so far. */
+int64_t dugks_kernel_launches(const dugks_handle* h);
+
+const char* dugks_last_error(const dugks_handle* h);
+void dugks_destroy(dugks_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,636 @@
+// C ABI of the B200 DUGKS step (declarations and reference mapping in
+// include/dugks.h).  Owns the device layout and drives the kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "dugks_internal.h"
+#include "dugks_kernels.cuh"
+
+using dugks::set_error;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+#define CUDA_TRY(h, call)                                                                               \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return set_error((h), e_ == cudaErrorMemoryAllocation ? DUGKS_ERR_OOM : DUGKS_ERR_CUDA,     \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+    } while (0)
+
+template <typename T>
+int dev_alloc(dugks_handle* h, T** p, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+        return set_error(h, e == cudaErrorMemoryAllocation ? DUGKS_ERR_OOM : DUGKS_ERR_CUDA,
+                         "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    h->allocations.push_back(q);
+    *p = static_cast<T*>(q);
+    return DUGKS_OK;
+}
+
+template <typename T>
+int upload(dugks_handle* h, T** p, const std::vector<T>& v) {
+    int st = dev_alloc(h, p, v.size());
+    if (st) return st;
+    if (!v.empty()) CUDA_TRY(h, cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return DUGKS_OK;
+}
+
+double inv_norm_host(double RT, int D) {
+    const double t = 2.0 * kPi * RT;
+    return D == 3 ? 1.0 / (t * std::sqrt(t)) : (D == 2 ? 1.0 / t : 1.0 / std::sqrt(t));
+}
+
+size_t real_size(const dugks_handle* h) { return h->precision == DUGKS_FP64 ? sizeof(double) : sizeof(float); }
+
+dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
+    dugks::StepArgs a{};
+    a.dm = h->dm;
+    a.ds = h->ds;
+    a.dt = dt;
+    a.dt_next = dt_next;
+    a.chunks = h->chunks;
+    a.chunk_begin = h->d_chunk_begin;
+    a.ipt = (h->tiling.max_items + dugks::kThreads - 1) / dugks::kThreads;
+    a.dims_local = h->tiling.max_local;
+    a.dims_l0 = h->tiling.max_l0;
+    a.dims_items = h->tiling.max_items;
+    dugks::pass_smem(h->dm, a.dims_local, a.dims_l0, a.dims_items, h->precision, &a.smemA, &a.smemB);
+    return a;
+}
+
+int check_device_errors(dugks_handle* h) {
+    int err[4] = {0, 0, 0, 0};
+    CUDA_TRY(h, cudaMemcpyAsync(err, h->ds.err, sizeof err, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (err[0] & 1) return set_error(h, DUGKS_ERR_NAN, "non-finite or non-positive rho/T in the cell macros");
+    if (err[0] & 2) return set_error(h, DUGKS_ERR_TIMEOUT, "a bounded device wait ran out");
+    return DUGKS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dugks_abi_version(void) { return DUGKS_ABI_VERSION; }
+
+void dugks_default_options(dugks_options* opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof *opt);
+    opt->precision = DUGKS_FP64;
+    opt->ls_weighting = DUGKS_LS_MAGSF;
+}
+
+int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
+                 const dugks_options* opt_in, dugks_handle** out) {
+    if (!out) return DUGKS_ERR_ARG;
+    *out = nullptr;
+    if (!mesh || !dv || !gas || !bc) return DUGKS_ERR_ARG;
+    dugks_options opt;
+    dugks_default_options(&opt);
+    if (opt_in) opt = *opt_in;
+    dugks_handle* h = new (std::nothrow) dugks_handle();
+    if (!h) return DUGKS_ERR_OOM;
+    auto fail = [&](int code, const std::string& msg) {
+        // keep the handle so that the caller can read the message
+        set_error(h, code, msg);
+        *out = h;
+        return code;
+    };
+    if (mesh->n_cells <= 0 || mesh->n_internal_faces < 0 || mesh->n_boundary_faces < 0 || !mesh->owner ||
+        (mesh->n_internal_faces > 0 && !mesh->neighbour) || !mesh->cell_centres || !mesh->cell_volumes ||
+        !mesh->face_centres || !mesh->face_areas || mesh->n_patches < 0 ||
+        (mesh->n_patches > 0 && !mesh->patch_start))
+        return fail(DUGKS_ERR_ARG, "dugks_create: incomplete mesh");
+    if (mesh->n_solution_dims != 2 && mesh->n_solution_dims != 3)
+        return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: n_solution_dims must be 2 or 3");
+    if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
+    if (opt.precision != DUGKS_FP64 && opt.precision != DUGKS_FP32C)
+        return fail(DUGKS_ERR_ARG, "dugks_create: unknown precision");
+    if (!(gas->R > 0) || !(gas->Tref > 0) || !(gas->mu_ref > 0)) return fail(DUGKS_ERR_ARG, "dugks_create: bad gas");
+    h->precision = opt.precision;
+    h->device = opt.device;
+    h->D = mesh->n_solution_dims;
+    h->nC = mesh->n_cells;
+    h->nIF = mesh->n_internal_faces;
+    h->nBF = mesh->n_boundary_faces;
+    h->nP = mesh->n_patches;
+    h->gas = *gas;
+    h->xi_max = dv->xi_max;
+    const int nC = h->nC, nIF = h->nIF, nBF = h->nBF, nF = nIF + nBF;
+    h->owner.assign(mesh->owner, mesh->owner + nF);
+    h->neighbour.assign(mesh->neighbour, mesh->neighbour + nIF);
+    for (int f = 0; f < nF; ++f)
+        if (h->owner[f] < 0 || h->owner[f] >= nC) return fail(DUGKS_ERR_ARG, "dugks_create: owner out of range");
+    for (int f = 0; f < nIF; ++f)
+        if (h->neighbour[f] < 0 || h->neighbour[f] >= nC || h->neighbour[f] == h->owner[f])
+            return fail(DUGKS_ERR_ARG, "dugks_create: neighbour out of range");
+    h->C.assign(mesh->cell_centres, mesh->cell_centres + 3 * static_cast<size_t>(nC));
+    h->V.assign(mesh->cell_volumes, mesh->cell_volumes + nC);
+    for (int c = 0; c < nC; ++c)
+        if (!(h->V[c] > 0)) return fail(DUGKS_ERR_ARG, "dugks_create: non-positive cell volume");
+    h->Cf.assign(mesh->face_centres, mesh->face_centres + 3 * static_cast<size_t>(nF));
+    h->Sf.assign(mesh->face_areas, mesh->face_areas + 3 * static_cast<size_t>(nF));
+    h->patch_start.assign(mesh->patch_start, mesh->patch_start + h->nP + 1);
+    if (h->nP == 0) h->patch_start.assign(1, 0);
+    if (h->patch_start[0] != 0 || h->patch_start[h->nP] != nBF)
+        return fail(DUGKS_ERR_ARG, "dugks_create: patch_start must span the boundary faces");
+    h->patch_type.assign(bc->patch_type, bc->patch_type + h->nP);
+    h->bface_ptype.assign(nBF, 0);
+    h->bface_patch_local.assign(nBF, 0);
+    for (int p = 0; p < h->nP; ++p) {
+        if (h->patch_type[p] != DUGKS_PATCH_MAXWELL_WALL && h->patch_type[p] != DUGKS_PATCH_FAR_FIELD)
+            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: unsupported patch type");
+        if (h->patch_start[p + 1] < h->patch_start[p]) return fail(DUGKS_ERR_ARG, "dugks_create: bad patch_start");
+        for (int b = h->patch_start[p]; b < h->patch_start[p + 1]; ++b) {
+            h->bface_ptype[b] = h->patch_type[p];
+            h->bface_patch_local[b] = b - h->patch_start[p];
+        }
+    }
+    if (nBF > 0 && (!bc->rho || !bc->U || !bc->T)) return fail(DUGKS_ERR_ARG, "dugks_create: missing BC values");
+    h->bc_rho.assign(bc->rho, bc->rho + nBF);
+    h->bc_U.assign(bc->U, bc->U + 3 * static_cast<size_t>(nBF));
+    h->bc_T.assign(bc->T, bc->T + nBF);
+    // tensor-product DV set, x fastest (fvDVM.C:293-374)
+    const int n = dv->n_per_dim;
+    h->n1d = n;
+    if (h->D == 3) {
+        for (int iz = 0; iz < n; ++iz)
+            for (int iy = 0; iy < n; ++iy)
+                for (int ix = 0; ix < n; ++ix) {
+                    h->w.push_back(dv->weights[iz] * dv->weights[iy] * dv->weights[ix]);
+                    h->xi.insert(h->xi.end(), {dv->xis[ix], dv->xis[iy], dv->xis[iz]});
+                }
+    } else {
+        for (int iy = 0; iy < n; ++iy)
+            for (int ix = 0; ix < n; ++ix) {
+                h->w.push_back(dv->weights[iy] * dv->weights[ix] * 1);
+                h->xi.insert(h->xi.end(), {dv->xis[ix], dv->xis[iy], 0.0});
+            }
+    }
+    h->nv = static_cast<int>(h->w.size());
+    if (opt.ls_weighting < 0 || opt.ls_weighting > 2) return fail(DUGKS_ERR_ARG, "dugks_create: bad ls_weighting");
+    dugks::compute_weights_and_ls(h, opt.ls_weighting);
+    for (double x : h->lsP)
+        if (!std::isfinite(x)) return fail(DUGKS_ERR_ARG, "dugks_create: singular least-squares system");
+
+    // tiles: at most 4 items per thread
+    int tile = opt.tile_cells > 0 ? opt.tile_cells : (h->D == 3 ? 128 : 192);
+    tile = std::min(tile, dugks::kThreads);
+    for (;;) {
+        dugks::build_tiling(h, tile);
+        if (h->tiling.max_items <= 4 * dugks::kThreads || tile <= 8) break;
+        tile /= 2;
+    }
+    if (h->tiling.max_items > 4 * dugks::kThreads)
+        return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: cells with too many faces for the tile layout");
+    // DV chunks: enough CTAs to fill the GPU several times over
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= 0)
+        return fail(DUGKS_ERR_CUDA, "dugks_create: no CUDA device");
+    if (h->device < 0 || h->device >= dev_count) return fail(DUGKS_ERR_ARG, "dugks_create: bad device ordinal");
+    cudaError_t ce = cudaSetDevice(h->device);
+    if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    int chunks = opt.dv_chunks > 0 ? opt.dv_chunks : (4 * sms + h->tiling.n_tiles - 1) / h->tiling.n_tiles;
+    chunks = std::max(1, std::min(chunks, h->nv / 4 > 0 ? h->nv / 4 : 1));
+    h->chunks = chunks;
+    h->chunk_begin.resize(chunks + 1);
+    for (int c = 0; c <= chunks; ++c)
+        h->chunk_begin[c] = static_cast<int32_t>((static_cast<int64_t>(h->nv) * c) / chunks);
+
+    // ---- device layout ----
+    const dugks::Tiling& t = h->tiling;
+    dugks::DevMesh& dm = h->dm;
+    dm.D = h->D;
+    dm.K = gas->K_inner;
+    dm.R = gas->R;
+    dm.Pr = gas->Pr;
+    dm.omega = gas->omega;
+    dm.Tref = gas->Tref;
+    dm.muRef = gas->mu_ref;
+    dm.nC = nC;
+    dm.nIF = nIF;
+    dm.nBF = nBF;
+    dm.nv = h->nv;
+    dm.n_tiles = t.n_tiles;
+    dm.n_items = static_cast<int>(t.items.size());
+    dm.n_tbf = t.n_tbf;
+    dm.xi_max_co = std::sqrt(static_cast<double>(h->D)) * h->xi_max;
+    int st;
+    ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(ce));
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    double *d_xi, *d_w, *d_grad_ls, *d_dtV, *d_dc, *d_bS;
+    int32_t *d_tb, *d_tlo, *d_lc, *d_tio, *d_go, *d_gnb, *d_cfo, *d_cfi, *d_fi, *d_bpl, *d_bpt, *d_bown;
+    dugks::Item* d_items;
+    std::vector<double> dtV(nC);
+    for (int c = 0; c < nC; ++c) dtV[c] = 1.0 / h->V[t.perm[c]];
+    std::vector<double> bS(3 * static_cast<size_t>(nBF));
+    std::vector<int32_t> bown(nBF);
+    for (int b = 0; b < nBF; ++b) {
+        for (int k = 0; k < 3; ++k) bS[3 * b + k] = h->Sf[3 * (nIF + b) + k];
+        bown[b] = t.iperm[h->owner[nIF + b]];
+    }
+    if ((st = upload(h, &d_xi, h->xi)) || (st = upload(h, &d_w, h->w)) || (st = upload(h, &d_tb, t.tile_begin)) ||
+        (st = upload(h, &d_tlo, t.tile_loc_off)) || (st = upload(h, &d_lc, t.loc_cells)) ||
+        (st = upload(h, &d_tio, t.tile_item_off)) || (st = upload(h, &d_items, t.items)) ||
+        (st = upload(h, &d_go, t.grad_off)) || (st = upload(h, &d_gnb, t.grad_nb)) ||
+        (st = upload(h, &d_grad_ls, t.grad_ls)) || (st = upload(h, &d_cfo, t.cf_off)) ||
+        (st = upload(h, &d_cfi, t.cf_item)) || (st = upload(h, &d_dtV, dtV)) || (st = upload(h, &d_fi, t.face_items)) ||
+        (st = upload(h, &d_bpl, h->bface_patch_local)) || (st = upload(h, &d_bpt, h->bface_ptype)) ||
+        (st = upload(h, &d_bown, bown)) || (st = upload(h, &d_dc, h->dc)) || (st = upload(h, &d_bS, bS)) ||
+        (st = upload(h, &h->d_chunk_begin, h->chunk_begin))) {
+        *out = h;
+        return st;
+    }
+    dm.xi = d_xi;
+    dm.w = d_w;
+    dm.tile_begin = d_tb;
+    dm.tile_loc_off = d_tlo;
+    dm.loc_cells = d_lc;
+    dm.tile_item_off = d_tio;
+    dm.items = d_items;
+    dm.grad_off = d_go;
+    dm.grad_nb = d_gnb;
+    dm.grad_ls = d_grad_ls;
+    dm.cf_off = d_cfo;
+    dm.cf_item = d_cfi;
+    dm.dtV = d_dtV;
+    dm.face_items = d_fi;
+    dm.bface_patch_local = d_bpl;
+    dm.bface_ptype = d_bpt;
+    dm.bface_owner = d_bown;
+    dm.dc = d_dc;
+    dm.bS = d_bS;
+    dugks::DevState& ds = h->ds;
+    const size_t rs = real_size(h);
+    const size_t nvc = static_cast<size_t>(h->nv) * nC;
+    const size_t nxb = static_cast<size_t>(h->nv) * std::max(t.n_tbf, 1);
+    unsigned char* p;
+    for (int i = 0; i < 2; ++i) {
+        if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
+        ds.g[i] = p;
+        if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
+        ds.h[i] = p;
+        if ((st = dev_alloc(h, &p, nxb * rs))) return *out = h, st;
+        ds.xbg[i] = p;
+        if ((st = dev_alloc(h, &p, nxb * rs))) return *out = h, st;
+        ds.xbh[i] = p;
+    }
+    ds.cur = 0;
+    if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
+        (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
+        (st = dev_alloc(h, &ds.cellrec, nC)) || (st = dev_alloc(h, &ds.facerec, nF)) ||
+        (st = dev_alloc(h, &ds.brec, nBF)) || (st = dev_alloc(h, &ds.bmom_in, static_cast<size_t>(nBF) * dugks::kNM)) ||
+        (st = dev_alloc(h, &ds.cm, static_cast<size_t>(nC) * 9)) ||
+        (st = dev_alloc(h, &ds.fm, static_cast<size_t>(nF) * 9)) || (st = dev_alloc(h, &ds.co, 2)) ||
+        (st = dev_alloc(h, &ds.err, 4))) {
+        *out = h;
+        return st;
+    }
+    ce = cudaMemset(ds.err, 0, 4 * sizeof(int));
+    if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, cudaGetErrorString(ce));
+    ce = cudaMemset(ds.partF, 0, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM * sizeof(double));
+    if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, cudaGetErrorString(ce));
+    dugks::StepArgs a = make_args(h, 0.0, 0.0);
+    ce = dugks::configure_kernels(h->precision, h->D, a.ipt, a.smemA, a.smemB);
+    if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("configure kernels: ") + cudaGetErrorString(ce));
+    *out = h;
+    return DUGKS_OK;
+}
+
+int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const double* T) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!rho || !U || !T) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: null field");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    const int nC = h->nC, nIF = h->nIF, nBF = h->nBF, D = h->D;
+    const double R = h->gas.R;
+    const dugks::Tiling& t = h->tiling;
+    std::vector<double> cm(static_cast<size_t>(nC) * 9);
+    std::vector<dugks::CellRec> cr(nC);
+    for (int c = 0; c < nC; ++c) {
+        const int o = t.perm[c];
+        if (!(rho[o] > 0) || !(T[o] > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: rho and T must be > 0");
+        const double tau = h->gas.mu_ref * std::exp(h->gas.omega * std::log(T[o] / h->gas.Tref)) / rho[o] / T[o] / R;
+        double* m = &cm[9 * static_cast<size_t>(c)];
+        m[0] = rho[o];
+        m[1] = U[3 * o];
+        m[2] = U[3 * o + 1];
+        m[3] = U[3 * o + 2];
+        m[4] = T[o];
+        m[5] = m[6] = m[7] = 0.0;
+        m[8] = tau;
+        const double RT = R * T[o];
+        dugks::CellRec& r = cr[c];
+        r.U[0] = m[1];
+        r.U[1] = m[2];
+        r.U[2] = m[3];
+        r.invRT = 1.0 / RT;
+        r.A = rho[o] * inv_norm_host(RT, D);
+        r.r = 0.0;
+        r.qv[0] = r.qv[1] = r.qv[2] = 0.0;
+        r.RT = RT;
+    }
+    // boundary records
+    const double K3D = h->gas.K_inner + 3.0 - D;
+    std::vector<dugks::BRec> br(nBF);
+    for (int b = 0; b < nBF; ++b) {
+        const double RT = R * h->bc_T[b];
+        if (!(RT > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: boundary T must be > 0");
+        br[b].U[0] = h->bc_U[3 * b];
+        br[b].U[1] = h->bc_U[3 * b + 1];
+        br[b].U[2] = h->bc_U[3 * b + 2];
+        br[b].K_in = inv_norm_host(RT, D);
+        br[b].invRT_in = 1.0 / RT;
+        br[b].hfac = RT * K3D;
+        br[b].rho_in = h->bface_ptype[b] == DUGKS_PATCH_FAR_FIELD ? h->bc_rho[b] : 1.0;
+        br[b].inByRho = 0.0;
+    }
+    // face velocity for the first Courant number: linear interpolation
+    // (fvDVM.C:2116), U_f = w (U_own - U_nei) + U_nei
+    std::vector<double> fm(static_cast<size_t>(nIF + nBF) * 9, 0.0);
+    double co_max = 0, co_sum = 0;
+    for (int f = 0; f < nIF; ++f) {
+        const int64_t o = h->owner[f], n = h->neighbour[f];
+        double u2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            const double uf = h->weights[f] * (U[3 * o + k] - U[3 * n + k]) + U[3 * n + k];
+            fm[9 * static_cast<size_t>(f) + 1 + k] = uf;
+            u2 += uf * uf;
+        }
+        const double co = h->dc[f] * (std::sqrt(u2) + h->dm.xi_max_co);
+        co_max = std::max(co_max, co);
+        co_sum += co;
+    }
+    double co_host[2];
+    std::memcpy(&co_host[0], &co_max, sizeof(double));
+    co_host[1] = co_sum;
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.cm, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.cellrec, cr.data(), cr.size() * sizeof(dugks::CellRec), cudaMemcpyHostToDevice,
+                                h->stream));
+    if (nBF > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(h->ds.brec, br.data(), br.size() * sizeof(dugks::BRec), cudaMemcpyHostToDevice,
+                                    h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.fm, fm.data(), fm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.co, co_host, sizeof co_host, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->ds.err, 0, 4 * sizeof(int), h->stream));
+    h->ds.cur = 0;
+    dugks::StepArgs a = make_args(h, 0.0, 0.0);
+    CUDA_TRY(h, dugks::launch_init(a, h->precision, h->stream));
+    h->launches += h->nBF > 0 ? 2 : 1;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->initialised = true;
+    h->last_step_ms = 0;
+    return DUGKS_OK;
+}
+
+static int run_steps(dugks_handle* h, int32_t n_steps, const double* dt, double* stage_ms) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_step before dugks_set_macros");
+    if (n_steps < 0 || (n_steps > 0 && !dt)) return set_error(h, DUGKS_ERR_ARG, "dugks_step: bad arguments");
+    for (int i = 0; i < n_steps; ++i)
+        if (!(dt[i] > 0) || !std::isfinite(dt[i])) return set_error(h, DUGKS_ERR_ARG, "dugks_step: dt must be > 0");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaEvent_t sev[5] = {};
+    if (stage_ms) {
+        for (int k = 0; k < 5; ++k) {
+            CUDA_TRY(h, cudaEventCreate(&sev[k]));
+            stage_ms[k] = 0.0;
+        }
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+    int launches = 0;
+    for (int i = 0; i < n_steps; ++i) {
+        dugks::StepArgs a = make_args(h, dt[i], i + 1 < n_steps ? dt[i + 1] : 0.0);
+        if (h->cellrec_dt != dt[i]) {
+            CUDA_TRY(h, dugks::launch_cell_prep(a, h->stream));
+            ++launches;
+        }
+        CUDA_TRY(h, cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream));
+        if (!stage_ms) {
+            CUDA_TRY(h, dugks::launch_step(a, h->precision, h->stream, &launches));
+        } else {
+            CUDA_TRY(h, cudaEventRecord(sev[0], h->stream));
+            for (int stg = 0; stg < 4; ++stg) {
+                CUDA_TRY(h, dugks::launch_stage(a, h->precision, stg, h->stream, &launches));
+                CUDA_TRY(h, cudaEventRecord(sev[stg + 1], h->stream));
+            }
+            CUDA_TRY(h, cudaEventSynchronize(sev[4]));
+            for (int stg = 0; stg < 4; ++stg) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, sev[stg], sev[stg + 1]);
+                stage_ms[stg] += ms;
+            }
+        }
+        h->cellrec_dt = a.dt_next;
+        h->ds.cur = 1 - h->ds.cur;
+        h->steps_done++;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+    h->launches += launches;
+    int st = check_device_errors(h);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_step_ms = ms;
+    if (stage_ms) {
+        stage_ms[4] = ms;
+        for (int k = 0; k < 5; ++k) cudaEventDestroy(sev[k]);
+    }
+    return st;
+}
+
+int dugks_step(dugks_handle* h, int32_t n_steps, const double* dt) { return run_steps(h, n_steps, dt, nullptr); }
+
+int dugks_step_timed(dugks_handle* h, int32_t n_steps, const double* dt, double* stage_ms) {
+    if (!stage_ms) return set_error(h, DUGKS_ERR_ARG, "dugks_step_timed: null stage_ms");
+    return run_steps(h, n_steps, dt, stage_ms);
+}
+
+int64_t dugks_kernel_launches(const dugks_handle* h) { return h ? h->launches : 0; }
+
+int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean) {
+    if (!h || !co_max || !co_mean) return set_error(h, DUGKS_ERR_ARG, "dugks_co_num: null output");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_co_num before dugks_set_macros");
+    double co[2];
+    CUDA_TRY(h, cudaMemcpyAsync(co, h->ds.co, sizeof co, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double mx;
+    std::memcpy(&mx, &co[0], sizeof mx);
+    *co_max = mx * dt;
+    *co_mean = h->nIF > 0 ? co[1] / h->nIF * dt : 0.0;
+    return DUGKS_OK;
+}
+
+int dugks_get_macros(dugks_handle* h, double* rho, double* U, double* T, double* q) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_macros before dugks_set_macros");
+    const int nC = h->nC;
+    std::vector<double> cm(static_cast<size_t>(nC) * 9);
+    CUDA_TRY(h, cudaMemcpyAsync(cm.data(), h->ds.cm, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const std::vector<int32_t>& perm = h->tiling.perm;
+    for (int c = 0; c < nC; ++c) {
+        const int o = perm[c];
+        const double* m = &cm[9 * static_cast<size_t>(c)];
+        if (rho) rho[o] = m[0];
+        if (U)
+            for (int k = 0; k < 3; ++k) U[3 * o + k] = m[1 + k];
+        if (T) T[o] = m[4];
+        if (q)
+            for (int k = 0; k < 3; ++k) q[3 * o + k] = m[5 + k];
+    }
+    return DUGKS_OK;
+}
+
+int dugks_get_face_macros(dugks_handle* h, double* rho, double* U, double* T, double* q) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_face_macros before dugks_set_macros");
+    const int nF = h->nIF + h->nBF;
+    std::vector<double> fm(static_cast<size_t>(nF) * 9);
+    CUDA_TRY(h, cudaMemcpyAsync(fm.data(), h->ds.fm, fm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int f = 0; f < nF; ++f) {
+        const double* m = &fm[9 * static_cast<size_t>(f)];
+        if (rho) rho[f] = m[0];
+        if (U)
+            for (int k = 0; k < 3; ++k) U[3 * f + k] = m[1 + k];
+        if (T) T[f] = m[4];
+        if (q)
+            for (int k = 0; k < 3; ++k) q[3 * f + k] = m[5 + k];
+    }
+    return DUGKS_OK;
+}
+
+int dugks_get_boundary_rho(dugks_handle* h, double* rho_b) {
+    if (!h || !rho_b) return set_error(h, DUGKS_ERR_ARG, "dugks_get_boundary_rho: null output");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_boundary_rho before dugks_set_macros");
+    std::vector<dugks::BRec> br(h->nBF);
+    if (h->nBF > 0) {
+        CUDA_TRY(h, cudaMemcpyAsync(br.data(), h->ds.brec, br.size() * sizeof(dugks::BRec), cudaMemcpyDeviceToHost,
+                                    h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+    for (int b = 0; b < h->nBF; ++b) rho_b[b] = br[b].rho_in;
+    return DUGKS_OK;
+}
+
+int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out, double* h_out) {
+    if (!h || (n > 0 && (!cells || !g_out))) return set_error(h, DUGKS_ERR_ARG, "dugks_get_df: bad arguments");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_df before dugks_set_macros");
+    const size_t rs = real_size(h);
+    std::vector<unsigned char> col(static_cast<size_t>(h->nv) * rs);
+    for (int i = 0; i < n; ++i) {
+        if (cells[i] < 0 || cells[i] >= h->nC) return set_error(h, DUGKS_ERR_ARG, "dugks_get_df: cell out of range");
+        const int c = h->tiling.iperm[cells[i]];
+        for (int which = 0; which < 2; ++which) {
+            double* dst = which == 0 ? g_out : h_out;
+            if (!dst) continue;
+            const unsigned char* src =
+                static_cast<const unsigned char*>(which == 0 ? h->ds.g[h->ds.cur] : h->ds.h[h->ds.cur]) + c * rs;
+            CUDA_TRY(h, cudaMemcpy2DAsync(col.data(), rs, src, static_cast<size_t>(h->nC) * rs, rs, h->nv,
+                                          cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            for (int d = 0; d < h->nv; ++d) {
+                double v;
+                if (rs == sizeof(double)) std::memcpy(&v, &col[d * rs], sizeof v);
+                else {
+                    float fv;
+                    std::memcpy(&fv, &col[d * rs], sizeof fv);
+                    v = fv;
+                }
+                dst[static_cast<size_t>(i) * h->nv + d] = v;
+            }
+        }
+    }
+    return DUGKS_OK;
+}
+
+static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, const double* hi, bool get) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "state access before dugks_set_macros");
+    const size_t rs = real_size(h);
+    const size_t nvc = static_cast<size_t>(h->nv) * h->nC;
+    std::vector<unsigned char> buf(nvc * rs);
+    const std::vector<int32_t>& perm = h->tiling.perm;
+    for (int which = 0; which < 2; ++which) {
+        void* dev = which == 0 ? h->ds.g[h->ds.cur] : h->ds.h[h->ds.cur];
+        if (get) {
+            double* dst = which == 0 ? g : hh;
+            if (!dst) continue;
+            CUDA_TRY(h, cudaMemcpy(buf.data(), dev, nvc * rs, cudaMemcpyDeviceToHost));
+            for (int d = 0; d < h->nv; ++d)
+                for (int c = 0; c < h->nC; ++c) {
+                    const size_t s = static_cast<size_t>(d) * h->nC + c;
+                    const size_t o = static_cast<size_t>(d) * h->nC + perm[c];
+                    if (rs == sizeof(double)) std::memcpy(&dst[o], &buf[s * rs], sizeof(double));
+                    else {
+                        float fv;
+                        std::memcpy(&fv, &buf[s * rs], sizeof fv);
+                        dst[o] = fv;
+                    }
+                }
+        } else {
+            const double* src = which == 0 ? gi : hi;
+            if (!src) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: null array");
+            for (int d = 0; d < h->nv; ++d)
+                for (int c = 0; c < h->nC; ++c) {
+                    const size_t s = static_cast<size_t>(d) * h->nC + c;
+                    const size_t o = static_cast<size_t>(d) * h->nC + perm[c];
+                    if (rs == sizeof(double)) std::memcpy(&buf[s * rs], &src[o], sizeof(double));
+                    else {
+                        const float fv = static_cast<float>(src[o]);
+                        std::memcpy(&buf[s * rs], &fv, sizeof fv);
+                    }
+                }
+            CUDA_TRY(h, cudaMemcpy(dev, buf.data(), nvc * rs, cudaMemcpyHostToDevice));
+        }
+    }
+    return DUGKS_OK;
+}
+
+int dugks_get_state(dugks_handle* h, double* g, double* hh) { return state_io(h, g, hh, nullptr, nullptr, true); }
+
+int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double dt_prev) {
+    int st = state_io(h, nullptr, nullptr, g, hh, false);
+    if (st) return st;
+    if (!(dt_prev > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: dt_prev must be > 0");
+    dugks::StepArgs a = make_args(h, dt_prev, 0.0);
+    CUDA_TRY(h, dugks::launch_state_macros(a, h->precision, h->stream));
+    h->launches += 2;
+    h->cellrec_dt = 0;
+    return check_device_errors(h);
+}
+
+int32_t dugks_n_dv(const dugks_handle* h) { return h ? h->nv : 0; }
+
+int dugks_last_step_ms(dugks_handle* h, double* ms) {
+    if (!h || !ms) return DUGKS_ERR_ARG;
+    *ms = h->last_step_ms;
+    return DUGKS_OK;
+}
+
+const char* dugks_last_error(const dugks_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+void dugks_destroy(dugks_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocations) cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Launch interface of the DUGKS step kernels (dugks_kernels.cu).
+#pragma once
+
+#include "dugks_internal.h"
+
+namespace dugks {
+
+struct StepArgs {
+    DevMesh dm;
+    DevState ds;
+    double dt;
+    int chunks;
+    const int32_t* chunk_begin;  // [chunks+1]
+    double dt_next;              // time step of the following step (0 = unknown)
+    int ipt;                     // items per thread
+    int dims_local, dims_l0, dims_items;  // largest tile: local cells, L0 cells, items
+    size_t smemA, smemB;
+};
+
+enum { STAGE_PASS_A = 0, STAGE_FACE_COMBINE = 1, STAGE_PASS_B = 2, STAGE_CELL_COMBINE = 3 };
+
+// one DUGKS step (fvDVM::evolution) on the handle's stream, or one stage
+// of it; `launches` (may be null) is incremented by the kernels launched
+cudaError_t launch_step(const StepArgs& a, int precision, cudaStream_t s, int* launches);
+cudaError_t launch_stage(const StepArgs& a, int precision, int stage, cudaStream_t s, int* launches);
+// r = 1.5 dt / (2 tau + dt) for every cell record
+cudaError_t launch_cell_prep(const StepArgs& a, cudaStream_t s);
+// g~, h~ = Maxwellian; wall inComingByRho and incoming-moment vectors
+cudaError_t launch_init(const StepArgs& a, int precision, cudaStream_t s);
+// cell macros from the current state (raw moments over all DVs, then the
+// cell combine with time step dt for the heat-flux correction)
+cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s);
+// compute the dynamic shared memory sizes of the passes
+void pass_smem(const DevMesh& dm, int max_local, int max_l0, int max_items, int precision, size_t* smemA,
+               size_t* smemB);
+cudaError_t configure_kernels(int precision, int D, int ipt, size_t smemA, size_t smemB);
+
+}  // namespace dugks

@@ -1,0 +1,274 @@
+"""ctypes binding of the C ABI in include/dugks.h (libdugks_b200.so).
+
+``Solver`` mirrors the reference's fvDVM class (src/fvDVM/fvDVM/fvDVM.H:80-409):
+construct it from a flattened case, then ``evolution(dt)`` advances one time
+step (fvDVM::evolution, fvDVM.C:2128-2174) and ``get_co_num(dt)`` is
+fvDVM::getCoNum (fvDVM.C:2177-2185).  Errors raise :class:`DugksError`.
+The library is required: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libdugks_b200.so"))
+
+FP64 = 0
+FP32C = 1
+PATCH_MAXWELL_WALL = 1
+PATCH_FAR_FIELD = 2
+LS_MAGSF, LS_INVDIST, LS_UNWEIGHTED = 0, 1, 2
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_TIMEOUT", 5: "ERR_NAN", 6: "ERR_STATE",
+          7: "ERR_UNSUPPORTED"}
+
+
+class DugksError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+
+
+class Mesh(C.Structure):
+    _fields_ = [("n_cells", C.c_int32), ("n_internal_faces", C.c_int32), ("n_boundary_faces", C.c_int32),
+                ("n_solution_dims", C.c_int32), ("owner", _i64p), ("neighbour", _i64p),
+                ("cell_centres", _dp), ("cell_volumes", _dp), ("face_centres", _dp), ("face_areas", _dp),
+                ("n_patches", C.c_int32), ("patch_start", _i32p)]
+
+
+class DVSet(C.Structure):
+    _fields_ = [("n_per_dim", C.c_int32), ("xis", _dp), ("weights", _dp), ("xi_max", C.c_double)]
+
+
+class Gas(C.Structure):
+    _fields_ = [("R", C.c_double), ("omega", C.c_double), ("Tref", C.c_double), ("mu_ref", C.c_double),
+                ("Pr", C.c_double), ("K_inner", C.c_int32)]
+
+
+class BC(C.Structure):
+    _fields_ = [("patch_type", _i32p), ("rho", _dp), ("U", _dp), ("T", _dp)]
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("ls_weighting", C.c_int32), ("device", C.c_int32),
+                ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("reserved", C.c_int32 * 11)]
+
+
+# every symbol include/dugks.h declares, with its ctypes signature
+SIGNATURES = {
+    "dugks_abi_version": (C.c_int, []),
+    "dugks_default_options": (None, [C.POINTER(Options)]),
+    "dugks_mesh_geometry": (C.c_int, [C.c_int32, _dp, C.c_int32, _i64p, _i64p, _i64p, C.c_int32, _i64p, C.c_int32,
+                                      _dp, _dp, _dp, _dp]),
+    "dugks_create": (C.c_int, [C.POINTER(Mesh), C.POINTER(DVSet), C.POINTER(Gas), C.POINTER(BC),
+                               C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "dugks_set_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "dugks_step": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "dugks_co_num": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp]),
+    "dugks_get_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "dugks_get_face_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "dugks_get_boundary_rho": (C.c_int, [C.c_void_p, _dp]),
+    "dugks_get_df": (C.c_int, [C.c_void_p, _i32p, C.c_int32, _dp, _dp]),
+    "dugks_get_state": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "dugks_set_state": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double]),
+    "dugks_n_dv": (C.c_int32, [C.c_void_p]),
+    "dugks_last_step_ms": (C.c_int, [C.c_void_p, _dp]),
+    "dugks_step_timed": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
+    "dugks_kernel_launches": (C.c_int64, [C.c_void_p]),
+    "dugks_last_error": (C.c_char_p, [C.c_void_p]),
+    "dugks_destroy": (None, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libdugks_b200.so (built by __graft_entry__.build()); raises if absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} not found: build the CUDA library first (python -c 'import __graft_entry__ as g; g.build()')")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def ptr(a: np.ndarray | None, ctype=C.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def mesh_geometry(pm) -> dict:
+    """OpenFOAM primitiveMesh geometry of a polyMesh via the library's host routine."""
+    lib = load()
+    nF = pm.n_faces
+    Cf = np.zeros((nF, 3))
+    Sf = np.zeros((nF, 3))
+    Cc = np.zeros((pm.n_cells, 3))
+    V = np.zeros(pm.n_cells)
+    pts = np.ascontiguousarray(pm.points, dtype=np.float64)
+    fo = np.ascontiguousarray(pm.face_offsets, dtype=np.int64)
+    fp = np.ascontiguousarray(pm.face_points, dtype=np.int64)
+    own = np.ascontiguousarray(pm.owner, dtype=np.int64)
+    nei = np.ascontiguousarray(pm.neighbour, dtype=np.int64)
+    st = lib.dugks_mesh_geometry(len(pts), ptr(pts), nF, ptr(fo, C.c_int64), ptr(fp, C.c_int64), ptr(own, C.c_int64),
+                                 pm.n_internal_faces, ptr(nei, C.c_int64), pm.n_cells, ptr(Cf), ptr(Sf), ptr(Cc), ptr(V))
+    if st != 0:
+        raise DugksError(st, "dugks_mesh_geometry failed")
+    return {"Cf": Cf, "Sf": Sf, "C": Cc, "V": V}
+
+
+class Solver:
+    """fvDVM-shaped wrapper over one dugks_handle."""
+
+    def __init__(self, case, precision: int = FP64, ls_weighting: int = LS_MAGSF, device: int = 0,
+                 tile_cells: int = 0, dv_chunks: int = 0):
+        self.lib = load()
+        self.case = case
+        fc = case.flat
+        self._keep = []
+
+        def keep(a, dtype):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            self._keep.append(a)
+            return a
+
+        own = keep(fc["owner"], np.int64)
+        nei = keep(fc["neighbour"], np.int64)
+        cc = keep(fc["C"], np.float64)
+        vv = keep(fc["V"], np.float64)
+        cf = keep(fc["Cf"], np.float64)
+        sf = keep(fc["Sf"], np.float64)
+        ps = keep(fc["patch_start"], np.int32)
+        self.mesh = Mesh(case.n_cells, fc["n_internal"], fc["n_boundary"], case.D, ptr(own, C.c_int64),
+                         ptr(nei, C.c_int64), ptr(cc), ptr(vv), ptr(cf), ptr(sf), len(fc["patch_type"]),
+                         ptr(ps, C.c_int32))
+        xis = keep(case.xis, np.float64)
+        ws = keep(case.weights, np.float64)
+        self.dv = DVSet(len(xis), ptr(xis), ptr(ws), case.xi_max)
+        g = case.gas
+        self.gas = Gas(g["R"], g["omega"], g["Tref"], g["muRef"], g["Pr"], int(g.get("K", 0)))
+        pt = keep(fc["patch_type"], np.int32)
+        rb = keep(fc["rho_b"], np.float64)
+        ub = keep(fc["U_b"], np.float64)
+        tb = keep(fc["T_b"], np.float64)
+        self.bc = BC(ptr(pt, C.c_int32), ptr(rb), ptr(ub), ptr(tb))
+        opt = Options()
+        self.lib.dugks_default_options(C.byref(opt))
+        opt.precision = precision
+        opt.ls_weighting = ls_weighting
+        opt.device = device
+        opt.tile_cells = tile_cells
+        opt.dv_chunks = dv_chunks
+        h = C.c_void_p()
+        st = self.lib.dugks_create(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas), C.byref(self.bc),
+                                   C.byref(opt), C.byref(h))
+        self.h = h
+        if st != 0:
+            msg = self.lib.dugks_last_error(h).decode() if h.value else "dugks_create failed"
+            self.close()
+            raise DugksError(st, msg)
+        self.n_dv = self.lib.dugks_n_dv(self.h)
+        self.set_macros(case.rho0, case.U0, case.T0)
+
+    def _check(self, st):
+        if st != 0:
+            raise DugksError(st, self.lib.dugks_last_error(self.h).decode())
+
+    def set_macros(self, rho, U, T):
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        self._check(self.lib.dugks_set_macros(self.h, ptr(rho), ptr(U), ptr(T)))
+
+    def evolution(self, dt: float):
+        self.step(1, dt)
+
+    def step(self, n: int, dt):
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (n,)))
+        self._check(self.lib.dugks_step(self.h, n, ptr(dts)))
+
+    def step_timed(self, n: int, dt) -> np.ndarray:
+        """n steps with CUDA events around every stage: [passA, face combine,
+        passB, cell combine, total] milliseconds summed over the steps."""
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (n,)))
+        out = np.zeros(5)
+        self._check(self.lib.dugks_step_timed(self.h, n, ptr(dts), ptr(out)))
+        return out
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.dugks_kernel_launches(self.h))
+
+    def last_step_ms(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.dugks_last_step_ms(self.h, C.byref(v)))
+        return v.value
+
+    def get_co_num(self, dt: float):
+        a, b = C.c_double(), C.c_double()
+        self._check(self.lib.dugks_co_num(self.h, dt, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def macros(self) -> dict:
+        n = self.case.n_cells
+        rho, T = np.zeros(n), np.zeros(n)
+        U, q = np.zeros((n, 3)), np.zeros((n, 3))
+        self._check(self.lib.dugks_get_macros(self.h, ptr(rho), ptr(U), ptr(T), ptr(q)))
+        return {"rho": rho, "U": U, "T": T, "q": q}
+
+    def face_macros(self) -> dict:
+        nF = self.case.flat["n_internal"] + self.case.flat["n_boundary"]
+        rho, T = np.zeros(nF), np.zeros(nF)
+        U, q = np.zeros((nF, 3)), np.zeros((nF, 3))
+        self._check(self.lib.dugks_get_face_macros(self.h, ptr(rho), ptr(U), ptr(T), ptr(q)))
+        return {"rho": rho, "U": U, "T": T, "q": q}
+
+    def boundary_rho(self) -> np.ndarray:
+        out = np.zeros(self.case.flat["n_boundary"])
+        self._check(self.lib.dugks_get_boundary_rho(self.h, ptr(out)))
+        return out
+
+    def df(self, cells) -> tuple[np.ndarray, np.ndarray]:
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        g = np.zeros((len(cells), self.n_dv))
+        hh = np.zeros((len(cells), self.n_dv))
+        self._check(self.lib.dugks_get_df(self.h, ptr(cells, C.c_int32), len(cells), ptr(g), ptr(hh)))
+        return g, hh
+
+    def state(self) -> tuple[np.ndarray, np.ndarray]:
+        g = np.zeros((self.n_dv, self.case.n_cells))
+        hh = np.zeros((self.n_dv, self.case.n_cells))
+        self._check(self.lib.dugks_get_state(self.h, ptr(g), ptr(hh)))
+        return g, hh
+
+    def set_state(self, g, hh, dt_prev: float):
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        hh = np.ascontiguousarray(hh, dtype=np.float64)
+        self._check(self.lib.dugks_set_state(self.h, ptr(g), ptr(hh), dt_prev))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.dugks_destroy(self.h)
+        self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
