@@ -43,22 +43,23 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
+    p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
     return p.parse_args()
 
 
-def build_case(name):
+def build_case(name, ndv1d=0):
     from dugks_b200 import case as cs
     if name == "ball":
-        c = cs.ball_case(24, 32, 1.12, 16, kn=0.1, mach=0.5)
+        c = cs.ball_case(24, 32, 1.12, ndv1d or 16, kn=0.1, mach=0.5)
         cfg = {"workload": "ball: cubed sphere 6x24x24x32 (110592 cells), stretch 1.12, r 1..10, 16^3 GH DVs, "
                            "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall",
                "cells": c.n_cells, "n_dv": c.n_dv}
     elif name == "cube":
-        c = cs.cube_case(64, 20, kn=0.1)
+        c = cs.cube_case(64, ndv1d or 20, kn=0.1)
         cfg = {"workload": "cube: 64^3 lid-driven cube, 20^3 GH DVs, Kn 0.1, lid 50 m/s", "cells": c.n_cells,
                "n_dv": c.n_dv}
     else:
-        c = cs.cavity_case(61, 28)
+        c = cs.cavity_case(61, ndv1d or 28)
         cfg = {"workload": "cavity: 61x61 lid-driven cavity, 28^2 GH DVs, Kn 0.075, lid 50 m/s", "cells": c.n_cells,
                "n_dv": c.n_dv}
     cfg["dt"] = c.dt
@@ -168,7 +169,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, cfg = build_case(args.workload)
+    _, cfg = build_case(args.workload, args.ndv1d)
     steps = max(1, min(args.steps, 5))
     warm = 1
     cb = cpu_baseline(args.workload, args.cpu_sample_ndv, steps, warm)
@@ -196,7 +197,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     from dugks_b200 import lib as dl
-    case, cfg = build_case(args.workload)
+    case, cfg = build_case(args.workload, args.ndv1d)
     prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
     solver = dl.Solver(case, precision=prec, device=local)
     nv, nc = solver.n_dv, case.n_cells

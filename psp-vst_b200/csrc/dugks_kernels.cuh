@@ -30,6 +30,8 @@ cudaError_t launch_init(const StepArgs& a, int precision, cudaStream_t s);
 // cell macros from the current state (raw moments over all DVs, then the
 // cell combine with time step dt for the heat-flux correction)
 cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s);
+// one of the two tile passes (dugks_passes.cu)
+cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s);
 // compute the dynamic shared memory sizes of the passes
 void pass_smem(const DevMesh& dm, int max_local, int max_l0, int max_items, int precision, size_t* smemA,
                size_t* smemB);

@@ -181,3 +181,19 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def macro_errors(a: dict, b: dict, R: float, floor: float = 1e-4) -> dict:
+    """Relative L2 errors of macro fields a against reference b.
+
+    rho and T: plain relative L2.  U and q are sums over DVs that cancel to
+    (nearly) zero in quiescent regions, where both results are rounding noise
+    of size ~1e-16 of the sums' natural scale; their denominators are floored
+    at `floor` times that scale (thermal speed sqrt(RT) for U, rho (RT)^1.5
+    for q), i.e. about 100 ulps of the sums."""
+    rt = R * np.asarray(b["T"], dtype=np.float64)
+    out = {"rho": rel_l2(a["rho"], b["rho"]), "T": rel_l2(a["T"], b["T"])}
+    for k, scale in (("U", np.sqrt(rt)), ("q", np.asarray(b["rho"]) * rt ** 1.5)):
+        den = max(np.linalg.norm(b[k]), floor * np.linalg.norm(scale))
+        out[k] = float(np.linalg.norm(np.asarray(a[k]) - np.asarray(b[k])) / den)
+    return out

@@ -2,13 +2,17 @@
 the same seeded inputs.
 
 Tolerances: the FP64 path must match the oracle to <= 1e-10 relative L2 in
-rho, U, T and q (the reference's own bar for the plain path).  The FP32c
-path is compared against the FP64 oracle at <= 1e-5 after the short runs
-used here (the long-run <= 1e-6 bar is measured by the benchmark's FP32c
-arm on the full workload)."""
+rho, U, T and q (cell and face macros), the boundary rho and the whole
+state -- the bar the reference sets for the plain path.  U and q errors are
+taken against max(|field|, 1e-4 x its natural scale) (oracle_bind.
+macro_errors): both paths sum DVs in different orders, and where a moment
+cancels to near zero the results are rounding noise of the sum.  The FP32c
+path is compared with the FP64 oracle at <= 2e-6 over these short runs; its
+long-run error is measured on the full workload by bench.py."""
 import numpy as np
 import pytest
 
+import golden_cases
 import oracle_bind as ob
 from dugks_b200 import case as cs
 from dugks_b200 import lib as dl
@@ -17,37 +21,28 @@ from dugks_b200 import quadrature
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-10
-TOL32 = 1e-5
+TOL32 = 2e-6
 
 
 def _pair(case, **kw):
-    gpu = dl.Solver(case, **kw)
-    orc = ob.Oracle(case)
-    return gpu, orc
+    return dl.Solver(case, **kw), ob.Oracle(case)
 
 
-def _compare(gpu, orc, tol, what=("rho", "U", "T", "q")):
-    a, b = gpu.macros(), orc.macros()
-    errs = {k: ob.rel_l2(a[k], b[k]) for k in what}
-    return errs, max(errs.values()) <= tol
-
-
-def _run(case, steps, tol=TOL64, check_faces=True, **kw):
+def _run(case, steps, tol=TOL64, check_faces=True, floor=1e-4, **kw):
     gpu, orc = _pair(case, **kw)
-    for s in range(steps):
+    for _ in range(steps):
         gpu.evolution(case.dt)
         orc.evolution(case.dt)
-    errs, ok = _compare(gpu, orc, tol)
-    assert ok, f"{case.name}: cell macros rel-L2 {errs}"
+    R = case.gas["R"]
+    errs = ob.macro_errors(gpu.macros(), orc.macros(), R, floor)
+    assert max(errs.values()) <= tol, f"{case.name}: cell macros {errs}"
     if check_faces:
-        fa, fb = gpu.face_macros(), orc.face_macros()
-        ferrs = {k: ob.rel_l2(fa[k], fb[k]) for k in ("rho", "U", "T", "q")}
-        assert max(ferrs.values()) <= tol, f"{case.name}: face macros rel-L2 {ferrs}"
-        rb_g, rb_o = gpu.boundary_rho(), orc.boundary_rho()
-        assert ob.rel_l2(rb_g, rb_o) <= tol, f"{case.name}: boundary rho"
-    gs, hs = gpu.state()
-    go, ho = orc.state()
-    assert ob.rel_l2(gs, go) <= tol and ob.rel_l2(hs, ho) <= tol, f"{case.name}: state"
+        ferrs = ob.macro_errors(gpu.face_macros(), orc.face_macros(), R)
+        assert max(ferrs.values()) <= tol, f"{case.name}: face macros {ferrs}"
+        assert ob.rel_l2(gpu.boundary_rho(), orc.boundary_rho()) <= tol, f"{case.name}: boundary rho"
+        gs, hs = gpu.state()
+        go, ho = orc.state()
+        assert ob.rel_l2(gs, go) <= tol and ob.rel_l2(hs, ho) <= tol, f"{case.name}: state"
     return gpu, orc
 
 
@@ -80,12 +75,19 @@ def test_cavity_newton_cotes_parallel_faces():
     _run(c, 6, tile_cells=11, dv_chunks=3)
 
 
-def test_cube_fp64():
-    c = cs.cube_case(5, 6, kn=0.1)
-    _run(c, 6)
+def test_cube_fp64_multi_tile():
+    c = cs.cube_case(6, 6, kn=0.1)
+    _run(c, 6, tile_cells=16, dv_chunks=2)
 
 
 def test_ball_far_field_fp64():
+    # cubed sphere: non-orthogonal faces, far field + wall, faces on the cube
+    # diagonals where xi.S is tangential up to rounding
+    c = cs.ball_case(4, 4, 1.12, 8, kn=0.1, mach=0.5)
+    _run(c, 10)
+
+
+def test_ball_far_field_small_tiles():
     c = cs.ball_case(4, 4, 1.12, 8, kn=0.1, mach=0.5)
     _run(c, 6, tile_cells=32, dv_chunks=3)
 
@@ -93,29 +95,21 @@ def test_ball_far_field_fp64():
 def test_demo_cavity_mesh_fp64():
     # the reference demo's own polyMesh (blockMesh face order, which the
     # boundary h relaxation's internal-face index depends on), quadrature and fields
-    import golden_cases
     c = golden_cases.demo_cavity()
     _run(c, 3)
 
 
+# FP32 storage: the noise floor of the U and q sums is FP32 rounding, so
+# their denominators are floored at 1e-2 of the natural scale (~1e-8 of it
+# in absolute terms, a fraction of an FP32 ulp of the sums)
 def test_fp32c_cavity():
     c = cs.cavity_case(8, 8)
-    gpu, orc = _pair(c, precision=dl.FP32C)
-    for _ in range(20):
-        gpu.evolution(c.dt)
-        orc.evolution(c.dt)
-    errs, ok = _compare(gpu, orc, TOL32)
-    assert ok, errs
+    _run(c, 20, tol=TOL32, check_faces=False, floor=1e-2, precision=dl.FP32C)
 
 
 def test_fp32c_ball():
     c = cs.ball_case(4, 4, 1.12, 8, kn=0.1, mach=0.5)
-    gpu, orc = _pair(c, precision=dl.FP32C)
-    for _ in range(6):
-        gpu.evolution(c.dt)
-        orc.evolution(c.dt)
-    errs, ok = _compare(gpu, orc, TOL32)
-    assert ok, errs
+    _run(c, 6, tol=TOL32, check_faces=False, floor=1e-2, precision=dl.FP32C)
 
 
 def test_state_restart_is_exact():
@@ -125,9 +119,8 @@ def test_state_restart_is_exact():
     g, h = a.state()
     b = dl.Solver(c)
     b.set_state(g, h, c.dt)
-    ma, mb = a.macros(), b.macros()
-    for k in ("rho", "U", "T", "q"):
-        assert ob.rel_l2(mb[k], ma[k]) <= 1e-13, k
+    errs = ob.macro_errors(b.macros(), a.macros(), c.gas["R"])
+    assert max(errs.values()) <= 1e-13, errs
     a.step(3, c.dt)
     b.step(3, c.dt)
     ga, _ = a.state()
@@ -143,6 +136,19 @@ def test_df_output_matches_state():
     cells = np.array([0, 7, 35], dtype=np.int32)
     gd, hd = s.df(cells)
     assert np.array_equal(gd, g[:, cells].T) and np.array_equal(hd, h[:, cells].T)
+
+
+def test_multi_step_call_equals_single_steps():
+    # dugks_step(n) precomputes the next step's relax factors; the result
+    # must equal n separate calls
+    c = cs.cavity_case(8, 8)
+    a, b = dl.Solver(c), dl.Solver(c)
+    a.step(7, c.dt)
+    for _ in range(7):
+        b.step(1, c.dt)
+    ga, _ = a.state()
+    gb, _ = b.state()
+    assert np.array_equal(ga, gb)
 
 
 def test_errors_are_reported_not_fatal():
