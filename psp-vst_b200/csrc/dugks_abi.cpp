@@ -182,15 +182,15 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     for (double x : h->lsP)
         if (!std::isfinite(x)) return fail(DUGKS_ERR_ARG, "dugks_create: singular least-squares system");
 
-    // tiles: at most 4 items per thread
-    int tile = opt.tile_cells > 0 ? opt.tile_cells : (h->D == 3 ? 128 : 192);
-    tile = std::min(tile, dugks::kThreads);
+    // tiles: at most kMaxTile cells and 3 items per thread
+    int tile = opt.tile_cells > 0 ? opt.tile_cells : dugks::kMaxTile;
+    tile = std::min(tile, dugks::kMaxTile);
     for (;;) {
         dugks::build_tiling(h, tile);
-        if (h->tiling.max_items <= 4 * dugks::kThreads || tile <= 8) break;
+        if (h->tiling.max_items <= 3 * dugks::kThreads || tile <= 8) break;
         tile /= 2;
     }
-    if (h->tiling.max_items > 4 * dugks::kThreads)
+    if (h->tiling.max_items > 3 * dugks::kThreads)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: cells with too many faces for the tile layout");
     // DV chunks: enough CTAs to fill the GPU several times over
     int dev_count = 0;
@@ -201,7 +201,8 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-    int chunks = opt.dv_chunks > 0 ? opt.dv_chunks : (4 * sms + h->tiling.n_tiles - 1) / h->tiling.n_tiles;
+    // one CTA per SM runs at a time; aim at about two waves
+    int chunks = opt.dv_chunks > 0 ? opt.dv_chunks : (2 * sms + h->tiling.n_tiles - 1) / h->tiling.n_tiles;
     chunks = std::max(1, std::min(chunks, h->nv / 4 > 0 ? h->nv / 4 : 1));
     h->chunks = chunks;
     h->chunk_begin.resize(chunks + 1);
@@ -222,18 +223,22 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dm.nIF = nIF;
     dm.nBF = nBF;
     dm.nv = h->nv;
+    dm.prec = h->precision;
+    dm.n1d = h->n1d;
     dm.n_tiles = t.n_tiles;
-    dm.n_items = static_cast<int>(t.items.size());
+    dm.n_items = t.n_items();
     dm.n_tbf = t.n_tbf;
+    dm.nb_max = t.nb_max;
+    dm.nf_max = t.nf_max;
     dm.xi_max_co = std::sqrt(static_cast<double>(h->D)) * h->xi_max;
     int st;
     ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(ce));
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
-    double *d_xi, *d_w, *d_grad_ls, *d_dtV, *d_dc, *d_bS;
-    int32_t *d_tb, *d_tlo, *d_lc, *d_tio, *d_go, *d_gnb, *d_cfo, *d_cfi, *d_fi, *d_bpl, *d_bpt, *d_bown;
-    dugks::Item* d_items;
+    double *d_xi, *d_w, *d_grad_ls, *d_dtV, *d_dc, *d_bS, *d_geo;
+    int32_t *d_tb, *d_tlo, *d_lc, *d_tio, *d_gnb, *d_cfi, *d_fi, *d_bpl, *d_bpt, *d_bown;
+    int32_t *d_meta, *d_loc, *d_face, *d_xbw, *d_xbr;
     std::vector<double> dtV(nC);
     for (int c = 0; c < nC; ++c) dtV[c] = 1.0 / h->V[t.perm[c]];
     std::vector<double> bS(3 * static_cast<size_t>(nBF));
@@ -242,11 +247,15 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         for (int k = 0; k < 3; ++k) bS[3 * b + k] = h->Sf[3 * (nIF + b) + k];
         bown[b] = t.iperm[h->owner[nIF + b]];
     }
-    if ((st = upload(h, &d_xi, h->xi)) || (st = upload(h, &d_w, h->w)) || (st = upload(h, &d_tb, t.tile_begin)) ||
+    h->X1.assign(dv->xis, dv->xis + h->n1d);
+    double* d_X1;
+    if ((st = upload(h, &d_X1, h->X1)) ||
+        (st = upload(h, &d_xi, h->xi)) || (st = upload(h, &d_w, h->w)) || (st = upload(h, &d_tb, t.tile_begin)) ||
         (st = upload(h, &d_tlo, t.tile_loc_off)) || (st = upload(h, &d_lc, t.loc_cells)) ||
-        (st = upload(h, &d_tio, t.tile_item_off)) || (st = upload(h, &d_items, t.items)) ||
-        (st = upload(h, &d_go, t.grad_off)) || (st = upload(h, &d_gnb, t.grad_nb)) ||
-        (st = upload(h, &d_grad_ls, t.grad_ls)) || (st = upload(h, &d_cfo, t.cf_off)) ||
+        (st = upload(h, &d_tio, t.tile_item_off)) || (st = upload(h, &d_meta, t.it_meta)) ||
+        (st = upload(h, &d_loc, t.it_loc)) || (st = upload(h, &d_face, t.it_face)) ||
+        (st = upload(h, &d_xbw, t.it_xbw)) || (st = upload(h, &d_xbr, t.it_xbr)) || (st = upload(h, &d_geo, t.it_geo)) ||
+        (st = upload(h, &d_gnb, t.grad_nb)) || (st = upload(h, &d_grad_ls, t.grad_ls)) ||
         (st = upload(h, &d_cfi, t.cf_item)) || (st = upload(h, &d_dtV, dtV)) || (st = upload(h, &d_fi, t.face_items)) ||
         (st = upload(h, &d_bpl, h->bface_patch_local)) || (st = upload(h, &d_bpt, h->bface_ptype)) ||
         (st = upload(h, &d_bown, bown)) || (st = upload(h, &d_dc, h->dc)) || (st = upload(h, &d_bS, bS)) ||
@@ -254,17 +263,21 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         *out = h;
         return st;
     }
+    dm.X1 = d_X1;
     dm.xi = d_xi;
     dm.w = d_w;
     dm.tile_begin = d_tb;
     dm.tile_loc_off = d_tlo;
     dm.loc_cells = d_lc;
     dm.tile_item_off = d_tio;
-    dm.items = d_items;
-    dm.grad_off = d_go;
+    dm.it_meta = d_meta;
+    dm.it_loc = d_loc;
+    dm.it_face = d_face;
+    dm.it_xbw = d_xbw;
+    dm.it_xbr = d_xbr;
+    dm.it_geo = d_geo;
     dm.grad_nb = d_gnb;
     dm.grad_ls = d_grad_ls;
-    dm.cf_off = d_cfo;
     dm.cf_item = d_cfi;
     dm.dtV = d_dtV;
     dm.face_items = d_fi;
@@ -291,7 +304,11 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     ds.cur = 0;
     if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
-        (st = dev_alloc(h, &ds.cellrec, nC)) || (st = dev_alloc(h, &ds.facerec, nF)) ||
+        (st = dev_alloc(h, &ds.cellrec, static_cast<size_t>(dugks::REC_N) * nC)) ||
+        (st = dev_alloc(h, &ds.facerec, static_cast<size_t>(dugks::REC_N) * dm.n_items)) ||
+        (st = dev_alloc(h, &p, static_cast<size_t>(h->D) * h->n1d * nC * rs)) ||
+        ((ds.ctab = p), (st = dev_alloc(h, &p, static_cast<size_t>(h->D) * h->n1d * dm.n_items * rs))) ||
+        ((ds.ftab = p), false) ||
         (st = dev_alloc(h, &ds.brec, nBF)) || (st = dev_alloc(h, &ds.bmom_in, static_cast<size_t>(nBF) * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.cm, static_cast<size_t>(nC) * 9)) ||
         (st = dev_alloc(h, &ds.fm, static_cast<size_t>(nF) * 9)) || (st = dev_alloc(h, &ds.co, 2)) ||
@@ -318,7 +335,7 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     const double R = h->gas.R;
     const dugks::Tiling& t = h->tiling;
     std::vector<double> cm(static_cast<size_t>(nC) * 9);
-    std::vector<dugks::CellRec> cr(nC);
+    std::vector<double> cr(static_cast<size_t>(dugks::REC_N) * nC, 0.0);
     for (int c = 0; c < nC; ++c) {
         const int o = t.perm[c];
         if (!(rho[o] > 0) || !(T[o] > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: rho and T must be > 0");
@@ -332,15 +349,13 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
         m[5] = m[6] = m[7] = 0.0;
         m[8] = tau;
         const double RT = R * T[o];
-        dugks::CellRec& r = cr[c];
-        r.U[0] = m[1];
-        r.U[1] = m[2];
-        r.U[2] = m[3];
-        r.invRT = 1.0 / RT;
-        r.A = rho[o] * inv_norm_host(RT, D);
-        r.r = 0.0;
-        r.qv[0] = r.qv[1] = r.qv[2] = 0.0;
-        r.RT = RT;
+        const size_t n = static_cast<size_t>(nC);
+        cr[dugks::REC_UX * n + c] = m[1];
+        cr[dugks::REC_UY * n + c] = m[2];
+        cr[dugks::REC_UZ * n + c] = m[3];
+        cr[dugks::REC_INVRT * n + c] = 1.0 / RT;
+        cr[dugks::REC_A * n + c] = rho[o] * inv_norm_host(RT, D);
+        cr[dugks::REC_RTH * n + c] = RT;  // relax factor and heat-flux terms stay 0 (q = 0)
     }
     // boundary records
     const double K3D = h->gas.K_inner + 3.0 - D;
@@ -377,7 +392,7 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     std::memcpy(&co_host[0], &co_max, sizeof(double));
     co_host[1] = co_sum;
     CUDA_TRY(h, cudaMemcpyAsync(h->ds.cm, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, cudaMemcpyAsync(h->ds.cellrec, cr.data(), cr.size() * sizeof(dugks::CellRec), cudaMemcpyHostToDevice,
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.cellrec, cr.data(), cr.size() * sizeof(double), cudaMemcpyHostToDevice,
                                 h->stream));
     if (nBF > 0)
         CUDA_TRY(h, cudaMemcpyAsync(h->ds.brec, br.data(), br.size() * sizeof(dugks::BRec), cudaMemcpyHostToDevice,
@@ -388,7 +403,7 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     h->ds.cur = 0;
     dugks::StepArgs a = make_args(h, 0.0, 0.0);
     CUDA_TRY(h, dugks::launch_init(a, h->precision, h->stream));
-    h->launches += h->nBF > 0 ? 2 : 1;
+    h->launches += h->nBF > 0 ? 3 : 2;
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->initialised = true;
     h->last_step_ms = 0;

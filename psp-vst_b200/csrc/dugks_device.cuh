@@ -51,29 +51,6 @@ struct Rec {
     Real U[3], invRT, A, r, qv[3], RTh;
 };
 
-template <typename Real>
-__device__ __forceinline__ Rec<Real> load_rec(const CellRec* p) {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
-    Rec<Real> r;
-    r.U[0] = Real(a.x);
-    r.U[1] = Real(a.y);
-    r.U[2] = Real(b.x);
-    r.invRT = Real(b.y);
-    r.A = Real(c.x);
-    r.r = Real(c.y);
-    r.qv[0] = Real(d.x);
-    r.qv[1] = Real(d.y);
-    r.qv[2] = Real(e.x);
-    r.RTh = Real(e.y);
-    return r;
-}
-
-template <typename Real>
-__device__ __forceinline__ Rec<Real> load_rec(const FaceRec* p) {
-    return load_rec<Real>(reinterpret_cast<const CellRec*>(p));
-}
-
 // Shakhov equilibrium pair at velocity xi (fvDVM.C:673-679,
 // discreteVelocity.C:997-1007):
 //   gS = A e^{-cs/2} (1 + s (cs - D - 2)),
@@ -87,6 +64,21 @@ __device__ __forceinline__ void shakhov(const Real xi[3], const Rec<Real>& r, Re
     const Real cs = (cx * cx + cy * cy + cz * cz) * r.invRT;
     const Real s = cx * r.qv[0] + cy * r.qv[1] + (D == 3 ? cz * r.qv[2] : Real(0));
     const Real E = r.A * RealOps<Real>::ex(Real(-0.5) * cs);
+    gS = E * (Real(1) + s * (cs - Real(D + 2)));
+    hS = E * r.RTh * (K3D + s * ((cs - Real(D)) * K3D - Real(2) * Kin));
+}
+
+// The same pair from a precomputed Maxwellian value E = A e^{-cs/2}: the
+// D-dimensional Maxwellian of a tensor-product DV set is the product of
+// D one-dimensional factors A e_x(xi_x) e_y(xi_y) e_z(xi_z), tabulated per
+// cell and per face by the combine kernels.
+template <int D, typename Real>
+__device__ __forceinline__ void shakhov_m(const Real xi[3], const Rec<Real>& r, Real E, Real K3D, Real Kin, Real& gS,
+                                          Real& hS) {
+    const Real cx = xi[0] - r.U[0], cy = xi[1] - r.U[1];
+    const Real cz = D == 3 ? xi[2] - r.U[2] : Real(0);
+    const Real cs = (cx * cx + cy * cy + cz * cz) * r.invRT;
+    const Real s = cx * r.qv[0] + cy * r.qv[1] + (D == 3 ? cz * r.qv[2] : Real(0));
     gS = E * (Real(1) + s * (cs - Real(D + 2)));
     hS = E * r.RTh * (K3D + s * ((cs - Real(D)) * K3D - Real(2) * Kin));
 }
@@ -139,36 +131,6 @@ __device__ __forceinline__ void macros_from_moments(const double* s, const Const
 __device__ __forceinline__ double inv_norm(double RT, int D) {  // (2 pi R T)^(-D/2)
     const double t = 2.0 * 3.14159265358979323846 * RT;
     return D == 3 ? 1.0 / (t * sqrt(t)) : (D == 2 ? 1.0 / t : 1.0 / sqrt(t));
-}
-
-struct ItemView {
-    int kind, lo, ln, face, xb_w, xb_r, ptype;
-    double S[3], dO[3], dN[3];
-};
-
-__device__ __forceinline__ ItemView load_item(const Item* p) {
-    ItemView v;
-    const int4* ip = reinterpret_cast<const int4*>(p);
-    const int4 i0 = __ldg(ip), i1 = __ldg(ip + 1);
-    v.kind = i0.x;
-    v.lo = i0.y;
-    v.ln = i0.z;
-    v.face = i0.w;
-    v.xb_w = i1.x;
-    v.xb_r = i1.y;
-    v.ptype = i1.z;
-    const double2* dp = reinterpret_cast<const double2*>(p) + 2;
-    const double2 a = __ldg(dp), b = __ldg(dp + 1), c = __ldg(dp + 2), d = __ldg(dp + 3), e = __ldg(dp + 4);
-    v.S[0] = a.x;
-    v.S[1] = a.y;
-    v.S[2] = b.x;
-    v.dO[0] = b.y;
-    v.dO[1] = c.x;
-    v.dO[2] = c.y;
-    v.dN[0] = d.x;
-    v.dN[1] = d.y;
-    v.dN[2] = e.x;
-    return v;
 }
 
 // upwind weights of the owner and neighbour reconstructions at an internal

@@ -32,16 +32,6 @@ void sym_apply(const double* t, const double* d, double* o) {
     o[2] = t[2] * d[0] + t[4] * d[1] + t[5] * d[2];
 }
 
-uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
-    v &= 0x1fffff;
-    v = (v | v << 32) & 0x1f00000000ffffULL;
-    v = (v | v << 16) & 0x1f0000ff0000ffULL;
-    v = (v | v << 8) & 0x100f00f00f00f00fULL;
-    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
-    v = (v | v << 2) & 0x1249249249249249ULL;
-    return v;
-}
-
 }  // namespace
 
 extern "C" int dugks_mesh_geometry(int32_t n_points, const double* p, int32_t n_faces, const int64_t* fo,
@@ -250,36 +240,48 @@ void compute_weights_and_ls(dugks_handle* h, int weighting) {
     }
 }
 
-// Tile layout.  Cells are renumbered along a Morton curve of their centres
-// and cut into tiles of `tile_cells` consecutive cells (L0).  Each tile also
-// holds its ring L1 (face neighbours of L0 outside it), the gradient
-// stencils of its L0 cells and one item per face touching L0.
+}  // namespace dugks
+
+namespace {
+
+// Recursive coordinate bisection: cut the cell set along the longest axis
+// of its bounding box so that the first part holds a whole number of tiles,
+// until every part is one tile.  Consecutive tiles are neighbours in space.
+void rcb_order(const std::vector<double>& C, std::vector<int32_t>& idx, size_t b, size_t e, int tile) {
+    const size_t n = e - b;
+    if (n <= static_cast<size_t>(tile)) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (size_t i = b; i < e; ++i)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], C[3 * idx[i] + k]);
+            hi[k] = std::max(hi[k], C[3 * idx[i] + k]);
+        }
+    int ax = 0;
+    for (int k = 1; k < 3; ++k)
+        if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
+    const size_t nt = (n + tile - 1) / tile;
+    const size_t nl = (nt / 2) * static_cast<size_t>(tile);
+    std::stable_sort(idx.begin() + b, idx.begin() + e, [&](int32_t p, int32_t q) { return C[3 * p + ax] < C[3 * q + ax]; });
+    rcb_order(C, idx, b, b + nl, tile);
+    rcb_order(C, idx, b + nl, e, tile);
+}
+
+}  // namespace
+
+namespace dugks {
+
+// Tile layout.  Cells are renumbered by recursive coordinate bisection and
+// cut into tiles of `tile_cells` consecutive cells (L0).  Each tile also
+// holds its ring L1 (face neighbours of L0 outside it), and one item per
+// face touching L0, sorted by item kind.  Gradient stencils and flux lists
+// are stored slot-major ([slot][cell]) so that consecutive threads read
+// consecutive words.
 void build_tiling(dugks_handle* h, int tile_cells) {
     Tiling& t = h->tiling;
     const int nC = h->nC, nIF = h->nIF, nBF = h->nBF;
-    // Morton renumbering
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int c = 0; c < nC; ++c)
-        for (int k = 0; k < 3; ++k) {
-            lo[k] = std::min(lo[k], h->C[3 * c + k]);
-            hi[k] = std::max(hi[k], h->C[3 * c + k]);
-        }
-    double span = 0;
-    for (int k = 0; k < 3; ++k) span = std::max(span, hi[k] - lo[k]);
-    if (span <= 0) span = 1;
-    std::vector<uint64_t> code(nC);
-    for (int c = 0; c < nC; ++c) {
-        uint64_t q[3];
-        for (int k = 0; k < 3; ++k) {
-            double x = (h->C[3 * c + k] - lo[k]) / span;
-            x = std::min(std::max(x, 0.0), 1.0);
-            q[k] = static_cast<uint64_t>(x * 2097151.0);
-        }
-        code[c] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
-    }
     t.perm.resize(nC);
     std::iota(t.perm.begin(), t.perm.end(), 0);
-    std::stable_sort(t.perm.begin(), t.perm.end(), [&](int a, int b) { return code[a] < code[b]; });
+    rcb_order(h->C, t.perm, 0, nC, tile_cells);
     t.iperm.assign(nC, 0);
     for (int c = 0; c < nC; ++c) t.iperm[t.perm[c]] = c;
 
@@ -291,6 +293,13 @@ void build_tiling(dugks_handle* h, int tile_cells) {
     std::vector<int32_t> cfl(cfo[nC]), fill(cfo.begin(), cfo.end() - 1);
     for (int f = 0; f < nIF + nBF; ++f) cfl[fill[h->owner[f]]++] = f;
     for (int f = 0; f < nIF; ++f) cfl[fill[h->neighbour[f]]++] = f;
+    t.nb_max = t.nf_max = 0;
+    for (int c = 0; c < nC; ++c) {
+        int nb = 0;
+        for (int k = cfo[c]; k < cfo[c + 1]; ++k) nb += cfl[k] < nIF;
+        t.nb_max = std::max(t.nb_max, nb);
+        t.nf_max = std::max(t.nf_max, cfo[c + 1] - cfo[c]);
+    }
 
     t.tile_cells = tile_cells;
     t.n_tiles = (nC + tile_cells - 1) / tile_cells;
@@ -298,18 +307,21 @@ void build_tiling(dugks_handle* h, int tile_cells) {
     t.tile_loc_off.assign(t.n_tiles + 1, 0);
     t.tile_item_off.assign(t.n_tiles + 1, 0);
     t.loc_cells.clear();
-    t.items.clear();
-    t.grad_off.assign(nC + 1, 0);
-    t.grad_nb.clear();
-    t.grad_ls.clear();
-    t.cf_off.assign(nC + 1, 0);
-    t.cf_item.clear();
+    t.it_meta.clear();
+    t.it_loc.clear();
+    t.it_face.clear();
+    t.it_xbw.clear();
+    t.it_xbr.clear();
+    std::vector<double> geo;  // item-major scratch [n_items][9]
+    t.grad_nb.assign(static_cast<size_t>(t.nb_max) * nC, -1);
+    t.grad_ls.assign(static_cast<size_t>(t.nb_max) * 3 * nC, 0.0);
+    t.cf_item.assign(static_cast<size_t>(t.nf_max) * nC, 0);
     t.max_local = t.max_l0 = t.max_items = 0;
-    std::vector<int32_t> tile_of(nC);
-    for (int c = 0; c < nC; ++c) tile_of[c] = c / tile_cells;
-    // first pass per tile; XB slots assigned afterwards
     std::vector<int32_t> face_item0(nIF + nBF, -1), face_item1(nIF + nBF, -1);
     std::vector<int32_t> local_of(nC, -1);
+    struct Pending {
+        int kind, f;
+    };
     for (int ti = 0; ti < t.n_tiles; ++ti) {
         const int b = ti * tile_cells, e = std::min(nC, b + tile_cells), n0 = e - b;
         t.tile_begin[ti] = b;
@@ -335,97 +347,112 @@ void build_tiling(dugks_handle* h, int tile_cells) {
             local_of[l1[i]] = n0 + static_cast<int>(i);
             t.loc_cells.push_back(l1[i]);
         }
-        const int item0 = static_cast<int>(t.items.size());
-        t.tile_item_off[ti] = item0;
-        // items and gradient/flux stencils of the L0 cells
-        std::unordered_map<int, int> face_to_local_item;
+        // the tile's faces, sorted by kind
+        std::vector<Pending> pend;
         for (int c = b; c < e; ++c) {
             const int o = t.perm[c];
+            for (int k = cfo[o]; k < cfo[o + 1]; ++k) {
+                const int f = cfl[k];
+                int kind;
+                if (f < nIF) {
+                    const int own_new = t.iperm[h->owner[f]], nei_new = t.iperm[h->neighbour[f]];
+                    const bool own_in = own_new >= b && own_new < e, nei_in = nei_new >= b && nei_new < e;
+                    if (own_in && nei_in && own_new != c) continue;  // listed once, from the owner
+                    kind = (own_in && nei_in) ? ITEM_TILE_INTERNAL : (own_in ? ITEM_TB_OWN : ITEM_TB_NEI);
+                } else {
+                    kind = ITEM_MESH_BOUNDARY;
+                }
+                pend.push_back({kind, f});
+            }
+        }
+        std::stable_sort(pend.begin(), pend.end(), [](const Pending& p, const Pending& q) { return p.kind < q.kind; });
+        const int item0 = t.n_items();
+        t.tile_item_off[ti] = item0;
+        std::unordered_map<int, int> face_to_local_item;
+        for (const Pending& p : pend) {
+            const int f = p.f;
+            const int64_t fo = h->owner[f];
+            const int lo = local_of[t.iperm[fo]];
+            int ln = 0xffff, ptype = 0;
+            double g9[9];
+            for (int q = 0; q < 3; ++q) {
+                g9[q] = h->Sf[3 * f + q];
+                g9[3 + q] = h->Cf[3 * f + q] - h->C[3 * fo + q];
+                g9[6 + q] = 0.0;
+            }
+            if (f < nIF) {
+                const int64_t fn = h->neighbour[f];
+                ln = local_of[t.iperm[fn]];
+                for (int q = 0; q < 3; ++q) g9[6 + q] = h->Cf[3 * f + q] - h->C[3 * fn + q];
+            } else {
+                ptype = h->bface_ptype[f - nIF];
+            }
+            t.it_meta.push_back(p.kind | (ptype << 4));
+            t.it_loc.push_back(lo | (ln << 16));
+            t.it_face.push_back(f < nIF ? f : f - nIF);
+            t.it_xbw.push_back(-1);
+            t.it_xbr.push_back(-1);
+            geo.insert(geo.end(), g9, g9 + 9);
+            const int li = t.n_items() - 1 - item0;
+            face_to_local_item[f] = li;
+            if (face_item0[f] < 0) face_item0[f] = item0 + li;
+            else face_item1[f] = item0 + li;
+        }
+        // gradient stencils and flux lists of the L0 cells
+        for (int c = b; c < e; ++c) {
+            const int o = t.perm[c];
+            int sb = 0, sf = 0;
             for (int k = cfo[o]; k < cfo[o + 1]; ++k) {
                 const int f = cfl[k];
                 const bool is_own = h->owner[f] == o;
                 if (f < nIF) {
                     const int other = is_own ? static_cast<int>(h->neighbour[f]) : static_cast<int>(h->owner[f]);
-                    const int on = t.iperm[other];
-                    // gradient stencil
-                    t.grad_nb.push_back(local_of[on]);
+                    t.grad_nb[static_cast<size_t>(sb) * nC + c] = local_of[t.iperm[other]];
                     const double* ls = is_own ? &h->lsP[3 * f] : &h->lsN[3 * f];
-                    t.grad_ls.insert(t.grad_ls.end(), ls, ls + 3);
+                    for (int q = 0; q < 3; ++q) t.grad_ls[(static_cast<size_t>(sb) * 3 + q) * nC + c] = ls[q];
+                    ++sb;
                 }
-                int li;
-                auto it = face_to_local_item.find(f);
-                if (it != face_to_local_item.end()) {
-                    li = it->second;
-                } else {
-                    Item item{};
-                    item.face = f < nIF ? f : f - nIF;
-                    item.xb_w = item.xb_r = -1;
-                    item.ptype = 0;
-                    const int64_t fo_ = h->owner[f];
-                    const int own_new = t.iperm[fo_];
-                    item.lo = local_of[own_new];
-                    for (int q = 0; q < 3; ++q) {
-                        item.S[q] = h->Sf[3 * f + q];
-                        item.dO[q] = h->Cf[3 * f + q] - h->C[3 * fo_ + q];
-                        item.dN[q] = 0.0;
-                    }
-                    if (f < nIF) {
-                        const int64_t fn_ = h->neighbour[f];
-                        const int nei_new = t.iperm[fn_];
-                        item.ln = local_of[nei_new];
-                        for (int q = 0; q < 3; ++q) item.dN[q] = h->Cf[3 * f + q] - h->C[3 * fn_ + q];
-                        const bool own_in = own_new >= b && own_new < e;
-                        const bool nei_in = nei_new >= b && nei_new < e;
-                        item.kind = (own_in && nei_in) ? ITEM_TILE_INTERNAL : (own_in ? ITEM_TB_OWN : ITEM_TB_NEI);
-                    } else {
-                        item.ln = -1;
-                        item.kind = ITEM_MESH_BOUNDARY;
-                        item.ptype = h->bface_ptype[f - nIF];
-                    }
-                    li = static_cast<int>(t.items.size()) - item0;
-                    t.items.push_back(item);
-                    face_to_local_item[f] = li;
-                    const int gi = item0 + li;
-                    if (face_item0[f] < 0) face_item0[f] = gi;
-                    else face_item1[f] = gi;
-                }
-                // flux gather: owner subtracts, neighbour adds
-                t.cf_item.push_back(is_own ? -(li + 1) : (li + 1));
+                const int li = face_to_local_item.at(f);
+                t.cf_item[static_cast<size_t>(sf) * nC + c] = is_own ? -(li + 1) : (li + 1);
+                ++sf;
             }
-            t.grad_off[c + 1] = static_cast<int32_t>(t.grad_nb.size());
-            t.cf_off[c + 1] = static_cast<int32_t>(t.cf_item.size());
         }
         for (int c = b; c < e; ++c) local_of[c] = -1;
         for (int c : l1) local_of[c] = -1;
         t.max_local = std::max(t.max_local, n0 + static_cast<int>(l1.size()));
         t.max_l0 = std::max(t.max_l0, n0);
-        t.max_items = std::max(t.max_items, static_cast<int>(t.items.size()) - item0);
+        t.max_items = std::max(t.max_items, t.n_items() - item0);
     }
     t.tile_begin[t.n_tiles] = nC;
     t.tile_loc_off[t.n_tiles] = static_cast<int32_t>(t.loc_cells.size());
-    t.tile_item_off[t.n_tiles] = static_cast<int32_t>(t.items.size());
-    // the per-cell offsets were filled only at c+1; make them cumulative
-    // (cells are visited in increasing order, so entries are already set)
-    // XB slots of tile-boundary faces: side 0 (owner side) numbered in the
-    // order the owner tiles list them, side 1 in the order of the neighbour tiles
+    t.tile_item_off[t.n_tiles] = t.n_items();
+    // XB slots of tile-boundary faces.  XB side 0 holds the owner side's
+    // contribution, which the neighbour's tile reads; it is numbered in the
+    // order the neighbour tiles list their faces (slot1).  Side 1 holds the
+    // neighbour side's contribution, numbered in the owner tiles' order
+    // (slot0).  Reads are contiguous; the scattered side is the write.
+    const int ni = t.n_items();
     std::vector<int32_t> slot0(nIF, -1), slot1(nIF, -1);
     int n0s = 0, n1s = 0;
-    for (size_t i = 0; i < t.items.size(); ++i) {
-        Item& it = t.items[i];
-        if (it.kind == ITEM_TB_OWN) slot0[it.face] = n0s++;
-        else if (it.kind == ITEM_TB_NEI) slot1[it.face] = n1s++;
+    for (int i = 0; i < ni; ++i) {
+        const int kind = t.it_meta[i] & 15;
+        if (kind == ITEM_TB_OWN) slot0[t.it_face[i]] = n0s++;
+        else if (kind == ITEM_TB_NEI) slot1[t.it_face[i]] = n1s++;
     }
     t.n_tbf = n0s;
-    for (size_t i = 0; i < t.items.size(); ++i) {
-        Item& it = t.items[i];
-        if (it.kind == ITEM_TB_OWN) {
-            it.xb_w = slot0[it.face];
-            it.xb_r = slot1[it.face];
-        } else if (it.kind == ITEM_TB_NEI) {
-            it.xb_w = slot1[it.face];
-            it.xb_r = slot0[it.face];
+    for (int i = 0; i < ni; ++i) {
+        const int kind = t.it_meta[i] & 15;
+        if (kind == ITEM_TB_OWN) {
+            t.it_xbw[i] = slot1[t.it_face[i]];
+            t.it_xbr[i] = slot0[t.it_face[i]];
+        } else if (kind == ITEM_TB_NEI) {
+            t.it_xbw[i] = slot0[t.it_face[i]];
+            t.it_xbr[i] = slot1[t.it_face[i]];
         }
     }
+    t.it_geo.assign(static_cast<size_t>(9) * ni, 0.0);
+    for (int i = 0; i < ni; ++i)
+        for (int q = 0; q < 9; ++q) t.it_geo[static_cast<size_t>(q) * ni + i] = geo[static_cast<size_t>(i) * 9 + q];
     t.face_items.assign(2 * static_cast<size_t>(nIF + nBF), -1);
     for (int f = 0; f < nIF + nBF; ++f) {
         t.face_items[2 * f] = face_item0[f];

