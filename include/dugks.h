@@ -212,6 +212,32 @@ int64_t dugks_kernel_launches(const dugks_handle* h);
 const char* dugks_last_error(const dugks_handle* h);
 void dugks_destroy(dugks_handle* h);
 
+/* Cell macros of caller-owned device DFs without any device allocation.
+ * No counterpart in the reference: it is the reduction of dugks_set_state
+ * (fvDVM::updateMacroVol, fvDVM.C:1528-1554, :1682-1742) for callers that
+ * cannot allocate -- a monitor or post-processing step between time steps,
+ * on its own stream, next to a solver that has taken the device memory up
+ * front: cudaMalloc would fail there, and cudaFree synchronises the whole
+ * device and stalls the solver's queued work.  Its scratch is a fixed
+ * 16 MiB device array inside this library.
+ *   n_dims, n_dv, xi [n_dv*3], w [n_dv]: the DV set, as dugks_get_state's
+ *       DV order uses it (x fastest); g, hh: DV-major [n_dv][n_cells] FP64;
+ *   gas, dt: as dugks_create's gas and the time step that produced g, hh
+ *       (it enters the heat-flux factor 2 tau/(2 tau + dt Pr));
+ *   rho [n], U [n*3], T [n], q [n*3]: outputs, any may be NULL.
+ * xi, w, g, hh and the outputs are DEVICE pointers of the current device
+ * (others are rejected); gas is a host pointer; stream is a cudaStream_t
+ * (NULL: the default stream); the call only enqueues work on it.  msg
+ * (msg_len bytes, may be NULL) receives the error text.
+ * Limits: n_cells <= 131072 per call (DUGKS_ERR_ARG beyond).  The first call
+ * on a device looks up the scratch address and caches it: make it before
+ * any stream capture on that device.  Nothing has to start at zero.  Calls
+ * that overlap in time on one device share the scratch and race: serialise
+ * them. */
+int dugks_cell_macros_noalloc(int32_t n_dims, int32_t n_dv, const double* xi, const double* w, int32_t n_cells,
+                              const double* g, const double* hh, const dugks_gas* gas, double dt, double* rho,
+                              double* U, double* T, double* q, void* stream, char* msg, int32_t msg_len);
+
 #ifdef __cplusplus
 }
 #endif

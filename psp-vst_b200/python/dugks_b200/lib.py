@@ -85,6 +85,9 @@ SIGNATURES = {
     "dugks_kernel_launches": (C.c_int64, [C.c_void_p]),
     "dugks_last_error": (C.c_char_p, [C.c_void_p]),
     "dugks_destroy": (None, [C.c_void_p]),
+    "dugks_cell_macros_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                            C.c_void_p, C.POINTER(Gas), C.c_double, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int32]),
 }
 
 _lib = None
