@@ -59,11 +59,7 @@ dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
     a.dt_next = dt_next;
     a.chunks = h->chunks;
     a.chunk_begin = h->d_chunk_begin;
-    a.ipt = (h->tiling.max_items + dugks::kThreads - 1) / dugks::kThreads;
-    a.dims_local = h->tiling.max_local;
-    a.dims_l0 = h->tiling.max_l0;
-    a.dims_items = h->tiling.max_items;
-    dugks::pass_smem(h->dm, a.dims_local, a.dims_l0, a.dims_items, h->precision, &a.smemA, &a.smemB);
+    dugks::pass_config(h->D, h->precision, h->n1d, &a.wideA, &a.wideB, &a.smemA, &a.smemB);
     return a;
 }
 
@@ -113,6 +109,8 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     if (mesh->n_solution_dims != 2 && mesh->n_solution_dims != 3)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: n_solution_dims must be 2 or 3");
     if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
+    if (dv->n_per_dim > dugks::kMaxN1d)
+        return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: more than 64 DV nodes per dimension");
     if (opt.precision != DUGKS_FP64 && opt.precision != DUGKS_FP32C)
         return fail(DUGKS_ERR_ARG, "dugks_create: unknown precision");
     if (!(gas->R > 0) || !(gas->Tref > 0) || !(gas->mu_ref > 0)) return fail(DUGKS_ERR_ARG, "dugks_create: bad gas");
@@ -182,15 +180,17 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     for (double x : h->lsP)
         if (!std::isfinite(x)) return fail(DUGKS_ERR_ARG, "dugks_create: singular least-squares system");
 
-    // tiles: at most kMaxTile cells and 3 items per thread
+    // tiles: at most kMaxTile cells, kMaxLocal cells with the ring, and one
+    // item per thread; shrink until the largest tile fits
     int tile = opt.tile_cells > 0 ? opt.tile_cells : dugks::kMaxTile;
     tile = std::min(tile, dugks::kMaxTile);
     for (;;) {
         dugks::build_tiling(h, tile);
-        if (h->tiling.max_items <= 3 * dugks::kThreads || tile <= 8) break;
-        tile /= 2;
+        const bool fits = h->tiling.max_items <= dugks::kMaxItems && h->tiling.max_local <= dugks::kMaxLocal;
+        if (fits || tile <= 4) break;
+        tile = std::max(4, tile * 7 / 8);
     }
-    if (h->tiling.max_items > 3 * dugks::kThreads)
+    if (h->tiling.max_items > dugks::kMaxItems || h->tiling.max_local > dugks::kMaxLocal)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: cells with too many faces for the tile layout");
     // DV chunks: enough CTAs to fill the GPU several times over
     int dev_count = 0;
@@ -201,13 +201,16 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-    // one CTA per SM runs at a time; aim at about two waves
+    // one CTA per SM runs at a time; aim at about two waves.  Chunks are
+    // whole DV rows (n1d DVs along x at fixed y, z): the passes walk a row in
+    // batches and factor the x direction out of their sums
+    const int rows = h->nv / h->n1d;
     int chunks = opt.dv_chunks > 0 ? opt.dv_chunks : (2 * sms + h->tiling.n_tiles - 1) / h->tiling.n_tiles;
-    chunks = std::max(1, std::min(chunks, h->nv / 4 > 0 ? h->nv / 4 : 1));
+    chunks = std::max(1, std::min(chunks, rows));
     h->chunks = chunks;
     h->chunk_begin.resize(chunks + 1);
     for (int c = 0; c <= chunks; ++c)
-        h->chunk_begin[c] = static_cast<int32_t>((static_cast<int64_t>(h->nv) * c) / chunks);
+        h->chunk_begin[c] = static_cast<int32_t>((static_cast<int64_t>(rows) * c) / chunks);
 
     // ---- device layout ----
     const dugks::Tiling& t = h->tiling;
@@ -227,7 +230,6 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dm.n1d = h->n1d;
     dm.n_tiles = t.n_tiles;
     dm.n_items = t.n_items();
-    dm.n_tbf = t.n_tbf;
     dm.nb_max = t.nb_max;
     dm.nf_max = t.nf_max;
     dm.xi_max_co = std::sqrt(static_cast<double>(h->D)) * h->xi_max;
@@ -238,7 +240,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     cudaEventCreate(&h->ev1);
     double *d_xi, *d_w, *d_grad_ls, *d_dtV, *d_dc, *d_bS, *d_geo;
     int32_t *d_tb, *d_tlo, *d_lc, *d_tio, *d_gnb, *d_cfi, *d_fi, *d_bpl, *d_bpt, *d_bown;
-    int32_t *d_meta, *d_loc, *d_face, *d_xbw, *d_xbr;
+    int32_t *d_meta, *d_loc, *d_face, *d_other;
     std::vector<double> dtV(nC);
     for (int c = 0; c < nC; ++c) dtV[c] = 1.0 / h->V[t.perm[c]];
     std::vector<double> bS(3 * static_cast<size_t>(nBF));
@@ -248,13 +250,14 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         bown[b] = t.iperm[h->owner[nIF + b]];
     }
     h->X1.assign(dv->xis, dv->xis + h->n1d);
-    double* d_X1;
-    if ((st = upload(h, &d_X1, h->X1)) ||
+    h->W1.assign(dv->weights, dv->weights + h->n1d);
+    double *d_X1, *d_W1;
+    if ((st = upload(h, &d_X1, h->X1)) || (st = upload(h, &d_W1, h->W1)) ||
         (st = upload(h, &d_xi, h->xi)) || (st = upload(h, &d_w, h->w)) || (st = upload(h, &d_tb, t.tile_begin)) ||
         (st = upload(h, &d_tlo, t.tile_loc_off)) || (st = upload(h, &d_lc, t.loc_cells)) ||
         (st = upload(h, &d_tio, t.tile_item_off)) || (st = upload(h, &d_meta, t.it_meta)) ||
         (st = upload(h, &d_loc, t.it_loc)) || (st = upload(h, &d_face, t.it_face)) ||
-        (st = upload(h, &d_xbw, t.it_xbw)) || (st = upload(h, &d_xbr, t.it_xbr)) || (st = upload(h, &d_geo, t.it_geo)) ||
+        (st = upload(h, &d_other, t.it_other)) || (st = upload(h, &d_geo, t.it_geo)) ||
         (st = upload(h, &d_gnb, t.grad_nb)) || (st = upload(h, &d_grad_ls, t.grad_ls)) ||
         (st = upload(h, &d_cfi, t.cf_item)) || (st = upload(h, &d_dtV, dtV)) || (st = upload(h, &d_fi, t.face_items)) ||
         (st = upload(h, &d_bpl, h->bface_patch_local)) || (st = upload(h, &d_bpt, h->bface_ptype)) ||
@@ -264,6 +267,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         return st;
     }
     dm.X1 = d_X1;
+    dm.W1 = d_W1;
     dm.xi = d_xi;
     dm.w = d_w;
     dm.tile_begin = d_tb;
@@ -273,8 +277,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dm.it_meta = d_meta;
     dm.it_loc = d_loc;
     dm.it_face = d_face;
-    dm.it_xbw = d_xbw;
-    dm.it_xbr = d_xbr;
+    dm.it_other = d_other;
     dm.it_geo = d_geo;
     dm.grad_nb = d_gnb;
     dm.grad_ls = d_grad_ls;
@@ -289,18 +292,18 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dugks::DevState& ds = h->ds;
     const size_t rs = real_size(h);
     const size_t nvc = static_cast<size_t>(h->nv) * nC;
-    const size_t nxb = static_cast<size_t>(h->nv) * std::max(t.n_tbf, 1);
+    const size_t nfv = static_cast<size_t>(h->nv) * std::max(dm.n_items, 1);
     unsigned char* p;
     for (int i = 0; i < 2; ++i) {
         if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
         ds.g[i] = p;
         if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
         ds.h[i] = p;
-        if ((st = dev_alloc(h, &p, nxb * rs))) return *out = h, st;
-        ds.xbg[i] = p;
-        if ((st = dev_alloc(h, &p, nxb * rs))) return *out = h, st;
-        ds.xbh[i] = p;
     }
+    if ((st = dev_alloc(h, &p, nfv * rs))) return *out = h, st;
+    ds.fvg = p;
+    if ((st = dev_alloc(h, &p, nfv * rs))) return *out = h, st;
+    ds.fvh = p;
     ds.cur = 0;
     if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
@@ -321,7 +324,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     ce = cudaMemset(ds.partF, 0, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM * sizeof(double));
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, cudaGetErrorString(ce));
     dugks::StepArgs a = make_args(h, 0.0, 0.0);
-    ce = dugks::configure_kernels(h->precision, h->D, a.ipt, a.smemA, a.smemB);
+    ce = dugks::configure_kernels(h->precision, h->D, a.wideA, a.wideB, a.smemA, a.smemB);
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("configure kernels: ") + cudaGetErrorString(ce));
     *out = h;
     return DUGKS_OK;

@@ -310,8 +310,7 @@ void build_tiling(dugks_handle* h, int tile_cells) {
     t.it_meta.clear();
     t.it_loc.clear();
     t.it_face.clear();
-    t.it_xbw.clear();
-    t.it_xbr.clear();
+    t.it_other.clear();
     std::vector<double> geo;  // item-major scratch [n_items][9]
     t.grad_nb.assign(static_cast<size_t>(t.nb_max) * nC, -1);
     t.grad_ls.assign(static_cast<size_t>(t.nb_max) * 3 * nC, 0.0);
@@ -390,8 +389,7 @@ void build_tiling(dugks_handle* h, int tile_cells) {
             t.it_meta.push_back(p.kind | (ptype << 4));
             t.it_loc.push_back(lo | (ln << 16));
             t.it_face.push_back(f < nIF ? f : f - nIF);
-            t.it_xbw.push_back(-1);
-            t.it_xbr.push_back(-1);
+            t.it_other.push_back(-1);
             geo.insert(geo.end(), g9, g9 + 9);
             const int li = t.n_items() - 1 - item0;
             face_to_local_item[f] = li;
@@ -426,29 +424,14 @@ void build_tiling(dugks_handle* h, int tile_cells) {
     t.tile_begin[t.n_tiles] = nC;
     t.tile_loc_off[t.n_tiles] = static_cast<int32_t>(t.loc_cells.size());
     t.tile_item_off[t.n_tiles] = t.n_items();
-    // XB slots of tile-boundary faces.  XB side 0 holds the owner side's
-    // contribution, which the neighbour's tile reads; it is numbered in the
-    // order the neighbour tiles list their faces (slot1).  Side 1 holds the
-    // neighbour side's contribution, numbered in the owner tiles' order
-    // (slot0).  Reads are contiguous; the scattered side is the write.
+    // the item of the other side of every tile-boundary face: pass B reads
+    // that side's share of the face value from the item's face-value slot
     const int ni = t.n_items();
-    std::vector<int32_t> slot0(nIF, -1), slot1(nIF, -1);
-    int n0s = 0, n1s = 0;
     for (int i = 0; i < ni; ++i) {
         const int kind = t.it_meta[i] & 15;
-        if (kind == ITEM_TB_OWN) slot0[t.it_face[i]] = n0s++;
-        else if (kind == ITEM_TB_NEI) slot1[t.it_face[i]] = n1s++;
-    }
-    t.n_tbf = n0s;
-    for (int i = 0; i < ni; ++i) {
-        const int kind = t.it_meta[i] & 15;
-        if (kind == ITEM_TB_OWN) {
-            t.it_xbw[i] = slot1[t.it_face[i]];
-            t.it_xbr[i] = slot0[t.it_face[i]];
-        } else if (kind == ITEM_TB_NEI) {
-            t.it_xbw[i] = slot0[t.it_face[i]];
-            t.it_xbr[i] = slot1[t.it_face[i]];
-        }
+        if (kind != ITEM_TB_OWN && kind != ITEM_TB_NEI) continue;
+        const int f = t.it_face[i];
+        t.it_other[i] = face_item0[f] == i ? face_item1[f] : face_item0[f];
     }
     t.it_geo.assign(static_cast<size_t>(9) * ni, 0.0);
     for (int i = 0; i < ni; ++i)

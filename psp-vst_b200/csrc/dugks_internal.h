@@ -13,7 +13,10 @@
 namespace dugks {
 
 constexpr int kThreads = 512;      // threads per CTA of the two tile passes
-constexpr int kMaxTile = 256;      // cells per tile (L0) at most
+constexpr int kMaxTile = 128;      // cells per tile (L0) at most
+constexpr int kMaxLocal = 256;     // L0 + L1 cells per tile at most
+constexpr int kMaxItems = kThreads;  // items per tile at most (one per thread)
+constexpr int kMaxN1d = 64;        // DV nodes per dimension at most
 constexpr int kNM = 16;            // stride of a partial-moment record (doubles)
 constexpr double kVSmall = 1.0e-300;  // OpenFOAM VSMALL (upwind switch, fvDVM.C:829-847)
 
@@ -72,6 +75,7 @@ struct DevMesh {
     const double* w;       // [nv]
     int n1d;               // nodes per dimension; DV d = (iz n + iy) n + ix
     const double* X1;      // [n1d] one-dimensional nodes
+    const double* W1;      // [n1d] one-dimensional weights
     // tiles
     const int32_t* tile_begin;     // [n_tiles+1] L0 = [begin, begin+n0) (renumbered cells)
     const int32_t* tile_loc_off;   // [n_tiles+1] into loc_cells
@@ -81,8 +85,7 @@ struct DevMesh {
     const int32_t* it_meta;        // kind | ptype << 4
     const int32_t* it_loc;         // lo | ln << 16 (0xffff: none); local indices
     const int32_t* it_face;        // internal face id, or boundary face id
-    const int32_t* it_xbw;         // XB slot written (tile-boundary items)
-    const int32_t* it_xbr;         // XB slot of the other side read
+    const int32_t* it_other;       // tile-boundary items: the item of the face's other side
     const double* it_geo;          // [9][n_items]: S, Cf - C_own, Cf - C_nei
     // gradient stencils and flux lists, slot-major [slot][cell]
     int nb_max, nf_max;
@@ -98,7 +101,6 @@ struct DevMesh {
     const double* dc;              // [nIF] deltaCoeffs
     const double* bS;              // [nBF*3] boundary face area vectors
     int n_items;
-    int n_tbf;
     double xi_max_co;              // sqrt(D) * xiMax
 };
 
@@ -107,8 +109,11 @@ struct DevState {
     void* g[2];        // state g~ double buffer [nv][nC] (Real)
     void* h[2];
     int cur;
-    void* xbg[2];      // XB buffers [side][nv][n_tbf]
-    void* xbh[2];
+    // face values [nv][n_items] (Real): pass A's upwind reconstruction at the
+    // half step of every item, weighted by the side's share on tile-boundary
+    // faces; pass B relaxes them instead of reconstructing again
+    void* fvg;
+    void* fvh;
     double* partF;     // [chunks][n_items][kNM]
     double* partC;     // [chunks][nC][kNM]
     double* cellrec;   // [REC_N][nC]
@@ -136,13 +141,12 @@ struct Tiling {
     std::vector<int32_t> perm;      // new -> old cell
     std::vector<int32_t> iperm;     // old -> new
     std::vector<int32_t> tile_begin, tile_loc_off, loc_cells, tile_item_off;
-    std::vector<int32_t> it_meta, it_loc, it_face, it_xbw, it_xbr;
+    std::vector<int32_t> it_meta, it_loc, it_face, it_other;
     std::vector<double> it_geo;     // [9][n_items]
     std::vector<int32_t> grad_nb;   // [nb_max][nC]
     std::vector<double> grad_ls;    // [nb_max][3][nC]
     std::vector<int32_t> cf_item;   // [nf_max][nC]
     std::vector<int32_t> face_items;
-    int n_tbf = 0;
     int n_items() const { return static_cast<int>(it_meta.size()); }
 };
 
@@ -159,13 +163,13 @@ struct dugks_handle {
     std::vector<int32_t> bface_ptype, bface_patch_local;
     std::vector<double> bc_rho, bc_U, bc_T;
     std::vector<double> xi, w;      // tensor-product DV set
-    std::vector<double> X1;         // one-dimensional nodes
+    std::vector<double> X1, W1;     // one-dimensional nodes and weights
     // geometry (original numbering)
     std::vector<int64_t> owner, neighbour;
     std::vector<double> C, V, Cf, Sf, weights, dc, lsP, lsN, lsB;
     dugks::Tiling tiling;
     int chunks = 1;
-    std::vector<int32_t> chunk_begin;   // DV chunk boundaries [chunks+1]
+    std::vector<int32_t> chunk_begin;   // DV chunk boundaries in DV rows [chunks+1]
     // device
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

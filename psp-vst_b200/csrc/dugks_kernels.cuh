@@ -10,11 +10,10 @@ struct StepArgs {
     DevState ds;
     double dt;
     int chunks;
-    const int32_t* chunk_begin;  // [chunks+1]
+    const int32_t* chunk_begin;  // [chunks+1] DV rows
     double dt_next;              // time step of the following step (0 = unknown)
-    int ipt;                     // items per thread
-    int dims_local, dims_l0, dims_items;  // largest tile: local cells, L0 cells, items
-    size_t smemA, smemB;
+    int wideA, wideB;            // batch width of each pass: 1 wide, 0 narrow
+    size_t smemA, smemB;         // dynamic shared memory of the passes
 };
 
 enum { STAGE_PASS_A = 0, STAGE_FACE_COMBINE = 1, STAGE_PASS_B = 2, STAGE_CELL_COMBINE = 3 };
@@ -32,9 +31,9 @@ cudaError_t launch_init(const StepArgs& a, int precision, cudaStream_t s);
 cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s);
 // one of the two tile passes (dugks_passes.cu)
 cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s);
-// compute the dynamic shared memory sizes of the passes
-void pass_smem(const DevMesh& dm, int max_local, int max_l0, int max_items, int precision, size_t* smemA,
-               size_t* smemB);
-cudaError_t configure_kernels(int precision, int D, int ipt, size_t smemA, size_t smemB);
+// batch widths and dynamic shared memory of the passes for a DV set of n1d
+// nodes per dimension
+void pass_config(int D, int precision, int n1d, int* wideA, int* wideB, size_t* smemA, size_t* smemB);
+cudaError_t configure_kernels(int precision, int D, int wideA, int wideB, size_t smemA, size_t smemB);
 
 }  // namespace dugks

@@ -1,95 +1,74 @@
 // The two tile passes of the DUGKS step (sm_100a).
 //
-// A CTA of 512 threads owns one tile (up to 256 L0 cells, their L1 ring, and
-// the items = faces touching L0, sorted by kind) and one chunk of discrete
-// velocities, which it walks in batches of NB DVs.  Per batch:
-//   stage 1  gbar+/hbar+ of the L0+L1 cells into shared memory
-//            (updateGHbarPvol, fvDVM.C:648-683); one thread per cell
+// Discrete velocities are walked in batches of NB consecutive DVs of one DV
+// row (the n1d DVs along x at fixed y and z).  Within a batch xi = (x_j, Y, Z)
+// varies in x only, so xi.S, the Shakhov exponent and the raw moments split
+// into a part computed once per batch (Y, Z) and a short per-DV part in x.
+//
+// Pass A: one CTA of 512 threads per (tile, DV chunk).  A tile is up to 128
+// L0 cells, their L1 ring (up to 256 local cells in all) and its items = the
+// faces touching L0 (up to 512, one per thread), sorted by kind.  Per batch:
+//   stage 0  cp.async of the NEXT batch's g~, h~ and one-dimensional
+//            Maxwellian factors of the local cells into shared memory,
+//            overlapping this batch's stages
+//   stage 1  gbar+/hbar+ of the local cells (updateGHbarPvol,
+//            fvDVM.C:648-683)
 //   stage 2  least-squares gradients of the L0 cells (leastSquaresGrad;
-//            boundary faces add lsB * (patch value - cell value) = 0, the
-//            gBarPvol patches being zero-gradient fixedGradient,
-//            fvDVM.C:456-485, :775-809); two threads per cell, DVs split
+//            the zero-gradient boundary terms vanish, fvDVM.C:456-485,
+//            :775-809)
 //   stage 3  per item: upwind reconstruction at the half step
-//            (updateGHbarSurf, fvDVM.C:755-1029), branch-free: the upwind
-//            side is selected, not branched on
-//            pass A: raw face moments in registers (updateMacroSurf,
-//                    :1181-1297), wall out-flux, XB hand-over
-//            pass B: face relaxation (updateGHsurf, :1362-1457), flux
-//   stage 4  (pass B) flux gather, g~/h~ update (updateGHtildeVol,
-//            :1462-1519) and raw cell moments (updateMacroVol, :1528-1554)
-// Every table the CTA reads (cell and face records, item geometry, stencils)
-// is a structure of arrays indexed by consecutive threads; the DV rows of
-// g~, h~ are read with consecutive threads on consecutive cells.
+//            (updateGHbarSurf, fvDVM.C:755-1029); raw face moments in
+//            registers (updateMacroSurf, :1181-1297) and the wall out-flux;
+//            the reconstructed value goes to the face-value buffer
+// Pass B: one CTA per (tile, DV chunk), L0 cells and items only.  Per batch:
+//   stage 3  per item: relaxation of the stored face value (updateGHsurf,
+//            :1362-1457), incoming boundary DFs, flux xi.S g_f to shared memory
+//   stage 4  per L0 cell: gbar+ of the cell, flux gather and g~/h~ update
+//            (updateGHtildeVol, :1462-1519), raw cell moments (updateMacroVol,
+//            :1528-1554)
 #include "dugks_device.cuh"
 
 namespace dugks {
 
 namespace {
 
-constexpr int kCellSplit = kThreads / kMaxTile;  // threads per L0 cell in stages 2 and 4
+constexpr int kSL = kMaxLocal;           // row stride of local-cell arrays in shared memory
+constexpr int kS0 = kMaxTile;            // row stride of L0-cell arrays
+constexpr int kSI = kMaxItems;           // row stride of item arrays
+constexpr int kPartsL = kThreads / kSL;  // threads per local cell in stages 0-1
+constexpr int kParts0 = kThreads / kS0;  // threads per L0 cell in stages 2 and 4
 
+// batch widths: pass A (narrow, wide), pass B (narrow, wide)
 template <typename Real>
-struct Batch;
+struct Width;
 template <>
-struct Batch<double> {
-    static constexpr int A = 8, B = 4;
+struct Width<double> {
+    static constexpr int A0 = 8, A1 = 8, B0 = 8, B1 = 8;
 };
 template <>
-struct Batch<float> {
-    static constexpr int A = 16, B = 8;
+struct Width<float> {
+    static constexpr int A0 = 8, A1 = 16, B0 = 8, B1 = 16;
 };
 
-template <int D, typename Real, int NB>
-struct Smem {
-    double* dv;      // [NB][5]: xi (3), w, |xi|^2
-    int* dvi;        // [NB][4]: ix, iy, iz of the DV
-    Real *gB, *hB;   // [NB][sl]
-    Real *Gg, *Gh;   // [NB][sg]
-    Real *Fg, *Fh;   // [NB][si]   pass B
-    Real *gT, *hT;   // [NB][s0]   pass B
-    int sl, sg, si, s0;
-};
-
-template <int D, typename Real, int NB>
-__device__ __forceinline__ Smem<D, Real, NB> carve(unsigned char* base, const StepArgs& a) {
-    Smem<D, Real, NB> s;
-    s.dv = reinterpret_cast<double*>(base);
-    s.dvi = reinterpret_cast<int*>(base + NB * 5 * sizeof(double));
-    Real* p = reinterpret_cast<Real*>(base + NB * 5 * sizeof(double) + NB * 4 * sizeof(int));
-    s.sl = a.dims_local;
-    s.sg = a.dims_l0 * D;
-    s.si = a.dims_items;
-    s.s0 = a.dims_l0;
-    s.gB = p;
-    p += NB * s.sl;
-    s.hB = p;
-    p += NB * s.sl;
-    s.Gg = p;
-    p += NB * s.sg;
-    s.Gh = p;
-    p += NB * s.sg;
-    s.Fg = p;
-    p += NB * s.si;
-    s.Fh = p;
-    p += NB * s.si;
-    s.gT = p;
-    p += NB * s.s0;
-    s.hT = p;
-    return s;
+// ---------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async, L1-allocating)
+// ---------------------------------------------------------------------
+template <typename Real>
+__device__ __forceinline__ void cp_async(Real* sdst, const Real* gsrc) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    if (sizeof(Real) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int D, typename Real, int NB>
-size_t smem_bytes(int max_local, int max_l0, int max_items, bool pass_b) {
-    size_t n = 2 * static_cast<size_t>(max_local) + 2 * static_cast<size_t>(max_l0) * D;
-    if (pass_b) n += 2 * static_cast<size_t>(max_items) + 2 * static_cast<size_t>(max_l0);
-    size_t bytes = NB * 5 * sizeof(double) + NB * 4 * sizeof(int) + NB * n * sizeof(Real);
-    // the end-of-CTA reduction of the split cell moments reuses the arrays
-    const size_t red = static_cast<size_t>(kMaxTile) * 15 * sizeof(double) + NB * 5 * sizeof(double);
-    return bytes > red ? bytes : red;
-}
-
+// ---------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------
 struct TileRange {
-    int b, n0, loff, nloc, ioff, nit, d0, d1;
+    int b, n0, loff, nloc, ioff, nit, r0, r1;
 };
 
 __device__ __forceinline__ TileRange tile_range(const DevMesh& m, const int32_t* chunk_begin) {
@@ -101,127 +80,390 @@ __device__ __forceinline__ TileRange tile_range(const DevMesh& m, const int32_t*
     t.nloc = __ldg(m.tile_loc_off + tile + 1) - t.loff;
     t.ioff = __ldg(m.tile_item_off + tile);
     t.nit = __ldg(m.tile_item_off + tile + 1) - t.ioff;
-    t.d0 = __ldg(chunk_begin + chunk);
-    t.d1 = __ldg(chunk_begin + chunk + 1);
+    t.r0 = __ldg(chunk_begin + chunk);
+    t.r1 = __ldg(chunk_begin + chunk + 1);
     return t;
 }
 
-// load a coefficient record (structure of arrays, n entities)
-template <typename Real>
-__device__ __forceinline__ Rec<Real> load_rec_soa(const double* __restrict__ rec, int n, int e) {
-    Rec<Real> r;
-    r.U[0] = Real(__ldg(rec + REC_UX * static_cast<size_t>(n) + e));
-    r.U[1] = Real(__ldg(rec + REC_UY * static_cast<size_t>(n) + e));
-    r.U[2] = Real(__ldg(rec + REC_UZ * static_cast<size_t>(n) + e));
-    r.invRT = Real(__ldg(rec + REC_INVRT * static_cast<size_t>(n) + e));
-    r.A = Real(__ldg(rec + REC_A * static_cast<size_t>(n) + e));
-    r.r = Real(__ldg(rec + REC_R * static_cast<size_t>(n) + e));
-    r.qv[0] = Real(__ldg(rec + REC_QX * static_cast<size_t>(n) + e));
-    r.qv[1] = Real(__ldg(rec + REC_QY * static_cast<size_t>(n) + e));
-    r.qv[2] = Real(__ldg(rec + REC_QZ * static_cast<size_t>(n) + e));
-    r.RTh = Real(__ldg(rec + REC_RTH * static_cast<size_t>(n) + e));
-    return r;
-}
-
-struct ItemSoa {
-    int kind, ptype, lo, ln, face, xbw, xbr;
-    double S[3], dO[3], dN[3];
+// position of batch k of a chunk: first x index, width, first DV, row indices
+struct BatchPos {
+    int ix0, nb, d0, iy, iz;
 };
 
-__device__ __forceinline__ ItemSoa load_item_soa(const DevMesh& m, int i) {
-    ItemSoa v;
-    const int meta = __ldg(m.it_meta + i), loc = __ldg(m.it_loc + i);
+// walks the batches of a chunk of DV rows in order (x batches of a row,
+// then the next row) without integer divisions per batch
+template <int D, int NB>
+struct BatchWalk {
+    int row, iy, iz, kb, nbr, n1d;
+    __device__ __forceinline__ BatchWalk(int r0, int n) : row(r0), kb(0), nbr((n + NB - 1) / NB), n1d(n) {
+        iy = D == 3 ? r0 % n : r0;
+        iz = D == 3 ? r0 / n : 0;
+    }
+    __device__ __forceinline__ BatchPos pos() const {
+        BatchPos p;
+        p.ix0 = kb * NB;
+        p.nb = min(NB, n1d - p.ix0);
+        p.d0 = row * n1d + p.ix0;
+        p.iy = iy;
+        p.iz = iz;
+        return p;
+    }
+    __device__ __forceinline__ void next() {
+        if (++kb == nbr) {
+            kb = 0;
+            ++row;
+            if (++iy == n1d && D == 3) {
+                iy = 0;
+                ++iz;
+            }
+        }
+    }
+};
+
+// per-batch DV constants: the y, z velocity and weight of the row and the
+// products the moment fold needs.  The DV weight is w1[iz] w1[iy] w1[ix]
+// (3-D) or w1[iy] w1[ix] (2-D), as the tensor product is formed.
+struct RowConst {
+    double Y, Z, wyz, R2, cY, cZ, cYY, cYZ, cZZ;
+};
+
+template <int D>
+__device__ __forceinline__ RowConst row_const(const double* x1, const double* w1, const BatchPos& p) {
+    RowConst q;
+    q.Y = x1[p.iy];
+    q.Z = D == 3 ? x1[p.iz] : 0.0;
+    q.wyz = D == 3 ? w1[p.iz] * w1[p.iy] : w1[p.iy];
+    q.R2 = q.Y * q.Y + q.Z * q.Z;
+    q.cY = q.wyz * q.Y;
+    q.cZ = q.wyz * q.Z;
+    q.cYY = q.cY * q.Y;
+    q.cYZ = q.cY * q.Z;
+    q.cZZ = q.cZ * q.Z;
+    return q;
+}
+
+// Raw moments of one batch, summed along x (a = w_x g, b = w_x h):
+// S_k = sum a x^k (k = 0..3), B_k = sum b x^k (k = 0, 1), O = sum a xi.S
+// over outgoing wall DVs.  row_fold turns them into the moment record
+// (layout in dugks_internal.h) with |xi|^2 = x^2 + Y^2 + Z^2.
+struct RowSums {
+    double S0, S1, S2, S3, B0, B1, O;
+};
+
+__device__ __forceinline__ void row_zero(RowSums& r) { r.S0 = r.S1 = r.S2 = r.S3 = r.B0 = r.B1 = r.O = 0.0; }
+
+__device__ __forceinline__ double row_add(RowSums& r, double wx, double x, double g, double h) {
+    const double a = wx * g, b = wx * h;
+    r.S0 += a;
+    const double ax = a * x;
+    r.S1 += ax;
+    const double ax2 = ax * x;
+    r.S2 += ax2;
+    r.S3 = fma(ax2, x, r.S3);
+    r.B0 += b;
+    r.B1 = fma(b, x, r.B1);
+    return a;
+}
+
+template <int D>
+__device__ __forceinline__ void row_fold(double* acc, const RowSums& r, const RowConst& q) {
+    const double c = q.wyz;
+    const double Wb = r.S2 + fma(q.R2, r.S0, r.B0);   // sum a |xi|^2 + b
+    const double Vx = r.S3 + fma(q.R2, r.S1, r.B1);   // sum (a |xi|^2 + b) x
+    acc[MOM_M0] = fma(c, r.S0, acc[MOM_M0]);
+    acc[MOM_M1] = fma(c, r.S1, acc[MOM_M1]);
+    acc[MOM_M1 + 1] = fma(q.cY, r.S0, acc[MOM_M1 + 1]);
+    acc[MOM_W] = fma(c, Wb, acc[MOM_W]);
+    acc[MOM_V3] = fma(c, Vx, acc[MOM_V3]);
+    acc[MOM_V3 + 1] = fma(q.cY, Wb, acc[MOM_V3 + 1]);
+    acc[MOM_M2] = fma(c, r.S2, acc[MOM_M2]);
+    acc[MOM_M2 + 1] = fma(q.cY, r.S1, acc[MOM_M2 + 1]);
+    acc[MOM_M2 + 3] = fma(q.cYY, r.S0, acc[MOM_M2 + 3]);
+    if (D == 3) {
+        acc[MOM_M1 + 2] = fma(q.cZ, r.S0, acc[MOM_M1 + 2]);
+        acc[MOM_V3 + 2] = fma(q.cZ, Wb, acc[MOM_V3 + 2]);
+        acc[MOM_M2 + 2] = fma(q.cZ, r.S1, acc[MOM_M2 + 2]);
+        acc[MOM_M2 + 4] = fma(q.cYZ, r.S0, acc[MOM_M2 + 4]);
+        acc[MOM_M2 + 5] = fma(q.cZZ, r.S0, acc[MOM_M2 + 5]);
+    }
+    acc[MOM_OUT] = fma(c, r.O, acc[MOM_OUT]);
+}
+
+// xi.S rounded as the reference evaluates it, ((x Sx + y Sy) + z Sz) without
+// fused multiply-adds, with the y and z products of the row precomputed
+__device__ __forceinline__ double xs_row(double x, double Sx, double p2, double p3) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(x, Sx), p2), p3);
+}
+
+// ---------------------------------------------------------------------
+// Shakhov relaxation pair of one DV from the per-batch parts of a record
+//   gbar = (1-r) g + r gS,  hbar = (1-r) h + r hS   (fvDVM.C:668-679, :1374-1391)
+//   gS = E (1 + s (cs - D - 2)),  hS = E RTh (K3D + s ((cs - D) K3D - 2 K))
+//   cs = |xi-U|^2 / RT = (x-Ux)^2 / RT + Cyz,  s = (xi-U).qv = (x-Ux) qx + Syz
+//   r E = (A e_x(x)) (r e_y(Y) e_z(Z))
+// ---------------------------------------------------------------------
+template <typename Real>
+struct Shk {
+    Real Ux, invRT, qx, RTh, omr;   // per entity
+    Real Cyz, Syz, eyzr;            // per entity and batch
+};
+
+template <int D, typename Real>
+__device__ __forceinline__ void shk_batch(Shk<Real>& s, Real Uy, Real Uz, Real qy, Real qz, Real r, double Y, double Z,
+                                          Real ey, Real ez) {
+    const Real cy = Real(Y) - Uy;
+    const Real cz = D == 3 ? Real(Z) - Uz : Real(0);
+    s.Cyz = (cy * cy + cz * cz) * s.invRT;
+    s.Syz = D == 3 ? cy * qy + cz * qz : cy * qy;
+    s.eyzr = D == 3 ? r * ey * ez : r * ey;
+}
+
+template <int D, typename Real>
+__device__ __forceinline__ void shk_relax(const Shk<Real>& s, Real x, Real ex, Real g, Real h, Real K3D, Real c0h,
+                                          Real& go, Real& ho) {
+    const Real cx = x - s.Ux;
+    const Real cs = fma(cx * cx, s.invRT, s.Cyz);
+    const Real sq = fma(cx, s.qx, s.Syz);
+    const Real Er = ex * s.eyzr;
+    const Real pg = fma(sq, cs - Real(D + 2), Real(1));
+    const Real ph = fma(sq, fma(cs, K3D, c0h), K3D);
+    go = fma(s.omr, g, Er * pg);
+    ho = fma(s.omr, h, (Er * s.RTh) * ph);
+}
+
+// ---------------------------------------------------------------------
+// Shared memory
+// ---------------------------------------------------------------------
+enum { CR_UX, CR_UY, CR_UZ, CR_INVRT, CR_QX, CR_QY, CR_QZ, CR_RTH, CR_OMR, CR_R, CR_N };
+
+template <int D, typename Real, int NB>
+struct SmemA {
+    double* x1;     // [kMaxN1d] 1-D nodes
+    double* w1;     // [kMaxN1d] 1-D weights
+    Real* crec;     // [CR_N][kSL] records of the local cells
+    Real* stg;      // [2][3][NB][kSL] staged g~, h~, e_x (double buffer)
+    Real* stgyz;    // [2][2][kSL] staged e_y, e_z
+    Real* gB;       // [NB][kSL] gbar+
+    Real* hB;
+    Real* Gg;       // [NB][D][kS0] gradients of the L0 cells
+    Real* Gh;
+    static constexpr size_t bytes() {
+        return 2 * kMaxN1d * sizeof(double) +
+               (static_cast<size_t>(CR_N) * kSL + 2 * 3 * NB * kSL + 2 * 2 * kSL + 2 * NB * kSL + 2 * NB * D * kS0) *
+                   sizeof(Real);
+    }
+};
+
+template <int D, typename Real, int NB>
+__device__ __forceinline__ SmemA<D, Real, NB> carve_a(unsigned char* base) {
+    SmemA<D, Real, NB> s;
+    s.x1 = reinterpret_cast<double*>(base);
+    s.w1 = s.x1 + kMaxN1d;
+    Real* p = reinterpret_cast<Real*>(s.w1 + kMaxN1d);
+    s.crec = p;
+    p += CR_N * kSL;
+    s.stg = p;
+    p += 2 * 3 * NB * kSL;
+    s.stgyz = p;
+    p += 2 * 2 * kSL;
+    s.gB = p;
+    p += NB * kSL;
+    s.hB = p;
+    p += NB * kSL;
+    s.Gg = p;
+    p += NB * D * kS0;
+    s.Gh = p;
+    return s;
+}
+
+template <typename Real, int NB>
+struct SmemB {
+    double* x1;
+    double* w1;
+    Real* Fg;     // [NB][kSI] fluxes xi.S g_f of the items
+    Real* Fh;
+    Real* frec;   // [CR_N][kSI] face records of the items
+    Real* crec;   // [CR_N][kS0] records of the L0 cells
+    Real* st;     // [3][NB][kSI] staged face values g, h and e_x of the items
+    double* red;  // end-of-CTA reduction of the split cell moments (aliases st)
+    static constexpr size_t bytes() {
+        return 2 * kMaxN1d * sizeof(double) +
+               (5 * static_cast<size_t>(NB) * kSI + static_cast<size_t>(CR_N) * (kSI + kS0)) * sizeof(Real);
+    }
+};
+
+template <typename Real, int NB>
+__device__ __forceinline__ SmemB<Real, NB> carve_b(unsigned char* base) {
+    SmemB<Real, NB> s;
+    s.x1 = reinterpret_cast<double*>(base);
+    s.w1 = s.x1 + kMaxN1d;
+    s.Fg = reinterpret_cast<Real*>(s.w1 + kMaxN1d);
+    s.Fh = s.Fg + NB * kSI;
+    s.frec = s.Fh + NB * kSI;
+    s.crec = s.frec + CR_N * kSI;
+    s.st = s.crec + CR_N * kS0;
+    s.red = reinterpret_cast<double*>(s.st);
+    return s;
+}
+
+// a coefficient record (structure of arrays over n entities) into shared
+// memory: U, 1/RT, qv, RTh, 1 - r, r
+template <typename Real>
+__device__ __forceinline__ void stash_rec(Real* dst, int stride, int l, const double* __restrict__ rec, size_t n, int e) {
+    dst[CR_UX * stride + l] = Real(__ldg(rec + REC_UX * n + e));
+    dst[CR_UY * stride + l] = Real(__ldg(rec + REC_UY * n + e));
+    dst[CR_UZ * stride + l] = Real(__ldg(rec + REC_UZ * n + e));
+    dst[CR_INVRT * stride + l] = Real(__ldg(rec + REC_INVRT * n + e));
+    dst[CR_QX * stride + l] = Real(__ldg(rec + REC_QX * n + e));
+    dst[CR_QY * stride + l] = Real(__ldg(rec + REC_QY * n + e));
+    dst[CR_QZ * stride + l] = Real(__ldg(rec + REC_QZ * n + e));
+    dst[CR_RTH * stride + l] = Real(__ldg(rec + REC_RTH * n + e));
+    const double r = __ldg(rec + REC_R * n + e);
+    dst[CR_OMR * stride + l] = Real(1.0 - r);
+    dst[CR_R * stride + l] = Real(r);
+}
+
+// the Shakhov parts of a stashed record for one batch
+template <int D, typename Real>
+__device__ __forceinline__ Shk<Real> shk_from(const Real* src, int stride, int l, const RowConst& q, Real ey, Real ez) {
+    Shk<Real> s;
+    s.Ux = src[CR_UX * stride + l];
+    s.invRT = src[CR_INVRT * stride + l];
+    s.qx = src[CR_QX * stride + l];
+    s.RTh = src[CR_RTH * stride + l];
+    s.omr = src[CR_OMR * stride + l];
+    shk_batch<D, Real>(s, src[CR_UY * stride + l], src[CR_UZ * stride + l], src[CR_QY * stride + l],
+                       src[CR_QZ * stride + l], src[CR_R * stride + l], q.Y, q.Z, ey, ez);
+    return s;
+}
+static_assert(static_cast<size_t>(kParts0 - 1) * kS0 * 15 * sizeof(double) <=
+                  3 * static_cast<size_t>(Width<double>::B0) * kSI * sizeof(double),
+              "the cell-moment reduction must fit in the staging arrays");
+static_assert(static_cast<size_t>(kParts0 - 1) * kS0 * 15 * sizeof(double) <=
+                  3 * static_cast<size_t>(Width<float>::B0) * kSI * sizeof(float),
+              "the cell-moment reduction must fit in the staging arrays");
+
+__device__ __forceinline__ void load_dv_tables(const DevMesh& m, double* x1, double* w1) {
+    if (threadIdx.x < m.n1d) {
+        x1[threadIdx.x] = __ldg(m.X1 + threadIdx.x);
+        w1[threadIdx.x] = __ldg(m.W1 + threadIdx.x);
+    }
+}
+
+// ---------------------------------------------------------------------
+// Items
+// ---------------------------------------------------------------------
+// Per-item registers.  la/da: the side reconstructed here (internal items:
+// the owner; tile-boundary items: the side in the tile; boundary items: the
+// owner), lb/db: the neighbour of internal items.
+struct Item {
+    int kind, ptype, la, lb, gi, face, other;
+    double S[3], da[3], db[3];
+};
+
+__device__ __forceinline__ Item load_item(const DevMesh& m, int gi) {
+    Item v;
+    const int meta = __ldg(m.it_meta + gi), loc = __ldg(m.it_loc + gi);
     v.kind = meta & 15;
     v.ptype = meta >> 4;
-    v.lo = loc & 0xffff;
-    v.ln = (loc >> 16) & 0xffff;
-    v.face = __ldg(m.it_face + i);
-    v.xbw = __ldg(m.it_xbw + i);
-    v.xbr = __ldg(m.it_xbr + i);
+    v.gi = gi;
+    v.face = __ldg(m.it_face + gi);
+    v.other = __ldg(m.it_other + gi);
+    const int lo = loc & 0xffff, ln = (loc >> 16) & 0xffff;
     const size_t n = static_cast<size_t>(m.n_items);
+    double dO[3], dN[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        v.S[q] = __ldg(m.it_geo + q * n + i);
-        v.dO[q] = __ldg(m.it_geo + (3 + q) * n + i);
-        v.dN[q] = __ldg(m.it_geo + (6 + q) * n + i);
+        v.S[q] = __ldg(m.it_geo + q * n + gi);
+        dO[q] = __ldg(m.it_geo + (3 + q) * n + gi);
+        dN[q] = __ldg(m.it_geo + (6 + q) * n + gi);
+    }
+    const bool nei_here = v.kind == ITEM_TB_NEI;
+    v.la = nei_here ? ln : lo;
+    v.lb = ln;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        v.da[q] = nei_here ? dN[q] : dO[q];
+        v.db[q] = dN[q];
     }
     return v;
 }
 
-// DV table of a batch (also the barrier that releases the previous batch's
-// shared arrays)
+// reconstruction at the half step from local L0 cell l (fvDVM.C:832-836):
+// gbar+_l + grad_l . v,  v = Cf - C_l - xi dt/2
 template <int D, typename Real, int NB>
-__device__ __forceinline__ int load_batch(const DevMesh& m, int d0, int d1, const Smem<D, Real, NB>& sm) {
-    const int nb = min(NB, d1 - d0);
-    __syncthreads();
-    if (threadIdx.x < nb) {
-        const int d = d0 + threadIdx.x;
-        const double x = __ldg(m.xi + 3 * d), y = __ldg(m.xi + 3 * d + 1), z = __ldg(m.xi + 3 * d + 2);
-        double* p = sm.dv + 5 * threadIdx.x;
-        p[0] = x;
-        p[1] = y;
-        p[2] = z;
-        p[3] = __ldg(m.w + d);
-        p[4] = x * x + y * y + z * z;
-        const int n = m.n1d;
-        int* q = sm.dvi + 4 * threadIdx.x;
-        q[0] = d % n;
-        q[1] = (d / n) % n;
-        q[2] = d / (n * n);
+__device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l, Real vx, Real vy, Real vz, Real& g,
+                                      Real& h) {
+    const Real* Gg = sm.Gg + j * D * kS0 + l;
+    const Real* Gh = sm.Gh + j * D * kS0 + l;
+    Real gg = fma(Gg[0], vx, sm.gB[j * kSL + l]);
+    Real hh = fma(Gh[0], vx, sm.hB[j * kSL + l]);
+    gg = fma(Gg[kS0], vy, gg);
+    hh = fma(Gh[kS0], vy, hh);
+    if (D == 3) {
+        gg = fma(Gg[2 * kS0], vz, gg);
+        hh = fma(Gh[2 * kS0], vz, hh);
     }
-    __syncthreads();
-    return nb;
+    g = gg;
+    h = hh;
 }
 
-// Maxwellian A e_x e_y e_z of entity e (cell or face) at the DV with 1-D
-// indices q[0..2], from the tables the combine kernels write
-template <int D, typename Real>
-__device__ __forceinline__ Real maxwell_tab(const Real* __restrict__ tab, size_t n, int n1d, int e, const int* q) {
-    Real E = __ldg(tab + static_cast<size_t>(q[0]) * n + e) * __ldg(tab + (static_cast<size_t>(n1d) + q[1]) * n + e);
-    if (D == 3) E *= __ldg(tab + (2 * static_cast<size_t>(n1d) + q[2]) * n + e);
-    return E;
-}
-
-template <int D, typename Real, int NB, bool KEEP>
-__device__ __forceinline__ void stage_ghbar(const DevMesh& m, const double* __restrict__ crec,
-                                            const Real* __restrict__ ctab, const Real* __restrict__ g,
-                                            const Real* __restrict__ h, int d0, int nb, const TileRange& t,
-                                            const Smem<D, Real, NB>& sm, Real K3D, Real Kin) {
-    // state rows are loaded LG DVs at a time (LG loads in flight per thread)
-    constexpr int LG = NB < 4 ? NB : 4;
-    for (int l = threadIdx.x; l < t.nloc; l += kThreads) {
-        const int c = __ldg(m.loc_cells + t.loff + l);
-        const Rec<Real> r = load_rec_soa<Real>(crec, m.nC, c);
-        const Real* gr = g + static_cast<size_t>(d0) * m.nC + c;
-        const Real* hr = h + static_cast<size_t>(d0) * m.nC + c;
-#pragma unroll 1
-        for (int b0 = 0; b0 < nb; b0 += LG) {
-            Real gt[LG], ht[LG];
+// ---------------------------------------------------------------------
+// Pass A stages
+// ---------------------------------------------------------------------
+// cp.async of batch bp's inputs of local cell l (thread part `part` of it)
+template <int D, typename Real, int NB>
+__device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
+                                       const Real* __restrict__ g, const Real* __restrict__ h,
+                                       const Real* __restrict__ ctab, int l, int part, int c, bool active) {
+    if (active) {
+        constexpr int H = NB / kPartsL;
+        Real* sg = sm.stg + static_cast<size_t>(buf) * 3 * NB * kSL;
+        const size_t nC = static_cast<size_t>(m.nC);
 #pragma unroll
-            for (int j = 0; j < LG; ++j) {
-                if (b0 + j < nb) {
-                    gt[j] = gr[static_cast<size_t>(b0 + j) * m.nC];
-                    ht[j] = hr[static_cast<size_t>(b0 + j) * m.nC];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < LG; ++j) {
-                const int b = b0 + j;
-                if (b >= nb) continue;
-                const Real xi[3] = {Real(sm.dv[5 * b]), Real(sm.dv[5 * b + 1]), Real(sm.dv[5 * b + 2])};
-                const Real E = maxwell_tab<D, Real>(ctab, m.nC, m.n1d, c, sm.dvi + 4 * b);
-                Real gS, hS;
-                shakhov_m<D, Real>(xi, r, E, K3D, Kin, gS, hS);
-                sm.gB[b * sm.sl + l] = gt[j] + r.r * (gS - gt[j]);
-                sm.hB[b * sm.sl + l] = ht[j] + r.r * (hS - ht[j]);
-                if (KEEP && l < t.n0) {
-                    sm.gT[b * sm.s0 + l] = gt[j];
-                    sm.hT[b * sm.s0 + l] = ht[j];
-                }
+        for (int jj = 0; jj < H; ++jj) {
+            const int j = part * H + jj;
+            if (j < bp.nb) {
+                cp_async(sg + j * kSL + l, g + static_cast<size_t>(bp.d0 + j) * nC + c);
+                cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
+                cp_async(sg + (2 * NB + j) * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
             }
         }
+        Real* syz = sm.stgyz + buf * 2 * kSL;
+        if (part == 0) cp_async(syz + l, ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
+        else if (D == 3) cp_async(syz + kSL + l, ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c);
     }
-    __syncthreads();
+    cp_commit();
+}
+
+template <int D, typename Real, int NB>
+__device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
+                                       int l, int part, bool active, Real K3D, Real c0h) {
+    if (!active) return;
+    Shk<Real> s;
+    s.Ux = sm.crec[CR_UX * kSL + l];
+    s.invRT = sm.crec[CR_INVRT * kSL + l];
+    s.qx = sm.crec[CR_QX * kSL + l];
+    s.RTh = sm.crec[CR_RTH * kSL + l];
+    s.omr = sm.crec[CR_OMR * kSL + l];
+    const Real* syz = sm.stgyz + buf * 2 * kSL;
+    shk_batch<D, Real>(s, sm.crec[CR_UY * kSL + l], sm.crec[CR_UZ * kSL + l], sm.crec[CR_QY * kSL + l],
+                       sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y, q.Z, syz[l],
+                       D == 3 ? syz[kSL + l] : Real(1));
+    const Real* sg = sm.stg + static_cast<size_t>(buf) * 3 * NB * kSL;
+    constexpr int H = NB / kPartsL;
+#pragma unroll
+    for (int jj = 0; jj < H; ++jj) {
+        const int j = part * H + jj;
+        if (j < bp.nb) {
+            const Real x = Real(sm.x1[bp.ix0 + j]);
+            Real go, ho;
+            shk_relax<D, Real>(s, x, sg[(2 * NB + j) * kSL + l], sg[j * kSL + l], sg[(NB + j) * kSL + l], K3D, c0h, go,
+                               ho);
+            sm.gB[j * kSL + l] = go;
+            sm.hB[j * kSL + l] = ho;
+        }
+    }
 }
 
 // Hex cells have at most 6 face neighbours: their stencil stays in
@@ -229,10 +471,10 @@ __device__ __forceinline__ void stage_ghbar(const DevMesh& m, const double* __re
 constexpr int kMaxRegStencil = 6;
 
 template <int D, typename Real, int NB>
-__device__ __forceinline__ void grad_one(const Smem<D, Real, NB>& sm, int b, int l, const int* nbi,
+__device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, int l, const int* nbi,
                                          const Real (*ls)[D], int nk) {
-    const Real* gB = sm.gB + b * sm.sl;
-    const Real* hB = sm.hB + b * sm.sl;
+    const Real* gB = sm.gB + j * kSL;
+    const Real* hB = sm.hB + j * kSL;
     const Real g0 = gB[l], h0 = hB[l];
     Real gx[D], hx[D];
 #pragma unroll
@@ -243,424 +485,534 @@ __device__ __forceinline__ void grad_one(const Smem<D, Real, NB>& sm, int b, int
             const Real dg = gB[nbi[k]] - g0, dh = hB[nbi[k]] - h0;
 #pragma unroll
             for (int q = 0; q < D; ++q) {
-                gx[q] += ls[k][q] * dg;
-                hx[q] += ls[k][q] * dh;
+                gx[q] = fma(ls[k][q], dg, gx[q]);
+                hx[q] = fma(ls[k][q], dh, hx[q]);
             }
         }
     }
 #pragma unroll
     for (int q = 0; q < D; ++q) {
-        sm.Gg[b * sm.sg + q * sm.s0 + l] = gx[q];
-        sm.Gh[b * sm.sg + q * sm.s0 + l] = hx[q];
+        sm.Gg[(j * D + q) * kS0 + l] = gx[q];
+        sm.Gh[(j * D + q) * kS0 + l] = hx[q];
     }
 }
 
 template <int D, typename Real, int NB>
-__device__ __forceinline__ void stage_grad(const DevMesh& m, int nb, const TileRange& t,
-                                           const Smem<D, Real, NB>& sm) {
-    const int l = threadIdx.x % kMaxTile, part = threadIdx.x / kMaxTile;
-    if (l < t.n0) {
-        const int c = t.b + l;
-        if (m.nb_max <= kMaxRegStencil) {
-            int nbi[kMaxRegStencil];
-            Real ls[kMaxRegStencil][D];
-            int nk = 0;
+__device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB>& sm, const BatchPos& bp,
+                                       const TileRange& t) {
+    const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
+    if (l >= t.n0) return;
+    const int c = t.b + l;
+    constexpr int H = (NB + kParts0 - 1) / kParts0;
+    if (m.nb_max <= kMaxRegStencil) {
+        int nbi[kMaxRegStencil];
+        Real ls[kMaxRegStencil][D];
+        int nk = 0;
 #pragma unroll
-            for (int k = 0; k < kMaxRegStencil; ++k) {
-                nbi[k] = l;
+        for (int k = 0; k < kMaxRegStencil; ++k) {
+            nbi[k] = l;
 #pragma unroll
-                for (int q = 0; q < D; ++q) ls[k][q] = Real(0);
-                if (k < m.nb_max) {
-                    const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
-                    if (n >= 0) {
-                        nbi[k] = n;
-                        nk = k + 1;
+            for (int q = 0; q < D; ++q) ls[k][q] = Real(0);
+            if (k < m.nb_max) {
+                const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
+                if (n >= 0) {
+                    nbi[k] = n;
+                    nk = k + 1;
 #pragma unroll
-                        for (int q = 0; q < D; ++q)
-                            ls[k][q] = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
-                    }
+                    for (int q = 0; q < D; ++q)
+                        ls[k][q] = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
                 }
             }
-#pragma unroll 1
-            for (int b = part; b < nb; b += kCellSplit) grad_one<D, Real, NB>(sm, b, l, nbi, ls, nk);
-        } else {
-#pragma unroll 1
-            for (int b = part; b < nb; b += kCellSplit) {
-                const Real* gB = sm.gB + b * sm.sl;
-                const Real* hB = sm.hB + b * sm.sl;
-                const Real g0 = gB[l], h0 = hB[l];
-                Real gx[D], hx[D];
+        }
 #pragma unroll
-                for (int q = 0; q < D; ++q) gx[q] = hx[q] = Real(0);
-                for (int k = 0; k < m.nb_max; ++k) {
-                    const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
-                    if (n < 0) continue;
-                    const Real dg = gB[n] - g0, dh = hB[n] - h0;
+        for (int jj = 0; jj < H; ++jj) {
+            const int j = part + kParts0 * jj;
+            if (j < bp.nb) grad_one<D, Real, NB>(sm, j, l, nbi, ls, nk);
+        }
+    } else {
+#pragma unroll 1
+        for (int jj = 0; jj < H; ++jj) {
+            const int j = part + kParts0 * jj;
+            if (j >= bp.nb) break;
+            const Real* gB = sm.gB + j * kSL;
+            const Real* hB = sm.hB + j * kSL;
+            const Real g0 = gB[l], h0 = hB[l];
+            Real gx[D], hx[D];
 #pragma unroll
-                    for (int q = 0; q < D; ++q) {
-                        const Real lsq = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
-                        gx[q] += lsq * dg;
-                        hx[q] += lsq * dh;
-                    }
-                }
+            for (int q = 0; q < D; ++q) gx[q] = hx[q] = Real(0);
+            for (int k = 0; k < m.nb_max; ++k) {
+                const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
+                if (n < 0) continue;
+                const Real dg = gB[n] - g0, dh = hB[n] - h0;
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
-                    sm.Gg[b * sm.sg + q * sm.s0 + l] = gx[q];
-                    sm.Gh[b * sm.sg + q * sm.s0 + l] = hx[q];
+                    const Real lsq = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
+                    gx[q] = fma(lsq, dg, gx[q]);
+                    hx[q] = fma(lsq, dh, hx[q]);
                 }
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                sm.Gg[(j * D + q) * kS0 + l] = gx[q];
+                sm.Gh[(j * D + q) * kS0 + l] = hx[q];
             }
         }
     }
-    __syncthreads();
-}
-
-// reconstruction at the half step from local cell l (fvDVM.C:832-836):
-// gbar+_l + grad_l . (Cf - C_l - xi dt/2)
-// (the offset d is passed by value: selecting between two arrays by pointer
-// would put the item in local memory)
-template <int D, typename Real, int NB>
-__device__ __forceinline__ void recon(const Smem<D, Real, NB>& sm, int b, int l, double dx, double dy, double dz,
-                                      const Real xi[3], Real hdt, Real& g, Real& h) {
-    const Real v[3] = {Real(dx) - hdt * xi[0], Real(dy) - hdt * xi[1], Real(dz) - hdt * xi[2]};
-    const Real* Gg = sm.Gg + b * sm.sg + l;
-    const Real* Gh = sm.Gh + b * sm.sg + l;
-    Real gg = sm.gB[b * sm.sl + l], hh = sm.hB[b * sm.sl + l];
-#pragma unroll
-    for (int q = 0; q < D; ++q) {
-        gg += Gg[q * sm.s0] * v[q];
-        hh += Gh[q * sm.s0] * v[q];
-    }
-    g = gg;
-    h = hh;
-}
-
-// reconstruction from the side `own` (owner) or not (neighbour) of an item
-template <int D, typename Real, int NB>
-__device__ __forceinline__ void recon_side(const Smem<D, Real, NB>& sm, int b, const ItemSoa& v, bool own,
-                                           const Real xi[3], Real hdt, Real& g, Real& h) {
-    recon<D, Real, NB>(sm, b, own ? v.lo : v.ln, own ? v.dO[0] : v.dN[0], own ? v.dO[1] : v.dN[1],
-                       own ? v.dO[2] : v.dN[2], xi, hdt, g, h);
-}
-
-// reconstruction from the upwind side of an item whose both sides are in
-// L0: the side is selected per DV, the code path is the same for all lanes
-// (the exactly tangential case, both sides averaged, is the only branch)
-template <int D, typename Real, int NB>
-__device__ __forceinline__ void recon_upwind(const Smem<D, Real, NB>& sm, int b, const ItemSoa& v, double xs,
-                                             const Real xi[3], Real hdt, Real& g, Real& h) {
-    const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
-    if (own_up || nei_up) {
-        recon_side<D, Real, NB>(sm, b, v, own_up, xi, hdt, g, h);
-    } else {
-        Real g1, h1, g2, h2;
-        recon_side<D, Real, NB>(sm, b, v, true, xi, hdt, g1, h1);
-        recon_side<D, Real, NB>(sm, b, v, false, xi, hdt, g2, h2);
-        g = Real(0.5) * (g2 + g1);
-        h = Real(0.5) * (h2 + h1);
-    }
 }
 
 // ---------------------------------------------------------------------
-// Pass A: face reconstruction and raw face moments
+// Pass A: face reconstruction, raw face moments, face values
 // ---------------------------------------------------------------------
-template <int D, typename Real, int IPT, int NB>
+template <int D, typename Real, int NB>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem<D, Real, NB> sm = carve<D, Real, NB>(smem_raw, a);
+    const SmemA<D, Real, NB> sm = carve_a<D, Real, NB>(smem_raw);
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
     const Real* ctab = reinterpret_cast<const Real*>(a.ds.ctab);
-    Real* const xbg0 = reinterpret_cast<Real*>(a.ds.xbg[0]);
-    Real* const xbg1 = reinterpret_cast<Real*>(a.ds.xbg[1]);
-    Real* const xbh0 = reinterpret_cast<Real*>(a.ds.xbh[0]);
-    Real* const xbh1 = reinterpret_cast<Real*>(a.ds.xbh[1]);
-    const Real K3D = Real(m.K + 3 - m.D), Kin = Real(m.K);
+    Real* const fvg = reinterpret_cast<Real*>(a.ds.fvg);
+    Real* const fvh = reinterpret_cast<Real*>(a.ds.fvh);
+    const Real K3D = Real(m.K + 3 - m.D), c0h = Real(-(m.D * (m.K + 3 - m.D) + 2 * m.K));
     const Real hdt = Real(0.5 * a.dt);
-    double acc[IPT][15];
-#pragma unroll
-    for (int i = 0; i < IPT; ++i)
-#pragma unroll
-        for (int j = 0; j < 15; ++j) acc[i][j] = 0.0;
+    const size_t nI = static_cast<size_t>(m.n_items);
 
-    for (int d0 = t.d0; d0 < t.d1; d0 += NB) {
-        const int nb = load_batch<D, Real, NB>(m, d0, t.d1, sm);
-        stage_ghbar<D, Real, NB, false>(m, a.ds.cellrec, ctab, g, h, d0, nb, t, sm, K3D, Kin);
-        stage_grad<D, Real, NB>(m, nb, t, sm);
+    // CTA set-up: DV tables, records of the local cells, this thread's cell
+    // of stages 0-1 and its item
+    load_dv_tables(m, sm.x1, sm.w1);
+    const int l1 = threadIdx.x % kSL, p1 = threadIdx.x / kSL;
+    const bool act1 = l1 < t.nloc;
+    const int c1 = act1 ? __ldg(m.loc_cells + t.loff + l1) : 0;
+    if (act1 && p1 == 0) {
+        const double* cr = a.ds.cellrec;
+        const size_t n = static_cast<size_t>(m.nC);
+        sm.crec[CR_UX * kSL + l1] = Real(__ldg(cr + REC_UX * n + c1));
+        sm.crec[CR_UY * kSL + l1] = Real(__ldg(cr + REC_UY * n + c1));
+        sm.crec[CR_UZ * kSL + l1] = Real(__ldg(cr + REC_UZ * n + c1));
+        sm.crec[CR_INVRT * kSL + l1] = Real(__ldg(cr + REC_INVRT * n + c1));
+        sm.crec[CR_QX * kSL + l1] = Real(__ldg(cr + REC_QX * n + c1));
+        sm.crec[CR_QY * kSL + l1] = Real(__ldg(cr + REC_QY * n + c1));
+        sm.crec[CR_QZ * kSL + l1] = Real(__ldg(cr + REC_QZ * n + c1));
+        sm.crec[CR_RTH * kSL + l1] = Real(__ldg(cr + REC_RTH * n + c1));
+        const double r = __ldg(cr + REC_R * n + c1);
+        sm.crec[CR_OMR * kSL + l1] = Real(1.0 - r);
+        sm.crec[CR_R * kSL + l1] = Real(r);
+    }
+    const int it = threadIdx.x;
+    const bool has_item = it < t.nit;
+    Item v{};
+    if (has_item) v = load_item(m, t.ioff + it);
+    double acc[15];
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int it = threadIdx.x + k * kThreads;
-            if (it >= t.nit) continue;
-            const ItemSoa v = load_item_soa(m, t.ioff + it);
-#pragma unroll 1
-            for (int b = 0; b < nb; ++b) {
-                const double xid[3] = {sm.dv[5 * b], sm.dv[5 * b + 1], sm.dv[5 * b + 2]};
-                const double wd = sm.dv[5 * b + 3], xi2 = sm.dv[5 * b + 4];
-                const Real xi[3] = {Real(xid[0]), Real(xid[1]), Real(xid[2])};
-                const double xs = xi_dot_s(xid, v.S);
-                if (v.kind == ITEM_TILE_INTERNAL) {
+    for (int j = 0; j < 15; ++j) acc[j] = 0.0;
+
+    BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
+    const int nbt = (t.r1 - t.r0) * walk.nbr;
+    if (nbt > 0) stage0<D, Real, NB>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+    for (int k = 0; k < nbt; ++k, walk.next()) {
+        const int buf = k & 1;
+        const BatchPos bp = walk.pos();
+        cp_wait_all();
+        __syncthreads();  // batch k staged; the previous batch's stage 3 is done
+        if (k + 1 < nbt) {
+            ahead.next();
+            stage0<D, Real, NB>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+        }
+        const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
+        stage1<D, Real, NB>(sm, buf, bp, q, l1, p1, act1, K3D, c0h);
+        __syncthreads();
+        stage2<D, Real, NB>(m, sm, bp, t);
+        __syncthreads();
+        if (!has_item) continue;
+        // stage 3
+        const double p2 = __dmul_rn(q.Y, v.S[1]);
+        const double p3 = D == 3 ? __dmul_rn(q.Z, v.S[2]) : 0.0;
+        const Real ay = Real(v.da[1]) - hdt * Real(q.Y), az = Real(v.da[2]) - hdt * Real(q.Z);
+        RowSums rs;
+        row_zero(rs);
+        Real* fg = fvg + static_cast<size_t>(bp.d0) * nI + v.gi;
+        Real* fh = fvh + static_cast<size_t>(bp.d0) * nI + v.gi;
+        if (v.kind == ITEM_TILE_INTERNAL) {
+            const Real by = Real(v.db[1]) - hdt * Real(q.Y), bz = Real(v.db[2]) - hdt * Real(q.Z);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if (j < bp.nb) {
+                    const double x = sm.x1[bp.ix0 + j];
+                    const double xs = xs_row(x, v.S[0], p2, p3);
+                    const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
+                    const Real hx = hdt * Real(x);
                     Real gg, hh;
-                    recon_upwind<D, Real, NB>(sm, b, v, xs, xi, hdt, gg, hh);
-                    accum<D>(acc[k], wd, xid, xi2, double(gg), double(hh));
-                } else if (v.kind != ITEM_MESH_BOUNDARY) {
-                    // tile-boundary face: this tile contributes its side only
-                    // (weight 1 upwind, 1/2 tangential, 0 downwind) and hands
-                    // it to the other tile through XB
-                    const bool own_side = v.kind == ITEM_TB_OWN;
-                    const bool up = own_side ? xs >= kVSmall : xs < -kVSmall;
-                    const bool tang = !(xs >= kVSmall) && !(xs < -kVSmall);
-                    const Real cs = up ? Real(1) : (tang ? Real(0.5) : Real(0));
-                    Real g1, h1;
-                    recon_side<D, Real, NB>(sm, b, v, own_side, xi, hdt, g1, h1);
-                    g1 *= cs;
-                    h1 *= cs;
-                    if (up || tang) {
-                        const size_t xi_ = static_cast<size_t>(d0 + b) * m.n_tbf + v.xbw;
-                        (own_side ? xbg0 : xbg1)[xi_] = g1;
-                        (own_side ? xbh0 : xbh1)[xi_] = h1;
+                    if (own_up || nei_up) {
+                        recon<D, Real, NB>(sm, j, own_up ? v.la : v.lb, Real(own_up ? v.da[0] : v.db[0]) - hx,
+                                           own_up ? ay : by, own_up ? az : bz, gg, hh);
+                    } else {
+                        // exactly tangential: both sides averaged (fvDVM.C:847-863)
+                        Real g1, h1, g2, h2;
+                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hx, ay, az, g1, h1);
+                        recon<D, Real, NB>(sm, j, v.lb, Real(v.db[0]) - hx, by, bz, g2, h2);
+                        gg = Real(0.5) * (g2 + g1);
+                        hh = Real(0.5) * (h2 + h1);
                     }
-                    accum<D>(acc[k], wd, xid, xi2, double(g1), double(h1));
-                } else if (xs > 0) {
-                    // outgoing boundary DF: upwind from the owner (fvDVM.C:916-923, :950-961)
+                    row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
+                    fg[j * nI] = gg;
+                    fh[j * nI] = hh;
+                }
+            }
+        } else if (v.kind != ITEM_MESH_BOUNDARY) {
+            // tile-boundary face: this tile's side only, weighted 1 upwind,
+            // 1/2 tangential, 0 downwind; the other tile adds its side.  The
+            // upwind tile writes the face value into both items' slots, so
+            // that pass B reads one slot; tangential halves stay in their
+            // own slots
+            const bool own_side = v.kind == ITEM_TB_OWN;
+            Real* og = fvg + static_cast<size_t>(bp.d0) * nI + v.other;
+            Real* oh = fvh + static_cast<size_t>(bp.d0) * nI + v.other;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if (j < bp.nb) {
+                    const double x = sm.x1[bp.ix0 + j];
+                    const double xs = xs_row(x, v.S[0], p2, p3);
+                    const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
+                    const bool up = own_side ? own_up : nei_up;
+                    const bool tang = !own_up && !nei_up;
+                    const Real cs = up ? Real(1) : (tang ? Real(0.5) : Real(0));
                     Real gg, hh;
-                    recon_side<D, Real, NB>(sm, b, v, true, xi, hdt, gg, hh);
-                    accum<D>(acc[k], wd, xid, xi2, double(gg), double(hh));
-                    if (v.ptype == DUGKS_PATCH_MAXWELL_WALL) acc[k][MOM_OUT] += wd * xs * double(gg);
-                } else if (v.ptype == DUGKS_PATCH_FAR_FIELD) {
-                    // incoming far field: rho_b M(xi; U_owner, T_b) (fvDVM.C:926-938);
-                    // incoming maxwellWall DFs enter through rho_w in the face combine
-                    const BRec* br = a.ds.brec + v.face;
-                    const int own = __ldg(m.bface_owner + v.face);
-                    const double ux = __ldg(a.ds.cellrec + REC_UX * static_cast<size_t>(m.nC) + own);
-                    const double uy = __ldg(a.ds.cellrec + REC_UY * static_cast<size_t>(m.nC) + own);
-                    const double uz = __ldg(a.ds.cellrec + REC_UZ * static_cast<size_t>(m.nC) + own);
-                    const double cx = xid[0] - ux, cy = xid[1] - uy, cz = xid[2] - uz;
-                    const double ge = __ldg(&br->rho_in) * __ldg(&br->K_in) *
-                                      exp(-0.5 * (cx * cx + cy * cy + cz * cz) * __ldg(&br->invRT_in));
-                    const Real gg = Real(ge), hh = Real(ge * __ldg(&br->hfac));
-                    accum<D>(acc[k], wd, xid, xi2, double(gg), double(hh));
+                    recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                    gg *= cs;
+                    hh *= cs;
+                    row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
+                    if (up || tang) {
+                        fg[j * nI] = gg;
+                        fh[j * nI] = hh;
+                    }
+                    if (up) {
+                        og[j * nI] = gg;
+                        oh[j * nI] = hh;
+                    }
+                }
+            }
+        } else {
+            // far-field inflow parameters (read per batch: boundary items are few)
+            const bool wall = v.ptype == DUGKS_PATCH_MAXWELL_WALL;
+            double bK = 0, bInv = 0, bHf = 0, bU[3] = {0, 0, 0};
+            if (!wall) {
+                const BRec* br = a.ds.brec + v.face;
+                const int own = __ldg(m.bface_owner + v.face);
+                const size_t n = static_cast<size_t>(m.nC);
+                bK = __ldg(&br->rho_in) * __ldg(&br->K_in);
+                bInv = __ldg(&br->invRT_in);
+                bHf = __ldg(&br->hfac);
+                for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * n + own);
+            }
+            const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if (j < bp.nb) {
+                    const double x = sm.x1[bp.ix0 + j];
+                    const double xs = xs_row(x, v.S[0], p2, p3);
+                    const double wx = sm.w1[bp.ix0 + j];
+                    if (xs > 0) {
+                        // outgoing: upwind from the owner (fvDVM.C:916-923, :950-961)
+                        Real gg, hh;
+                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                        const double aw = row_add(rs, wx, x, double(gg), double(hh));
+                        if (wall) rs.O = fma(aw, xs, rs.O);
+                        fg[j * nI] = gg;
+                        fh[j * nI] = hh;
+                    } else if (!wall) {
+                        // incoming far field: rho_b M(xi; U_owner, T_b) (fvDVM.C:926-938);
+                        // incoming wall DFs enter through rho_w in the face combine
+                        const double cx = x - bU[0];
+                        const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
+                        row_add(rs, wx, x, double(Real(ge)), double(Real(ge * bHf)));
+                    }
                 }
             }
         }
+        row_fold<D>(acc, rs, q);
     }
-    const size_t base = static_cast<size_t>(blockIdx.y) * m.n_items + t.ioff;
+    if (has_item) {
+        double* p = a.ds.partF + (static_cast<size_t>(blockIdx.y) * m.n_items + v.gi) * kNM;
 #pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        const int it = threadIdx.x + k * kThreads;
-        if (it >= t.nit) continue;
-        double* p = a.ds.partF + (base + it) * kNM;
-#pragma unroll
-        for (int j = 0; j < 15; ++j) p[j] = acc[k][j];
+        for (int j = 0; j < 15; ++j) p[j] = acc[j];
     }
 }
 
 // ---------------------------------------------------------------------
 // Pass B: face relaxation, volume update, raw cell moments
 // ---------------------------------------------------------------------
-template <int D, typename Real, int IPT, int NB>
+// cp.async of an item's own face-value slot and Maxwellian x factors for a
+// batch (each thread stages and later reads only its own item's entries)
+template <typename Real, int NB>
+__device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
+                                            const Real* __restrict__ fvh, const Real* __restrict__ ftab, size_t nI,
+                                            int it, int gi) {
+    const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
+    const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < bp.nb) {
+            cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
+            cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
+            cp_async(sm.st + (2 * NB + j) * kSI + it, ftab + tb + j * nI);
+        }
+    }
+    cp_commit();
+}
+
+// the L0 cell's g~, h~ and Maxwellian x factors of its DVs of a batch, into
+// registers one batch ahead
+template <typename Real, int NB>
+__device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __restrict__ g, const Real* __restrict__ h,
+                                            const Real* __restrict__ ctab, size_t nC, int c, int part, Real* pg,
+                                            Real* ph, Real* pe) {
+    constexpr int H = (NB + kParts0 - 1) / kParts0;
+#pragma unroll
+    for (int jj = 0; jj < H; ++jj) {
+        const int j = part + kParts0 * jj;
+        if (j < bp.nb) {
+            const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
+            pg[jj] = __ldg(g + idx);
+            ph[jj] = __ldg(h + idx);
+            pe[jj] = __ldg(ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
+        }
+    }
+}
+
+template <int D, typename Real, int NB>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem<D, Real, NB> sm = carve<D, Real, NB>(smem_raw, a);
+    const SmemB<Real, NB> sm = carve_b<Real, NB>(smem_raw);
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
     Real* gn = reinterpret_cast<Real*>(a.ds.g[1 - a.ds.cur]);
     Real* hn = reinterpret_cast<Real*>(a.ds.h[1 - a.ds.cur]);
-    const Real* const xbg0 = reinterpret_cast<const Real*>(a.ds.xbg[0]);
-    const Real* const xbg1 = reinterpret_cast<const Real*>(a.ds.xbg[1]);
-    const Real* const xbh0 = reinterpret_cast<const Real*>(a.ds.xbh[0]);
-    const Real* const xbh1 = reinterpret_cast<const Real*>(a.ds.xbh[1]);
+    const Real* fvg = reinterpret_cast<const Real*>(a.ds.fvg);
+    const Real* fvh = reinterpret_cast<const Real*>(a.ds.fvh);
     const Real* ctab = reinterpret_cast<const Real*>(a.ds.ctab);
     const Real* ftab = reinterpret_cast<const Real*>(a.ds.ftab);
-    const Real K3D = Real(m.K + 3 - m.D), Kin = Real(m.K);
-    const Real hdt = Real(0.5 * a.dt);
-    const int lc = threadIdx.x % kMaxTile, part = threadIdx.x / kMaxTile;
+    const Real K3D = Real(m.K + 3 - m.D), c0h = Real(-(m.D * (m.K + 3 - m.D) + 2 * m.K));
+    const size_t nI = static_cast<size_t>(m.n_items), nC = static_cast<size_t>(m.nC);
+    load_dv_tables(m, sm.x1, sm.w1);
+
+    // item of stage 3; its face record (item order) goes to shared memory
+    const int it = threadIdx.x;
+    const bool has_item = it < t.nit;
+    const int gi = t.ioff + (has_item ? it : 0);
+    int kind = 0, other = 0;
+    double S[3] = {0, 0, 0};
+    if (has_item) {
+        kind = __ldg(m.it_meta + gi) & 15;
+        other = __ldg(m.it_other + gi);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) S[q] = __ldg(m.it_geo + q * nI + gi);
+        stash_rec(sm.frec, kSI, it, a.ds.facerec, nI, gi);
+    }
+    // L0 cell of stage 4 (kParts0 threads per cell, DVs interleaved)
+    const int lc = threadIdx.x % kS0, part = threadIdx.x / kS0;
+    const bool has_cell = lc < t.n0;
+    const int c = t.b + (has_cell ? lc : 0);
+    if (has_cell && part == 0) stash_rec(sm.crec, kS0, lc, a.ds.cellrec, nC, c);
+    const Real dtV = has_cell ? Real(a.dt * __ldg(m.dtV + c)) : Real(0);
+    int ent[8];
+    const int nf = m.nf_max < 8 ? m.nf_max : 8;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) ent[s] = (has_cell && s < nf) ? __ldg(m.cf_item + static_cast<size_t>(s) * nC + c) : 0;
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
 
-    for (int d0 = t.d0; d0 < t.d1; d0 += NB) {
-        const int nb = load_batch<D, Real, NB>(m, d0, t.d1, sm);
-        stage_ghbar<D, Real, NB, true>(m, a.ds.cellrec, ctab, g, h, d0, nb, t, sm, K3D, Kin);
-        stage_grad<D, Real, NB>(m, nb, t, sm);
+    constexpr int H = (NB + kParts0 - 1) / kParts0;
+    Real pg[H], ph[H], pe[H];
+    BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
+    const int nbt = (t.r1 - t.r0) * walk.nbr;
+    if (nbt > 0) {
+        if (has_item) stage_items<Real, NB>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
+        if (has_cell) fetch_cells<Real, NB>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
+    }
+    for (int k = 0; k < nbt; ++k, walk.next()) {
+        const BatchPos bp = walk.pos();
+        if (k + 1 < nbt) ahead.next();
+        __syncthreads();  // records stashed; the previous batch's stage 4 is done with the fluxes
+        const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
+        // stage 3: relaxed face DFs and fluxes of the items
+        if (has_item) {
+            const double p2 = __dmul_rn(q.Y, S[1]);
+            const double p3 = D == 3 ? __dmul_rn(q.Z, S[2]) : 0.0;
+            const Real ey = __ldg(ftab + static_cast<size_t>(m.n1d + bp.iy) * nI + gi);
+            const Real ez = D == 3 ? __ldg(ftab + static_cast<size_t>(2 * m.n1d + bp.iz) * nI + gi) : Real(1);
+            const Shk<Real> fs = shk_from<D, Real>(sm.frec, kSI, it, q, ey, ez);
+            cp_wait_all();  // this item's staged entries of batch k
+            const Real* sg = sm.st + it;
+            if (kind != ITEM_MESH_BOUNDARY) {
+                // internal and tile-boundary faces: the staged slot holds the
+                // upwind face value; on an exactly tangential tile-boundary
+                // face it holds this side's half and the other slot the rest
+                const bool tb = kind != ITEM_TILE_INTERNAL;
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int it = threadIdx.x + k * kThreads;
-            if (it >= t.nit) continue;
-            const ItemSoa v = load_item_soa(m, t.ioff + it);
-            const bool boundary = v.kind == ITEM_MESH_BOUNDARY;
-            const int fe = t.ioff + it;  // face records and tables are in item order
-            const Rec<Real> fr = load_rec_soa<Real>(a.ds.facerec, m.n_items, fe);
-#pragma unroll 1
-            for (int b = 0; b < nb; ++b) {
-                const double xid[3] = {sm.dv[5 * b], sm.dv[5 * b + 1], sm.dv[5 * b + 2]};
-                const Real xi[3] = {Real(xid[0]), Real(xid[1]), Real(xid[2])};
-                const double xs = xi_dot_s(xid, v.S);
-                Real gf, hf;
-                if (v.kind == ITEM_TILE_INTERNAL) {
-                    Real gg, hh, gS, hS;
-                    recon_upwind<D, Real, NB>(sm, b, v, xs, xi, hdt, gg, hh);
-                    const Real E = maxwell_tab<D, Real>(ftab, m.n_items, m.n1d, fe, sm.dvi + 4 * b);
-                    shakhov_m<D, Real>(xi, fr, E, K3D, Kin, gS, hS);
-                    gf = gg + fr.r * (gS - gg);
-                    hf = hh + fr.r * (hS - hh);
-                } else if (!boundary) {
-                    // tile-boundary face: this side reconstructed here, the
-                    // other side's contribution from XB (written in pass A)
-                    const bool own_side = v.kind == ITEM_TB_OWN;
-                    const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
-                    const bool here_up = own_side ? own_up : nei_up;
-                    const bool there_up = own_side ? nei_up : own_up;
-                    const bool tang = !own_up && !nei_up;
-                    Real g1, h1;
-                    recon_side<D, Real, NB>(sm, b, v, own_side, xi, hdt, g1, h1);
-                    Real xg = 0, xh = 0;
-                    if (there_up || tang) {
-                        const size_t xr = static_cast<size_t>(d0 + b) * m.n_tbf + v.xbr;
-                        xg = (own_side ? xbg1 : xbg0)[xr];
-                        xh = (own_side ? xbh1 : xbh0)[xr];
+                for (int j = 0; j < NB; ++j) {
+                    if (j < bp.nb) {
+                        const double x = sm.x1[bp.ix0 + j];
+                        const double xs = xs_row(x, S[0], p2, p3);
+                        Real rg = sg[j * kSI], rh = sg[(NB + j) * kSI];
+                        if (tb && !(xs >= kVSmall) && !(xs < -kVSmall)) {
+                            const size_t o = static_cast<size_t>(bp.d0 + j) * nI + other;
+                            rg += __ldg(fvg + o);
+                            rh += __ldg(fvh + o);
+                        }
+                        Real gf, hf;
+                        shk_relax<D, Real>(fs, Real(x), sg[(2 * NB + j) * kSI], rg, rh, K3D, c0h, gf, hf);
+                        sm.Fg[j * kSI + it] = Real(xs) * gf;
+                        sm.Fh[j * kSI + it] = Real(xs) * hf;
                     }
-                    const Real gg = here_up ? g1 : (there_up ? xg : Real(0.5) * g1 + xg);
-                    const Real hh = here_up ? h1 : (there_up ? xh : Real(0.5) * h1 + xh);
-                    Real gS, hS;
-                    const Real E = maxwell_tab<D, Real>(ftab, m.n_items, m.n1d, fe, sm.dvi + 4 * b);
-                    shakhov_m<D, Real>(xi, fr, E, K3D, Kin, gS, hS);
-                    gf = gg + fr.r * (gS - gg);
-                    hf = hh + fr.r * (hS - hh);
-                } else if (xs > 0) {
-                    // outgoing boundary DF: reconstruct and relax with the
-                    // boundary face coefficients; h uses the internal-face T at
-                    // the patch-local index (fvDVM.C:1367, :1413, :1429-1444)
-                    Real gg, hh, gS, hS;
-                    recon_side<D, Real, NB>(sm, b, v, true, xi, hdt, gg, hh);
-                    const Real E = maxwell_tab<D, Real>(ftab, m.n_items, m.n1d, fe, sm.dvi + 4 * b);
-                    shakhov_m<D, Real>(xi, fr, E, K3D, Kin, gS, hS);
-                    gf = gg + fr.r * (gS - gg);
-                    hf = hh + fr.r * (hS - hh);
-                } else {
-                    // incoming, never relaxed: wall rho_w M(U_w,T_w)
-                    // (fvDVM.C:1079-1092), far field rho_b M(U_owner,T_b)
-                    const BRec* br = a.ds.brec + v.face;
-                    double ux, uy, uz;
-                    if (v.ptype == DUGKS_PATCH_FAR_FIELD) {
-                        const int own = __ldg(m.bface_owner + v.face);
-                        ux = __ldg(a.ds.cellrec + REC_UX * static_cast<size_t>(m.nC) + own);
-                        uy = __ldg(a.ds.cellrec + REC_UY * static_cast<size_t>(m.nC) + own);
-                        uz = __ldg(a.ds.cellrec + REC_UZ * static_cast<size_t>(m.nC) + own);
-                    } else {
-                        ux = __ldg(&br->U[0]);
-                        uy = __ldg(&br->U[1]);
-                        uz = __ldg(&br->U[2]);
-                    }
-                    const double cx = xid[0] - ux, cy = xid[1] - uy, cz = xid[2] - uz;
-                    const double ge = br->rho_in * __ldg(&br->K_in) *
-                                      exp(-0.5 * (cx * cx + cy * cy + cz * cz) * __ldg(&br->invRT_in));
-                    gf = Real(ge);
-                    hf = Real(ge * __ldg(&br->hfac));
                 }
-                const Real xsr = Real(xs);
-                sm.Fg[b * sm.si + it] = xsr * gf;
-                sm.Fh[b * sm.si + it] = xsr * hf;
+            } else {
+                // incoming DFs, never relaxed: wall rho_w M(U_w, T_w)
+                // (fvDVM.C:1079-1092), far field rho_b M(U_owner, T_b)
+                // (fvDVM.C:926-938); read per batch, boundary items are few
+                const int face = __ldg(m.it_face + gi);
+                const bool wall = (__ldg(m.it_meta + gi) >> 4) == DUGKS_PATCH_MAXWELL_WALL;
+                const BRec* br = a.ds.brec + face;
+                const double bK = br->rho_in * __ldg(&br->K_in);
+                const double bInv = __ldg(&br->invRT_in), bHf = __ldg(&br->hfac);
+                double bU[3];
+                if (wall) {
+                    for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
+                } else {
+                    const int own = __ldg(m.bface_owner + face);
+                    for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * nC + own);
+                }
+                const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    if (j < bp.nb) {
+                        const double x = sm.x1[bp.ix0 + j];
+                        const double xs = xs_row(x, S[0], p2, p3);
+                        Real gf, hf;
+                        if (xs > 0) {
+                            // outgoing: relaxed with the boundary face's record,
+                            // whose h uses the internal-face T at the patch-local
+                            // index (fvDVM.C:1367, :1413, :1429-1444)
+                            shk_relax<D, Real>(fs, Real(x), sg[(2 * NB + j) * kSI], sg[j * kSI], sg[(NB + j) * kSI],
+                                               K3D, c0h, gf, hf);
+                        } else {
+                            const double cx = x - bU[0];
+                            const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
+                            gf = Real(ge);
+                            hf = Real(ge * bHf);
+                        }
+                        sm.Fg[j * kSI + it] = Real(xs) * gf;
+                        sm.Fh[j * kSI + it] = Real(xs) * hf;
+                    }
+                }
             }
+            // this thread has read its staged entries: stage the next batch
+            if (k + 1 < nbt) stage_items<Real, NB>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
         }
         __syncthreads();
-        // volume update of the L0 cells, two threads per cell with the DVs
-        // split: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f
-        if (lc < t.n0) {
-            const int c = t.b + lc;
-            const Real dtV = Real(a.dt * __ldg(m.dtV + c));
-            int ent[8];
-            const int nf = m.nf_max < 8 ? m.nf_max : 8;
+        // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
+        if (has_cell) {
+            const Real ey = __ldg(ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
+            const Real ez = D == 3 ? __ldg(ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c) : Real(1);
+            const Shk<Real> cs = shk_from<D, Real>(sm.crec, kS0, lc, q, ey, ez);
+            RowSums rs;
+            row_zero(rs);
 #pragma unroll
-            for (int s = 0; s < 8; ++s) ent[s] = s < nf ? __ldg(m.cf_item + static_cast<size_t>(s) * m.nC + c) : 0;
-#pragma unroll 1
-            for (int b = part; b < nb; b += kCellSplit) {
-                const Real* Fg = sm.Fg + b * sm.si;
-                const Real* Fh = sm.Fh + b * sm.si;
-                Real sg = 0, sh = 0;
+            for (int jj = 0; jj < H; ++jj) {
+                const int j = part + kParts0 * jj;
+                if (j < bp.nb) {
+                    const Real gt = pg[jj], ht = ph[jj];
+                    const double x = sm.x1[bp.ix0 + j];
+                    Real gb, hb;
+                    shk_relax<D, Real>(cs, Real(x), pe[jj], gt, ht, K3D, c0h, gb, hb);
+                    const Real* Fg = sm.Fg + j * kSI;
+                    const Real* Fh = sm.Fh + j * kSI;
+                    Real sg = 0, sh = 0;
 #pragma unroll
-                for (int s = 0; s < 8; ++s) {
-                    const int e = ent[s];
-                    if (e != 0) {
-                        const int it = (e > 0 ? e : -e) - 1;
-                        sg += e > 0 ? Fg[it] : -Fg[it];
-                        sh += e > 0 ? Fh[it] : -Fh[it];
+                    for (int s = 0; s < 8; ++s) {
+                        const int e = ent[s];
+                        if (e != 0) {
+                            const int i = (e > 0 ? e : -e) - 1;
+                            sg += e > 0 ? Fg[i] : -Fg[i];
+                            sh += e > 0 ? Fh[i] : -Fh[i];
+                        }
                     }
-                }
-                for (int s = 8; s < m.nf_max; ++s) {
-                    const int e = __ldg(m.cf_item + static_cast<size_t>(s) * m.nC + c);
-                    if (e != 0) {
-                        const int it = (e > 0 ? e : -e) - 1;
-                        sg += e > 0 ? Fg[it] : -Fg[it];
-                        sh += e > 0 ? Fh[it] : -Fh[it];
+                    for (int s = 8; s < m.nf_max; ++s) {
+                        const int e = __ldg(m.cf_item + static_cast<size_t>(s) * nC + c);
+                        if (e != 0) {
+                            const int i = (e > 0 ? e : -e) - 1;
+                            sg += e > 0 ? Fg[i] : -Fg[i];
+                            sh += e > 0 ? Fh[i] : -Fh[i];
+                        }
                     }
+                    const Real g_new = fma(Real(-1.0 / 3), gt, fma(Real(4.0 / 3), gb, sg * dtV));
+                    const Real h_new = fma(Real(-1.0 / 3), ht, fma(Real(4.0 / 3), hb, sh * dtV));
+                    const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
+                    gn[idx] = g_new;
+                    hn[idx] = h_new;
+                    row_add(rs, sm.w1[bp.ix0 + j], x, double(g_new), double(h_new));
                 }
-                const Real g_new =
-                    Real(-1.0 / 3) * sm.gT[b * sm.s0 + lc] + Real(4.0 / 3) * sm.gB[b * sm.sl + lc] + sg * dtV;
-                const Real h_new =
-                    Real(-1.0 / 3) * sm.hT[b * sm.s0 + lc] + Real(4.0 / 3) * sm.hB[b * sm.sl + lc] + sh * dtV;
-                const size_t idx = static_cast<size_t>(d0 + b) * m.nC + c;
-                gn[idx] = g_new;
-                hn[idx] = h_new;
-                const double xid[3] = {sm.dv[5 * b], sm.dv[5 * b + 1], sm.dv[5 * b + 2]};
-                accum<D>(acc, sm.dv[5 * b + 3], xid, sm.dv[5 * b + 4], double(g_new), double(h_new));
             }
+            row_fold<D>(acc, rs, q);
+            // the next batch's cell inputs fly during the barrier and stage 3
+            if (k + 1 < nbt) fetch_cells<Real, NB>(ahead.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
         }
     }
-    // the cell moments of a cell are split over kCellSplit threads: reduce
-    // them through shared memory in a fixed order
+    // the cell moments of a cell are split over kParts0 threads: reduce them
+    // through shared memory in a fixed order
     __syncthreads();
-    double* red = reinterpret_cast<double*>(smem_raw);
-    if (part > 0 && lc < t.n0)
-        for (int j = 0; j < 15; ++j) red[((part - 1) * kMaxTile + lc) * 15 + j] = acc[j];
+    if (part > 0 && has_cell)
+        for (int j = 0; j < 15; ++j) sm.red[((part - 1) * kS0 + lc) * 15 + j] = acc[j];
     __syncthreads();
-    if (part == 0 && lc < t.n0) {
-        for (int p = 1; p < kCellSplit; ++p)
-            for (int j = 0; j < 15; ++j) acc[j] += red[((p - 1) * kMaxTile + lc) * 15 + j];
-        double* dst = a.ds.partC + (static_cast<size_t>(blockIdx.y) * m.nC + t.b + lc) * kNM;
+    if (part == 0 && has_cell) {
+        for (int p = 1; p < kParts0; ++p)
+            for (int j = 0; j < 15; ++j) acc[j] += sm.red[((p - 1) * kS0 + lc) * 15 + j];
+        double* dst = a.ds.partC + (static_cast<size_t>(blockIdx.y) * m.nC + c) * kNM;
 #pragma unroll
         for (int j = 0; j < 15; ++j) dst[j] = acc[j];
     }
 }
 
-template <int D, typename Real, int IPT>
-void launch_pass_t(const StepArgs& a, bool pass_b, cudaStream_t s) {
-    dim3 grid(a.dm.n_tiles, a.chunks);
-    if (!pass_b) k_pass_a<D, Real, IPT, Batch<Real>::A><<<grid, kThreads, a.smemA, s>>>(a);
-    else k_pass_b<D, Real, IPT, Batch<Real>::B><<<grid, kThreads, a.smemB, s>>>(a);
-}
-
+// ---------------------------------------------------------------------
+// launch plumbing
+// ---------------------------------------------------------------------
 template <int D, typename Real>
 cudaError_t launch_pass_d(const StepArgs& a, bool pass_b, cudaStream_t s) {
-    switch (a.ipt) {
-        case 1: launch_pass_t<D, Real, 1>(a, pass_b, s); break;
-        case 2: launch_pass_t<D, Real, 2>(a, pass_b, s); break;
-        case 3: launch_pass_t<D, Real, 3>(a, pass_b, s); break;
-        default: return cudaErrorInvalidConfiguration;
+    const dim3 grid(a.dm.n_tiles, a.chunks);
+    if (!pass_b) {
+        if (a.wideA) k_pass_a<D, Real, Width<Real>::A1><<<grid, kThreads, a.smemA, s>>>(a);
+        else k_pass_a<D, Real, Width<Real>::A0><<<grid, kThreads, a.smemA, s>>>(a);
+    } else {
+        if (a.wideB) k_pass_b<D, Real, Width<Real>::B1><<<grid, kThreads, a.smemB, s>>>(a);
+        else k_pass_b<D, Real, Width<Real>::B0><<<grid, kThreads, a.smemB, s>>>(a);
     }
     return cudaGetLastError();
 }
 
-template <int D, typename Real, int IPT>
-cudaError_t configure_t(size_t smemA, size_t smemB) {
-    cudaError_t e = cudaFuncSetAttribute(k_pass_a<D, Real, IPT, Batch<Real>::A>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemA));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_pass_b<D, Real, IPT, Batch<Real>::B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smemB));
+template <int D, typename Real>
+void smem_d(bool wideA, bool wideB, size_t* smemA, size_t* smemB) {
+    *smemA = wideA ? SmemA<D, Real, Width<Real>::A1>::bytes() : SmemA<D, Real, Width<Real>::A0>::bytes();
+    *smemB = wideB ? SmemB<Real, Width<Real>::B1>::bytes() : SmemB<Real, Width<Real>::B0>::bytes();
 }
 
 template <int D, typename Real>
-cudaError_t configure_d(int ipt, size_t smemA, size_t smemB) {
-    switch (ipt) {
-        case 1: return configure_t<D, Real, 1>(smemA, smemB);
-        case 2: return configure_t<D, Real, 2>(smemA, smemB);
-        case 3: return configure_t<D, Real, 3>(smemA, smemB);
-        default: return cudaErrorInvalidConfiguration;
-    }
+cudaError_t configure_d(bool wideA, bool wideB, size_t smemA, size_t smemB) {
+    cudaError_t e = wideA ? cudaFuncSetAttribute(k_pass_a<D, Real, Width<Real>::A1>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemA))
+                          : cudaFuncSetAttribute(k_pass_a<D, Real, Width<Real>::A0>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemA));
+    if (e != cudaSuccess) return e;
+    return wideB ? cudaFuncSetAttribute(k_pass_b<D, Real, Width<Real>::B1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smemB))
+                 : cudaFuncSetAttribute(k_pass_b<D, Real, Width<Real>::B0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smemB));
 }
+
+// padding of the last batch of a row of n1d DVs at width nb
+int row_waste(int n1d, int nb) { return (n1d + nb - 1) / nb * nb - n1d; }
 
 }  // namespace
 
@@ -670,31 +1022,28 @@ cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStrea
     return a.dm.D == 3 ? launch_pass_d<3, float>(a, pass_b, s) : launch_pass_d<2, float>(a, pass_b, s);
 }
 
-void pass_smem(const DevMesh& dm, int max_local, int max_l0, int max_items, int precision, size_t* smemA,
-               size_t* smemB) {
-    if (precision == DUGKS_FP64) {
-        if (dm.D == 3) {
-            *smemA = smem_bytes<3, double, Batch<double>::A>(max_local, max_l0, max_items, false);
-            *smemB = smem_bytes<3, double, Batch<double>::B>(max_local, max_l0, max_items, true);
-        } else {
-            *smemA = smem_bytes<2, double, Batch<double>::A>(max_local, max_l0, max_items, false);
-            *smemB = smem_bytes<2, double, Batch<double>::B>(max_local, max_l0, max_items, true);
-        }
+void pass_config(int D, int precision, int n1d, int* wideA, int* wideB, size_t* smemA, size_t* smemB) {
+    const bool f64 = precision == DUGKS_FP64;
+    const int a0 = f64 ? Width<double>::A0 : Width<float>::A0, a1 = f64 ? Width<double>::A1 : Width<float>::A1;
+    const int b0 = f64 ? Width<double>::B0 : Width<float>::B0, b1 = f64 ? Width<double>::B1 : Width<float>::B1;
+    // the wide batch unless it pads the rows more than the narrow one
+    *wideA = row_waste(n1d, a1) <= row_waste(n1d, a0) ? 1 : 0;
+    *wideB = row_waste(n1d, b1) <= row_waste(n1d, b0) ? 1 : 0;
+    if (f64) {
+        if (D == 3) smem_d<3, double>(*wideA, *wideB, smemA, smemB);
+        else smem_d<2, double>(*wideA, *wideB, smemA, smemB);
     } else {
-        if (dm.D == 3) {
-            *smemA = smem_bytes<3, float, Batch<float>::A>(max_local, max_l0, max_items, false);
-            *smemB = smem_bytes<3, float, Batch<float>::B>(max_local, max_l0, max_items, true);
-        } else {
-            *smemA = smem_bytes<2, float, Batch<float>::A>(max_local, max_l0, max_items, false);
-            *smemB = smem_bytes<2, float, Batch<float>::B>(max_local, max_l0, max_items, true);
-        }
+        if (D == 3) smem_d<3, float>(*wideA, *wideB, smemA, smemB);
+        else smem_d<2, float>(*wideA, *wideB, smemA, smemB);
     }
 }
 
-cudaError_t configure_kernels(int precision, int D, int ipt, size_t smemA, size_t smemB) {
+cudaError_t configure_kernels(int precision, int D, int wideA, int wideB, size_t smemA, size_t smemB) {
     if (precision == DUGKS_FP64)
-        return D == 3 ? configure_d<3, double>(ipt, smemA, smemB) : configure_d<2, double>(ipt, smemA, smemB);
-    return D == 3 ? configure_d<3, float>(ipt, smemA, smemB) : configure_d<2, float>(ipt, smemA, smemB);
+        return D == 3 ? configure_d<3, double>(wideA, wideB, smemA, smemB)
+                      : configure_d<2, double>(wideA, wideB, smemA, smemB);
+    return D == 3 ? configure_d<3, float>(wideA, wideB, smemA, smemB)
+                  : configure_d<2, float>(wideA, wideB, smemA, smemB);
 }
 
 }  // namespace dugks
