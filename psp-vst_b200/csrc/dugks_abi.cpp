@@ -59,7 +59,7 @@ dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
     a.dt_next = dt_next;
     a.chunks = h->chunks;
     a.chunk_begin = h->d_chunk_begin;
-    dugks::pass_config(h->D, h->precision, h->n1d, &a.wideA, &a.wideB, &a.smemA, &a.smemB);
+    dugks::pass_config(h->D, h->precision, h->n1d, &a);
     return a;
 }
 
@@ -324,7 +324,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     ce = cudaMemset(ds.partF, 0, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM * sizeof(double));
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, cudaGetErrorString(ce));
     dugks::StepArgs a = make_args(h, 0.0, 0.0);
-    ce = dugks::configure_kernels(h->precision, h->D, a.wideA, a.wideB, a.smemA, a.smemB);
+    ce = dugks::configure_kernels(h->precision, a);
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("configure kernels: ") + cudaGetErrorString(ce));
     *out = h;
     return DUGKS_OK;

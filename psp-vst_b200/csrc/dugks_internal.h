@@ -15,7 +15,7 @@ namespace dugks {
 constexpr int kThreads = 512;      // threads per CTA of the two tile passes
 constexpr int kMaxTile = 128;      // cells per tile (L0) at most
 constexpr int kMaxLocal = 256;     // L0 + L1 cells per tile at most
-constexpr int kMaxItems = kThreads;  // items per tile at most (one per thread)
+constexpr int kMaxItems = kThreads - 1;  // items per tile at most (one per thread; one flux slot kept zero)
 constexpr int kMaxN1d = 64;        // DV nodes per dimension at most
 constexpr int kNM = 16;            // stride of a partial-moment record (doubles)
 constexpr double kVSmall = 1.0e-300;  // OpenFOAM VSMALL (upwind switch, fvDVM.C:829-847)

@@ -13,6 +13,7 @@ struct StepArgs {
     const int32_t* chunk_begin;  // [chunks+1] DV rows
     double dt_next;              // time step of the following step (0 = unknown)
     int wideA, wideB;            // batch width of each pass: 1 wide, 0 narrow
+    int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
 };
 
@@ -33,7 +34,7 @@ cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s
 cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s);
 // batch widths and dynamic shared memory of the passes for a DV set of n1d
 // nodes per dimension
-void pass_config(int D, int precision, int n1d, int* wideA, int* wideB, size_t* smemA, size_t* smemB);
-cudaError_t configure_kernels(int precision, int D, int wideA, int wideB, size_t smemA, size_t smemB);
+void pass_config(int D, int precision, int n1d, StepArgs* a);
+cudaError_t configure_kernels(int precision, const StepArgs& a);
 
 }  // namespace dugks

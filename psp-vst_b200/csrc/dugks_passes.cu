@@ -34,9 +34,12 @@ namespace {
 
 constexpr int kSL = kMaxLocal;           // row stride of local-cell arrays in shared memory
 constexpr int kS0 = kMaxTile;            // row stride of L0-cell arrays
-constexpr int kSI = kMaxItems;           // row stride of item arrays
+constexpr int kSI = kMaxItems + 1;       // row stride of item arrays (slot kSI - 1: zero flux)
 constexpr int kPartsL = kThreads / kSL;  // threads per local cell in stages 0-1
 constexpr int kParts0 = kThreads / kS0;  // threads per L0 cell in stages 2 and 4
+// Hex cells have at most 6 face neighbours: such stencils are kept in
+// shared memory for the whole CTA (larger ones are read from global memory)
+constexpr int kMaxRegStencil = 6;
 
 // batch widths: pass A (narrow, wide), pass B (narrow, wide)
 template <typename Real>
@@ -247,9 +250,12 @@ struct SmemA {
     Real* hB;
     Real* Gg;       // [NB][D][kS0] gradients of the L0 cells
     Real* Gh;
+    int* snb;       // [kMaxRegStencil][kS0] gradient stencils of the L0 cells: local neighbour
+    Real* sls;      // [kMaxRegStencil][D][kS0] and least-squares vector
     static constexpr size_t bytes() {
-        return 2 * kMaxN1d * sizeof(double) +
-               (static_cast<size_t>(CR_N) * kSL + 2 * 3 * NB * kSL + 2 * 2 * kSL + 2 * NB * kSL + 2 * NB * D * kS0) *
+        return 2 * kMaxN1d * sizeof(double) + static_cast<size_t>(kMaxRegStencil) * kS0 * sizeof(int) +
+               (static_cast<size_t>(CR_N) * kSL + 2 * 3 * NB * kSL + 2 * 2 * kSL + 2 * NB * kSL + 2 * NB * D * kS0 +
+                static_cast<size_t>(kMaxRegStencil) * D * kS0) *
                    sizeof(Real);
     }
 };
@@ -273,6 +279,10 @@ __device__ __forceinline__ SmemA<D, Real, NB> carve_a(unsigned char* base) {
     s.Gg = p;
     p += NB * D * kS0;
     s.Gh = p;
+    p += NB * D * kS0;
+    s.sls = p;
+    p += kMaxRegStencil * D * kS0;
+    s.snb = reinterpret_cast<int*>(p);
     return s;
 }
 
@@ -412,7 +422,7 @@ __device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l
 // Pass A stages
 // ---------------------------------------------------------------------
 // cp.async of batch bp's inputs of local cell l (thread part `part` of it)
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
                                        const Real* __restrict__ g, const Real* __restrict__ h,
                                        const Real* __restrict__ ctab, int l, int part, int c, bool active) {
@@ -423,7 +433,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 #pragma unroll
         for (int jj = 0; jj < H; ++jj) {
             const int j = part * H + jj;
-            if (j < bp.nb) {
+            if (FULL || j < bp.nb) {
                 cp_async(sg + j * kSL + l, g + static_cast<size_t>(bp.d0 + j) * nC + c);
                 cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
                 cp_async(sg + (2 * NB + j) * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
@@ -436,7 +446,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
     cp_commit();
 }
 
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
                                        int l, int part, bool active, Real K3D, Real c0h) {
     if (!active) return;
@@ -455,7 +465,7 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
 #pragma unroll
     for (int jj = 0; jj < H; ++jj) {
         const int j = part * H + jj;
-        if (j < bp.nb) {
+        if (FULL || j < bp.nb) {
             const Real x = Real(sm.x1[bp.ix0 + j]);
             Real go, ho;
             shk_relax<D, Real>(s, x, sg[(2 * NB + j) * kSL + l], sg[j * kSL + l], sg[(NB + j) * kSL + l], K3D, c0h, go,
@@ -466,9 +476,6 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
     }
 }
 
-// Hex cells have at most 6 face neighbours: their stencil stays in
-// registers while the thread walks its DVs of the batch
-constexpr int kMaxRegStencil = 6;
 
 template <int D, typename Real, int NB>
 __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, int l, const int* nbi,
@@ -497,7 +504,7 @@ __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, in
     }
 }
 
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB>& sm, const BatchPos& bp,
                                        const TileRange& t) {
     const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
@@ -505,35 +512,26 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
     const int c = t.b + l;
     constexpr int H = (NB + kParts0 - 1) / kParts0;
     if (m.nb_max <= kMaxRegStencil) {
+        // stencil from shared memory (absent neighbours: the cell itself
+        // with a zero vector)
         int nbi[kMaxRegStencil];
         Real ls[kMaxRegStencil][D];
-        int nk = 0;
 #pragma unroll
         for (int k = 0; k < kMaxRegStencil; ++k) {
-            nbi[k] = l;
+            nbi[k] = sm.snb[k * kS0 + l];
 #pragma unroll
-            for (int q = 0; q < D; ++q) ls[k][q] = Real(0);
-            if (k < m.nb_max) {
-                const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
-                if (n >= 0) {
-                    nbi[k] = n;
-                    nk = k + 1;
-#pragma unroll
-                    for (int q = 0; q < D; ++q)
-                        ls[k][q] = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
-                }
-            }
+            for (int q = 0; q < D; ++q) ls[k][q] = sm.sls[(k * D + q) * kS0 + l];
         }
 #pragma unroll
         for (int jj = 0; jj < H; ++jj) {
             const int j = part + kParts0 * jj;
-            if (j < bp.nb) grad_one<D, Real, NB>(sm, j, l, nbi, ls, nk);
+            if (FULL || j < bp.nb) grad_one<D, Real, NB>(sm, j, l, nbi, ls, kMaxRegStencil);
         }
     } else {
 #pragma unroll 1
         for (int jj = 0; jj < H; ++jj) {
             const int j = part + kParts0 * jj;
-            if (j >= bp.nb) break;
+            if (!FULL && j >= bp.nb) break;
             const Real* gB = sm.gB + j * kSL;
             const Real* hB = sm.hB + j * kSL;
             const Real g0 = gB[l], h0 = hB[l];
@@ -563,7 +561,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
 // ---------------------------------------------------------------------
 // Pass A: face reconstruction, raw face moments, face values
 // ---------------------------------------------------------------------
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool FULL>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -599,6 +597,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         sm.crec[CR_OMR * kSL + l1] = Real(1.0 - r);
         sm.crec[CR_R * kSL + l1] = Real(r);
     }
+    // gradient stencils of the L0 cells (slot-major tables, -1: none)
+    if (threadIdx.x < kS0 && m.nb_max <= kMaxRegStencil) {
+        const int l = threadIdx.x;
+        const int c = t.b + l;
+#pragma unroll
+        for (int k = 0; k < kMaxRegStencil; ++k) {
+            const int n = (l < t.n0 && k < m.nb_max) ? __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c) : -1;
+            sm.snb[k * kS0 + l] = n >= 0 ? n : l;
+#pragma unroll
+            for (int q = 0; q < D; ++q)
+                sm.sls[(k * D + q) * kS0 + l] =
+                    n >= 0 ? Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c)) : Real(0);
+        }
+    }
     const int it = threadIdx.x;
     const bool has_item = it < t.nit;
     Item v{};
@@ -609,7 +621,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 
     BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
-    if (nbt > 0) stage0<D, Real, NB>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+    if (nbt > 0) stage0<D, Real, NB, FULL>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const int buf = k & 1;
         const BatchPos bp = walk.pos();
@@ -617,12 +629,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         __syncthreads();  // batch k staged; the previous batch's stage 3 is done
         if (k + 1 < nbt) {
             ahead.next();
-            stage0<D, Real, NB>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+            stage0<D, Real, NB, FULL>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
         }
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
-        stage1<D, Real, NB>(sm, buf, bp, q, l1, p1, act1, K3D, c0h);
+        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h);
         __syncthreads();
-        stage2<D, Real, NB>(m, sm, bp, t);
+        stage2<D, Real, NB, FULL>(m, sm, bp, t);
         __syncthreads();
         if (!has_item) continue;
         // stage 3
@@ -637,7 +649,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
             const Real by = Real(v.db[1]) - hdt * Real(q.Y), bz = Real(v.db[2]) - hdt * Real(q.Z);
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
-                if (j < bp.nb) {
+                if (FULL || j < bp.nb) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
@@ -670,7 +682,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
             Real* oh = fvh + static_cast<size_t>(bp.d0) * nI + v.other;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
-                if (j < bp.nb) {
+                if (FULL || j < bp.nb) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
@@ -708,7 +720,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
             const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
-                if (j < bp.nb) {
+                if (FULL || j < bp.nb) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const double wx = sm.w1[bp.ix0 + j];
@@ -742,9 +754,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 // ---------------------------------------------------------------------
 // Pass B: face relaxation, volume update, raw cell moments
 // ---------------------------------------------------------------------
+// faces of a cell whose flux list stays in registers (hex cells have 6)
+constexpr int kRegFaces = 6;
+
+// v with its sign flipped when neg is 1
+__device__ __forceinline__ double flip_sign(double v, unsigned neg) {
+    return __hiloint2double(__double2hiint(v) ^ static_cast<int>(neg << 31), __double2loint(v));
+}
+__device__ __forceinline__ float flip_sign(float v, unsigned neg) {
+    return __int_as_float(__float_as_int(v) ^ static_cast<int>(neg << 31));
+}
+
 // cp.async of an item's own face-value slot and Maxwellian x factors for a
 // batch (each thread stages and later reads only its own item's entries)
-template <typename Real, int NB>
+template <typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
                                             const Real* __restrict__ fvh, const Real* __restrict__ ftab, size_t nI,
                                             int it, int gi) {
@@ -752,7 +775,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
     const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        if (j < bp.nb) {
+        if (FULL || j < bp.nb) {
             cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
             cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
             cp_async(sm.st + (2 * NB + j) * kSI + it, ftab + tb + j * nI);
@@ -763,7 +786,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
 
 // the L0 cell's g~, h~ and Maxwellian x factors of its DVs of a batch, into
 // registers one batch ahead
-template <typename Real, int NB>
+template <typename Real, int NB, bool FULL>
 __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __restrict__ g, const Real* __restrict__ h,
                                             const Real* __restrict__ ctab, size_t nC, int c, int part, Real* pg,
                                             Real* ph, Real* pe) {
@@ -771,7 +794,7 @@ __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __re
 #pragma unroll
     for (int jj = 0; jj < H; ++jj) {
         const int j = part + kParts0 * jj;
-        if (j < bp.nb) {
+        if (FULL || j < bp.nb) {
             const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
             pg[jj] = __ldg(g + idx);
             ph[jj] = __ldg(h + idx);
@@ -780,7 +803,7 @@ __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __re
     }
 }
 
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool FULL>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -817,10 +840,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const int c = t.b + (has_cell ? lc : 0);
     if (has_cell && part == 0) stash_rec(sm.crec, kS0, lc, a.ds.cellrec, nC, c);
     const Real dtV = has_cell ? Real(a.dt * __ldg(m.dtV + c)) : Real(0);
-    int ent[8];
-    const int nf = m.nf_max < 8 ? m.nf_max : 8;
+    // flux list of the cell: item slot and sign (owner side: outflow, negated
+    // by flipping the sign bit); absent entries read the zero slot kSI - 1,
+    // which no item uses
+    int ent_off[kRegFaces];
+    unsigned ent_neg[kRegFaces];
 #pragma unroll
-    for (int s = 0; s < 8; ++s) ent[s] = (has_cell && s < nf) ? __ldg(m.cf_item + static_cast<size_t>(s) * nC + c) : 0;
+    for (int s = 0; s < kRegFaces; ++s) {
+        const int e = (has_cell && s < m.nf_max) ? __ldg(m.cf_item + static_cast<size_t>(s) * nC + c) : 0;
+        ent_off[s] = e == 0 ? kSI - 1 : (e > 0 ? e : -e) - 1;
+        ent_neg[s] = e < 0 ? 1u : 0u;
+    }
+    if (threadIdx.x == kThreads - 1) {
+        for (int j = 0; j < NB; ++j) {
+            sm.Fg[j * kSI + kSI - 1] = Real(0);
+            sm.Fh[j * kSI + kSI - 1] = Real(0);
+        }
+    }
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
@@ -830,8 +866,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
-        if (has_item) stage_items<Real, NB>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
-        if (has_cell) fetch_cells<Real, NB>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
+        if (has_item) stage_items<Real, NB, FULL>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
+        if (has_cell) fetch_cells<Real, NB, FULL>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
     }
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const BatchPos bp = walk.pos();
@@ -854,7 +890,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 const bool tb = kind != ITEM_TILE_INTERNAL;
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
-                    if (j < bp.nb) {
+                    if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
                         Real rg = sg[j * kSI], rh = sg[(NB + j) * kSI];
@@ -888,7 +924,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
-                    if (j < bp.nb) {
+                    if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
                         Real gf, hf;
@@ -910,7 +946,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 }
             }
             // this thread has read its staged entries: stage the next batch
-            if (k + 1 < nbt) stage_items<Real, NB>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
+            if (k + 1 < nbt) stage_items<Real, NB, FULL>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
         }
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
@@ -923,7 +959,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
 #pragma unroll
             for (int jj = 0; jj < H; ++jj) {
                 const int j = part + kParts0 * jj;
-                if (j < bp.nb) {
+                if (FULL || j < bp.nb) {
                     const Real gt = pg[jj], ht = ph[jj];
                     const double x = sm.x1[bp.ix0 + j];
                     Real gb, hb;
@@ -932,15 +968,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     const Real* Fh = sm.Fh + j * kSI;
                     Real sg = 0, sh = 0;
 #pragma unroll
-                    for (int s = 0; s < 8; ++s) {
-                        const int e = ent[s];
-                        if (e != 0) {
-                            const int i = (e > 0 ? e : -e) - 1;
-                            sg += e > 0 ? Fg[i] : -Fg[i];
-                            sh += e > 0 ? Fh[i] : -Fh[i];
-                        }
+                    for (int s = 0; s < kRegFaces; ++s) {
+                        sg += flip_sign(Fg[ent_off[s]], ent_neg[s]);
+                        sh += flip_sign(Fh[ent_off[s]], ent_neg[s]);
                     }
-                    for (int s = 8; s < m.nf_max; ++s) {
+                    for (int s = kRegFaces; s < m.nf_max; ++s) {
                         const int e = __ldg(m.cf_item + static_cast<size_t>(s) * nC + c);
                         if (e != 0) {
                             const int i = (e > 0 ? e : -e) - 1;
@@ -958,7 +990,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             }
             row_fold<D>(acc, rs, q);
             // the next batch's cell inputs fly during the barrier and stage 3
-            if (k + 1 < nbt) fetch_cells<Real, NB>(ahead.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
+            if (k + 1 < nbt) fetch_cells<Real, NB, FULL>(ahead.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
         }
     }
     // the cell moments of a cell are split over kParts0 threads: reduce them
@@ -979,17 +1011,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
 // ---------------------------------------------------------------------
 // launch plumbing
 // ---------------------------------------------------------------------
-template <int D, typename Real>
-cudaError_t launch_pass_d(const StepArgs& a, bool pass_b, cudaStream_t s) {
+template <int D, typename Real, int NA, int NBB>
+cudaError_t launch_nb(const StepArgs& a, bool pass_b, cudaStream_t s) {
     const dim3 grid(a.dm.n_tiles, a.chunks);
     if (!pass_b) {
-        if (a.wideA) k_pass_a<D, Real, Width<Real>::A1><<<grid, kThreads, a.smemA, s>>>(a);
-        else k_pass_a<D, Real, Width<Real>::A0><<<grid, kThreads, a.smemA, s>>>(a);
+        if (a.fullA) k_pass_a<D, Real, NA, true><<<grid, kThreads, a.smemA, s>>>(a);
+        else k_pass_a<D, Real, NA, false><<<grid, kThreads, a.smemA, s>>>(a);
     } else {
-        if (a.wideB) k_pass_b<D, Real, Width<Real>::B1><<<grid, kThreads, a.smemB, s>>>(a);
-        else k_pass_b<D, Real, Width<Real>::B0><<<grid, kThreads, a.smemB, s>>>(a);
+        if (a.fullB) k_pass_b<D, Real, NBB, true><<<grid, kThreads, a.smemB, s>>>(a);
+        else k_pass_b<D, Real, NBB, false><<<grid, kThreads, a.smemB, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+template <int D, typename Real>
+cudaError_t launch_pass_d(const StepArgs& a, bool pass_b, cudaStream_t s) {
+    using W = Width<Real>;
+    if (!pass_b) return a.wideA ? launch_nb<D, Real, W::A1, W::B0>(a, false, s) : launch_nb<D, Real, W::A0, W::B0>(a, false, s);
+    return a.wideB ? launch_nb<D, Real, W::A0, W::B1>(a, true, s) : launch_nb<D, Real, W::A0, W::B0>(a, true, s);
 }
 
 template <int D, typename Real>
@@ -998,17 +1037,23 @@ void smem_d(bool wideA, bool wideB, size_t* smemA, size_t* smemB) {
     *smemB = wideB ? SmemB<Real, Width<Real>::B1>::bytes() : SmemB<Real, Width<Real>::B0>::bytes();
 }
 
+template <typename K>
+cudaError_t set_smem(K* kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
+template <int D, typename Real, int NA, int NBB>
+cudaError_t configure_nb(const StepArgs& a, bool pass_b) {
+    if (!pass_b) return a.fullA ? set_smem(k_pass_a<D, Real, NA, true>, a.smemA) : set_smem(k_pass_a<D, Real, NA, false>, a.smemA);
+    return a.fullB ? set_smem(k_pass_b<D, Real, NBB, true>, a.smemB) : set_smem(k_pass_b<D, Real, NBB, false>, a.smemB);
+}
+
 template <int D, typename Real>
-cudaError_t configure_d(bool wideA, bool wideB, size_t smemA, size_t smemB) {
-    cudaError_t e = wideA ? cudaFuncSetAttribute(k_pass_a<D, Real, Width<Real>::A1>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemA))
-                          : cudaFuncSetAttribute(k_pass_a<D, Real, Width<Real>::A0>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemA));
+cudaError_t configure_d(const StepArgs& a) {
+    using W = Width<Real>;
+    cudaError_t e = a.wideA ? configure_nb<D, Real, W::A1, W::B0>(a, false) : configure_nb<D, Real, W::A0, W::B0>(a, false);
     if (e != cudaSuccess) return e;
-    return wideB ? cudaFuncSetAttribute(k_pass_b<D, Real, Width<Real>::B1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smemB))
-                 : cudaFuncSetAttribute(k_pass_b<D, Real, Width<Real>::B0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smemB));
+    return a.wideB ? configure_nb<D, Real, W::A0, W::B1>(a, true) : configure_nb<D, Real, W::A0, W::B0>(a, true);
 }
 
 // padding of the last batch of a row of n1d DVs at width nb
@@ -1022,28 +1067,28 @@ cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStrea
     return a.dm.D == 3 ? launch_pass_d<3, float>(a, pass_b, s) : launch_pass_d<2, float>(a, pass_b, s);
 }
 
-void pass_config(int D, int precision, int n1d, int* wideA, int* wideB, size_t* smemA, size_t* smemB) {
+void pass_config(int D, int precision, int n1d, StepArgs* a) {
     const bool f64 = precision == DUGKS_FP64;
     const int a0 = f64 ? Width<double>::A0 : Width<float>::A0, a1 = f64 ? Width<double>::A1 : Width<float>::A1;
     const int b0 = f64 ? Width<double>::B0 : Width<float>::B0, b1 = f64 ? Width<double>::B1 : Width<float>::B1;
-    // the wide batch unless it pads the rows more than the narrow one
-    *wideA = row_waste(n1d, a1) <= row_waste(n1d, a0) ? 1 : 0;
-    *wideB = row_waste(n1d, b1) <= row_waste(n1d, b0) ? 1 : 0;
+    // the wide batch unless it pads the rows more than the narrow one;
+    // rows that split into whole batches take the unguarded kernels
+    a->wideA = row_waste(n1d, a1) <= row_waste(n1d, a0) ? 1 : 0;
+    a->wideB = row_waste(n1d, b1) <= row_waste(n1d, b0) ? 1 : 0;
+    a->fullA = row_waste(n1d, a->wideA ? a1 : a0) == 0 ? 1 : 0;
+    a->fullB = row_waste(n1d, a->wideB ? b1 : b0) == 0 ? 1 : 0;
     if (f64) {
-        if (D == 3) smem_d<3, double>(*wideA, *wideB, smemA, smemB);
-        else smem_d<2, double>(*wideA, *wideB, smemA, smemB);
+        if (D == 3) smem_d<3, double>(a->wideA, a->wideB, &a->smemA, &a->smemB);
+        else smem_d<2, double>(a->wideA, a->wideB, &a->smemA, &a->smemB);
     } else {
-        if (D == 3) smem_d<3, float>(*wideA, *wideB, smemA, smemB);
-        else smem_d<2, float>(*wideA, *wideB, smemA, smemB);
+        if (D == 3) smem_d<3, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
+        else smem_d<2, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
     }
 }
 
-cudaError_t configure_kernels(int precision, int D, int wideA, int wideB, size_t smemA, size_t smemB) {
-    if (precision == DUGKS_FP64)
-        return D == 3 ? configure_d<3, double>(wideA, wideB, smemA, smemB)
-                      : configure_d<2, double>(wideA, wideB, smemA, smemB);
-    return D == 3 ? configure_d<3, float>(wideA, wideB, smemA, smemB)
-                  : configure_d<2, float>(wideA, wideB, smemA, smemB);
+cudaError_t configure_kernels(int precision, const StepArgs& a) {
+    if (precision == DUGKS_FP64) return a.dm.D == 3 ? configure_d<3, double>(a) : configure_d<2, double>(a);
+    return a.dm.D == 3 ? configure_d<3, float>(a) : configure_d<2, float>(a);
 }
 
 }  // namespace dugks
