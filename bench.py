@@ -180,6 +180,23 @@ def cpu_baseline(case_name: str, n1d: int, steps: int, warmup: int):
                       f"{steps} steps after {warmup} warm-up, OpenMP over DVs/faces/cells ({cores} threads)"}
 
 
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The largest x over all ranks of the default process group (x itself
+    without one): multi-GPU times are the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, cells: int, dvs: int, steps: int, seconds: float) -> float:
+    """Whole-job cell.DV updates/s of `world` replicas that each advanced
+    cells x dvs pairs `steps` times, timed by the slowest rank."""
+    return world * cells * dvs * steps / seconds
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -222,13 +239,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # warm-up
     solver.step(W, case.dt)
     barrier()
@@ -243,8 +253,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop() if sampler else None
-    t_ms = max_over_ranks(float(stage[4]))
-    value = world * nc * nv * K / (t_ms / 1e3)
+    t_ms = max_over_ranks(float(stage[4]), dist)
+    value = replica_rate(world, nc, nv, K, t_ms / 1e3)
 
     # end to end through the public API with host buffers: each step is
     # fvDVM::evolution (dt passed by value) followed by the copy of the
@@ -254,8 +264,8 @@ def main():
     for _ in range(K):
         solver.step(1, case.dt)
         solver.macros()
-    te = max_over_ranks(time.perf_counter() - te0)
-    e2e = world * nc * nv * K / te
+    te = max_over_ranks(time.perf_counter() - te0, dist)
+    e2e = replica_rate(world, nc, nv, K, te)
 
     rs = 8 if prec == dl.FP64 else 4
     peak, peak_kind = measured_peaks()
