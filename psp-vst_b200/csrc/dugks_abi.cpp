@@ -309,9 +309,8 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.cellrec, static_cast<size_t>(dugks::REC_N) * nC)) ||
         (st = dev_alloc(h, &ds.facerec, static_cast<size_t>(dugks::REC_N) * dm.n_items)) ||
-        (st = dev_alloc(h, &p, static_cast<size_t>(h->D) * h->n1d * nC * rs)) ||
-        ((ds.ctab = p), (st = dev_alloc(h, &p, static_cast<size_t>(h->D) * h->n1d * dm.n_items * rs))) ||
-        ((ds.ftab = p), false) ||
+        (st = dev_alloc(h, &ds.ctab, static_cast<size_t>(h->D) * h->n1d * nC)) ||
+        (st = dev_alloc(h, &ds.ftab, static_cast<size_t>(h->D) * h->n1d * dm.n_items)) ||
         (st = dev_alloc(h, &ds.brec, nBF)) || (st = dev_alloc(h, &ds.bmom_in, static_cast<size_t>(nBF) * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.cm, static_cast<size_t>(nC) * 9)) ||
         (st = dev_alloc(h, &ds.fm, static_cast<size_t>(nF) * 9)) || (st = dev_alloc(h, &ds.co, 2)) ||

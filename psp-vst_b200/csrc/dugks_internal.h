@@ -120,11 +120,13 @@ struct DevState {
     // face records in item order (each face's record is written to its one
     // or two items, so that a tile reads its faces' records contiguously)
     double* facerec;   // [REC_N][n_items]
-    // one-dimensional Maxwellian factors (Real): table k of entity e at node i
-    // is tab[(k * n1d + i) * n + e] = exp(-(X_i - U_k)^2 / (2 R T)), the x
-    // table multiplied by A = rho (2 pi R T)^(-D/2)
-    void* ctab;        // [D][n1d][nC]
-    void* ftab;        // [D][n1d][n_items]  (item order, as facerec)
+    // one-dimensional Maxwellian factors, FP64 for both precisions (the
+    // equilibrium and the relaxation are evaluated in FP64, so that the FP32
+    // path injects no rounding bias into the conserved moments): table k of
+    // entity e at node i is tab[(k * n1d + i) * n + e] = exp(-(X_i - U_k)^2 /
+    // (2 R T)), the x table multiplied by A = rho (2 pi R T)^(-D/2)
+    double* ctab;      // [D][n1d][nC]
+    double* ftab;      // [D][n1d][n_items]  (item order, as facerec)
     BRec* brec;        // [nBF]
     double* bmom_in;   // [nBF][kNM] incoming wall moments per unit rho_w
     double* cm;        // cell macros [nC][9]: rho U(3) T q(3) tau (renumbered)

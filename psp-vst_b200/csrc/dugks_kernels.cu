@@ -37,7 +37,7 @@ __device__ __forceinline__ void sum_face_partials(const StepArgs& a, int f, doub
 
 // one-dimensional Maxwellian factors of one cell or face (layout in
 // dugks_internal.h): D * n1d exponentials instead of one per DV
-__device__ __forceinline__ void write_maxwell_tables(const DevMesh& m, void* tab, size_t n, int e, const double U[3],
+__device__ __forceinline__ void write_maxwell_tables(const DevMesh& m, double* tab, size_t n, int e, const double U[3],
                                                      double invRT, double A) {
     for (int k = 0; k < m.D; ++k)
         for (int i = 0; i < m.n1d; ++i) {
@@ -45,8 +45,7 @@ __device__ __forceinline__ void write_maxwell_tables(const DevMesh& m, void* tab
             double v = exp(-0.5 * x * x * invRT);
             if (k == 0) v *= A;
             const size_t idx = (static_cast<size_t>(k) * m.n1d + i) * n + e;
-            if (m.prec == DUGKS_FP64) static_cast<double*>(tab)[idx] = v;
-            else static_cast<float*>(tab)[idx] = static_cast<float>(v);
+            tab[idx] = v;
         }
 }
 

@@ -50,7 +50,7 @@ struct Width<double> {
 };
 template <>
 struct Width<float> {
-    static constexpr int A0 = 8, A1 = 16, B0 = 8, B1 = 16;
+    static constexpr int A0 = 8, A1 = 8, B0 = 8, B1 = 8;
 };
 
 // ---------------------------------------------------------------------
@@ -243,9 +243,10 @@ template <int D, typename Real, int NB>
 struct SmemA {
     double* x1;     // [kMaxN1d] 1-D nodes
     double* w1;     // [kMaxN1d] 1-D weights
-    Real* crec;     // [CR_N][kSL] records of the local cells
-    Real* stg;      // [2][3][NB][kSL] staged g~, h~, e_x (double buffer)
-    Real* stgyz;    // [2][2][kSL] staged e_y, e_z
+    double* crec;   // [CR_N][kSL] records of the local cells
+    double* stgx;   // [2][NB][kSL] staged e_x (double buffer)
+    double* stgyz;  // [2][2][kSL] staged e_y, e_z
+    Real* stg;      // [2][2][NB][kSL] staged g~, h~
     Real* gB;       // [NB][kSL] gbar+
     Real* hB;
     Real* Gg;       // [NB][D][kS0] gradients of the L0 cells
@@ -254,7 +255,8 @@ struct SmemA {
     Real* sls;      // [kMaxRegStencil][D][kS0] and least-squares vector
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) + static_cast<size_t>(kMaxRegStencil) * kS0 * sizeof(int) +
-               (static_cast<size_t>(CR_N) * kSL + 2 * 3 * NB * kSL + 2 * 2 * kSL + 2 * NB * kSL + 2 * NB * D * kS0 +
+               (static_cast<size_t>(CR_N) * kSL + 2 * NB * kSL + 2 * 2 * kSL) * sizeof(double) +
+               (2 * 2 * static_cast<size_t>(NB) * kSL + 2 * NB * kSL + 2 * NB * D * kS0 +
                 static_cast<size_t>(kMaxRegStencil) * D * kS0) *
                    sizeof(Real);
     }
@@ -265,13 +267,12 @@ __device__ __forceinline__ SmemA<D, Real, NB> carve_a(unsigned char* base) {
     SmemA<D, Real, NB> s;
     s.x1 = reinterpret_cast<double*>(base);
     s.w1 = s.x1 + kMaxN1d;
-    Real* p = reinterpret_cast<Real*>(s.w1 + kMaxN1d);
-    s.crec = p;
-    p += CR_N * kSL;
+    s.crec = s.w1 + kMaxN1d;
+    s.stgx = s.crec + CR_N * kSL;
+    s.stgyz = s.stgx + 2 * NB * kSL;
+    Real* p = reinterpret_cast<Real*>(s.stgyz + 2 * 2 * kSL);
     s.stg = p;
-    p += 2 * 3 * NB * kSL;
-    s.stgyz = p;
-    p += 2 * 2 * kSL;
+    p += 2 * 2 * NB * kSL;
     s.gB = p;
     p += NB * kSL;
     s.hB = p;
@@ -290,15 +291,17 @@ template <typename Real, int NB>
 struct SmemB {
     double* x1;
     double* w1;
-    Real* Fg;     // [NB][kSI] fluxes xi.S g_f of the items
+    double* frec;  // [CR_N][kSI] face records of the items
+    double* crec;  // [CR_N][kS0] records of the L0 cells
+    double* stx;   // [NB][kSI] staged e_x of the items
+    Real* st;      // [2][NB][kSI] staged face values g, h of the items
+    Real* Fg;      // [NB][kSI] fluxes xi.S g_f of the items
     Real* Fh;
-    Real* frec;   // [CR_N][kSI] face records of the items
-    Real* crec;   // [CR_N][kS0] records of the L0 cells
-    Real* st;     // [3][NB][kSI] staged face values g, h and e_x of the items
-    double* red;  // end-of-CTA reduction of the split cell moments (aliases st)
+    double* red;   // end-of-CTA reduction of the split cell moments (aliases stx and st)
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) +
-               (5 * static_cast<size_t>(NB) * kSI + static_cast<size_t>(CR_N) * (kSI + kS0)) * sizeof(Real);
+               (static_cast<size_t>(CR_N) * (kSI + kS0) + static_cast<size_t>(NB) * kSI) * sizeof(double) +
+               4 * static_cast<size_t>(NB) * kSI * sizeof(Real);
     }
 };
 
@@ -307,12 +310,13 @@ __device__ __forceinline__ SmemB<Real, NB> carve_b(unsigned char* base) {
     SmemB<Real, NB> s;
     s.x1 = reinterpret_cast<double*>(base);
     s.w1 = s.x1 + kMaxN1d;
-    s.Fg = reinterpret_cast<Real*>(s.w1 + kMaxN1d);
-    s.Fh = s.Fg + NB * kSI;
-    s.frec = s.Fh + NB * kSI;
+    s.frec = s.w1 + kMaxN1d;
     s.crec = s.frec + CR_N * kSI;
-    s.st = s.crec + CR_N * kS0;
-    s.red = reinterpret_cast<double*>(s.st);
+    s.stx = s.crec + CR_N * kS0;
+    s.st = reinterpret_cast<Real*>(s.stx + NB * kSI);
+    s.Fg = s.st + 2 * NB * kSI;
+    s.Fh = s.Fg + NB * kSI;
+    s.red = s.stx;
     return s;
 }
 
@@ -347,10 +351,10 @@ __device__ __forceinline__ Shk<Real> shk_from(const Real* src, int stride, int l
     return s;
 }
 static_assert(static_cast<size_t>(kParts0 - 1) * kS0 * 15 * sizeof(double) <=
-                  3 * static_cast<size_t>(Width<double>::B0) * kSI * sizeof(double),
+                  static_cast<size_t>(Width<double>::B0) * kSI * (sizeof(double) + 2 * sizeof(double)),
               "the cell-moment reduction must fit in the staging arrays");
 static_assert(static_cast<size_t>(kParts0 - 1) * kS0 * 15 * sizeof(double) <=
-                  3 * static_cast<size_t>(Width<float>::B0) * kSI * sizeof(float),
+                  static_cast<size_t>(Width<float>::B0) * kSI * (sizeof(double) + 2 * sizeof(float)),
               "the cell-moment reduction must fit in the staging arrays");
 
 __device__ __forceinline__ void load_dv_tables(const DevMesh& m, double* x1, double* w1) {
@@ -425,10 +429,11 @@ __device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
                                        const Real* __restrict__ g, const Real* __restrict__ h,
-                                       const Real* __restrict__ ctab, int l, int part, int c, bool active) {
+                                       const double* __restrict__ ctab, int l, int part, int c, bool active) {
     if (active) {
         constexpr int H = NB / kPartsL;
-        Real* sg = sm.stg + static_cast<size_t>(buf) * 3 * NB * kSL;
+        Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
+        double* sx = sm.stgx + static_cast<size_t>(buf) * NB * kSL;
         const size_t nC = static_cast<size_t>(m.nC);
 #pragma unroll
         for (int jj = 0; jj < H; ++jj) {
@@ -436,10 +441,10 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
             if (FULL || j < bp.nb) {
                 cp_async(sg + j * kSL + l, g + static_cast<size_t>(bp.d0 + j) * nC + c);
                 cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
-                cp_async(sg + (2 * NB + j) * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
+                cp_async(sx + j * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
             }
         }
-        Real* syz = sm.stgyz + buf * 2 * kSL;
+        double* syz = sm.stgyz + buf * 2 * kSL;
         if (part == 0) cp_async(syz + l, ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
         else if (D == 3) cp_async(syz + kSL + l, ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c);
     }
@@ -448,30 +453,30 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
-                                       int l, int part, bool active, Real K3D, Real c0h) {
+                                       int l, int part, bool active, double K3D, double c0h) {
     if (!active) return;
-    Shk<Real> s;
+    Shk<double> s;
     s.Ux = sm.crec[CR_UX * kSL + l];
     s.invRT = sm.crec[CR_INVRT * kSL + l];
     s.qx = sm.crec[CR_QX * kSL + l];
     s.RTh = sm.crec[CR_RTH * kSL + l];
     s.omr = sm.crec[CR_OMR * kSL + l];
-    const Real* syz = sm.stgyz + buf * 2 * kSL;
-    shk_batch<D, Real>(s, sm.crec[CR_UY * kSL + l], sm.crec[CR_UZ * kSL + l], sm.crec[CR_QY * kSL + l],
-                       sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y, q.Z, syz[l],
-                       D == 3 ? syz[kSL + l] : Real(1));
-    const Real* sg = sm.stg + static_cast<size_t>(buf) * 3 * NB * kSL;
+    const double* syz = sm.stgyz + buf * 2 * kSL;
+    shk_batch<D, double>(s, sm.crec[CR_UY * kSL + l], sm.crec[CR_UZ * kSL + l], sm.crec[CR_QY * kSL + l],
+                         sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y, q.Z, syz[l],
+                         D == 3 ? syz[kSL + l] : 1.0);
+    const Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
+    const double* sx = sm.stgx + static_cast<size_t>(buf) * NB * kSL;
     constexpr int H = NB / kPartsL;
 #pragma unroll
     for (int jj = 0; jj < H; ++jj) {
         const int j = part * H + jj;
         if (FULL || j < bp.nb) {
-            const Real x = Real(sm.x1[bp.ix0 + j]);
-            Real go, ho;
-            shk_relax<D, Real>(s, x, sg[(2 * NB + j) * kSL + l], sg[j * kSL + l], sg[(NB + j) * kSL + l], K3D, c0h, go,
-                               ho);
-            sm.gB[j * kSL + l] = go;
-            sm.hB[j * kSL + l] = ho;
+            double go, ho;
+            shk_relax<D, double>(s, sm.x1[bp.ix0 + j], sx[j * kSL + l], double(sg[j * kSL + l]),
+                                 double(sg[(NB + j) * kSL + l]), K3D, c0h, go, ho);
+            sm.gB[j * kSL + l] = Real(go);
+            sm.hB[j * kSL + l] = Real(ho);
         }
     }
 }
@@ -569,10 +574,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
-    const Real* ctab = reinterpret_cast<const Real*>(a.ds.ctab);
+    const double* ctab = a.ds.ctab;
     Real* const fvg = reinterpret_cast<Real*>(a.ds.fvg);
     Real* const fvh = reinterpret_cast<Real*>(a.ds.fvh);
-    const Real K3D = Real(m.K + 3 - m.D), c0h = Real(-(m.D * (m.K + 3 - m.D) + 2 * m.K));
+    const double K3D = m.K + 3.0 - m.D, c0h = -(m.D * (m.K + 3.0 - m.D) + 2.0 * m.K);
     const Real hdt = Real(0.5 * a.dt);
     const size_t nI = static_cast<size_t>(m.n_items);
 
@@ -585,17 +590,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     if (act1 && p1 == 0) {
         const double* cr = a.ds.cellrec;
         const size_t n = static_cast<size_t>(m.nC);
-        sm.crec[CR_UX * kSL + l1] = Real(__ldg(cr + REC_UX * n + c1));
-        sm.crec[CR_UY * kSL + l1] = Real(__ldg(cr + REC_UY * n + c1));
-        sm.crec[CR_UZ * kSL + l1] = Real(__ldg(cr + REC_UZ * n + c1));
-        sm.crec[CR_INVRT * kSL + l1] = Real(__ldg(cr + REC_INVRT * n + c1));
-        sm.crec[CR_QX * kSL + l1] = Real(__ldg(cr + REC_QX * n + c1));
-        sm.crec[CR_QY * kSL + l1] = Real(__ldg(cr + REC_QY * n + c1));
-        sm.crec[CR_QZ * kSL + l1] = Real(__ldg(cr + REC_QZ * n + c1));
-        sm.crec[CR_RTH * kSL + l1] = Real(__ldg(cr + REC_RTH * n + c1));
+        sm.crec[CR_UX * kSL + l1] = __ldg(cr + REC_UX * n + c1);
+        sm.crec[CR_UY * kSL + l1] = __ldg(cr + REC_UY * n + c1);
+        sm.crec[CR_UZ * kSL + l1] = __ldg(cr + REC_UZ * n + c1);
+        sm.crec[CR_INVRT * kSL + l1] = __ldg(cr + REC_INVRT * n + c1);
+        sm.crec[CR_QX * kSL + l1] = __ldg(cr + REC_QX * n + c1);
+        sm.crec[CR_QY * kSL + l1] = __ldg(cr + REC_QY * n + c1);
+        sm.crec[CR_QZ * kSL + l1] = __ldg(cr + REC_QZ * n + c1);
+        sm.crec[CR_RTH * kSL + l1] = __ldg(cr + REC_RTH * n + c1);
         const double r = __ldg(cr + REC_R * n + c1);
-        sm.crec[CR_OMR * kSL + l1] = Real(1.0 - r);
-        sm.crec[CR_R * kSL + l1] = Real(r);
+        sm.crec[CR_OMR * kSL + l1] = 1.0 - r;
+        sm.crec[CR_R * kSL + l1] = r;
     }
     // gradient stencils of the L0 cells (slot-major tables, -1: none)
     if (threadIdx.x < kS0 && m.nb_max <= kMaxRegStencil) {
@@ -769,7 +774,7 @@ __device__ __forceinline__ float flip_sign(float v, unsigned neg) {
 // batch (each thread stages and later reads only its own item's entries)
 template <typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
-                                            const Real* __restrict__ fvh, const Real* __restrict__ ftab, size_t nI,
+                                            const Real* __restrict__ fvh, const double* __restrict__ ftab, size_t nI,
                                             int it, int gi) {
     const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
     const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
@@ -778,7 +783,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
         if (FULL || j < bp.nb) {
             cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
             cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
-            cp_async(sm.st + (2 * NB + j) * kSI + it, ftab + tb + j * nI);
+            cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
         }
     }
     cp_commit();
@@ -788,8 +793,8 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
 // registers one batch ahead
 template <typename Real, int NB, bool FULL>
 __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __restrict__ g, const Real* __restrict__ h,
-                                            const Real* __restrict__ ctab, size_t nC, int c, int part, Real* pg,
-                                            Real* ph, Real* pe) {
+                                            const double* __restrict__ ctab, size_t nC, int c, int part, Real* pg,
+                                            Real* ph, double* pe) {
     constexpr int H = (NB + kParts0 - 1) / kParts0;
 #pragma unroll
     for (int jj = 0; jj < H; ++jj) {
@@ -815,9 +820,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     Real* hn = reinterpret_cast<Real*>(a.ds.h[1 - a.ds.cur]);
     const Real* fvg = reinterpret_cast<const Real*>(a.ds.fvg);
     const Real* fvh = reinterpret_cast<const Real*>(a.ds.fvh);
-    const Real* ctab = reinterpret_cast<const Real*>(a.ds.ctab);
-    const Real* ftab = reinterpret_cast<const Real*>(a.ds.ftab);
-    const Real K3D = Real(m.K + 3 - m.D), c0h = Real(-(m.D * (m.K + 3 - m.D) + 2 * m.K));
+    const double* ctab = a.ds.ctab;
+    const double* ftab = a.ds.ftab;
+    const double K3D = m.K + 3.0 - m.D, c0h = -(m.D * (m.K + 3.0 - m.D) + 2.0 * m.K);
     const size_t nI = static_cast<size_t>(m.n_items), nC = static_cast<size_t>(m.nC);
     load_dv_tables(m, sm.x1, sm.w1);
 
@@ -839,7 +844,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const bool has_cell = lc < t.n0;
     const int c = t.b + (has_cell ? lc : 0);
     if (has_cell && part == 0) stash_rec(sm.crec, kS0, lc, a.ds.cellrec, nC, c);
-    const Real dtV = has_cell ? Real(a.dt * __ldg(m.dtV + c)) : Real(0);
+    const double dtV = has_cell ? a.dt * __ldg(m.dtV + c) : 0.0;
     // flux list of the cell: item slot and sign (owner side: outflow, negated
     // by flipping the sign bit); absent entries read the zero slot kSI - 1,
     // which no item uses
@@ -862,7 +867,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
 
     constexpr int H = (NB + kParts0 - 1) / kParts0;
-    Real pg[H], ph[H], pe[H];
+    Real pg[H], ph[H];
+    double pe[H];
     BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
@@ -878,9 +884,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
         if (has_item) {
             const double p2 = __dmul_rn(q.Y, S[1]);
             const double p3 = D == 3 ? __dmul_rn(q.Z, S[2]) : 0.0;
-            const Real ey = __ldg(ftab + static_cast<size_t>(m.n1d + bp.iy) * nI + gi);
-            const Real ez = D == 3 ? __ldg(ftab + static_cast<size_t>(2 * m.n1d + bp.iz) * nI + gi) : Real(1);
-            const Shk<Real> fs = shk_from<D, Real>(sm.frec, kSI, it, q, ey, ez);
+            const double ey = __ldg(ftab + static_cast<size_t>(m.n1d + bp.iy) * nI + gi);
+            const double ez = D == 3 ? __ldg(ftab + static_cast<size_t>(2 * m.n1d + bp.iz) * nI + gi) : 1.0;
+            const Shk<double> fs = shk_from<D, double>(sm.frec, kSI, it, q, ey, ez);
+            const double* sx = sm.stx + it;
             cp_wait_all();  // this item's staged entries of batch k
             const Real* sg = sm.st + it;
             if (kind != ITEM_MESH_BOUNDARY) {
@@ -899,10 +906,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             rg += __ldg(fvg + o);
                             rh += __ldg(fvh + o);
                         }
-                        Real gf, hf;
-                        shk_relax<D, Real>(fs, Real(x), sg[(2 * NB + j) * kSI], rg, rh, K3D, c0h, gf, hf);
-                        sm.Fg[j * kSI + it] = Real(xs) * gf;
-                        sm.Fh[j * kSI + it] = Real(xs) * hf;
+                        double gf, hf;
+                        shk_relax<D, double>(fs, x, sx[j * kSI], double(rg), double(rh), K3D, c0h, gf, hf);
+                        sm.Fg[j * kSI + it] = Real(xs * gf);
+                        sm.Fh[j * kSI + it] = Real(xs * hf);
                     }
                 }
             } else {
@@ -927,21 +934,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
-                        Real gf, hf;
+                        double gf, hf;
                         if (xs > 0) {
                             // outgoing: relaxed with the boundary face's record,
                             // whose h uses the internal-face T at the patch-local
                             // index (fvDVM.C:1367, :1413, :1429-1444)
-                            shk_relax<D, Real>(fs, Real(x), sg[(2 * NB + j) * kSI], sg[j * kSI], sg[(NB + j) * kSI],
-                                               K3D, c0h, gf, hf);
+                            shk_relax<D, double>(fs, x, sx[j * kSI], double(sg[j * kSI]), double(sg[(NB + j) * kSI]),
+                                                 K3D, c0h, gf, hf);
                         } else {
                             const double cx = x - bU[0];
                             const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
-                            gf = Real(ge);
-                            hf = Real(ge * bHf);
+                            gf = double(Real(ge));
+                            hf = double(Real(ge * bHf));
                         }
-                        sm.Fg[j * kSI + it] = Real(xs) * gf;
-                        sm.Fh[j * kSI + it] = Real(xs) * hf;
+                        sm.Fg[j * kSI + it] = Real(xs * gf);
+                        sm.Fh[j * kSI + it] = Real(xs * hf);
                     }
                 }
             }
@@ -951,9 +958,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
         if (has_cell) {
-            const Real ey = __ldg(ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
-            const Real ez = D == 3 ? __ldg(ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c) : Real(1);
-            const Shk<Real> cs = shk_from<D, Real>(sm.crec, kS0, lc, q, ey, ez);
+            const double ey = __ldg(ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
+            const double ez = D == 3 ? __ldg(ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c) : 1.0;
+            const Shk<double> cs = shk_from<D, double>(sm.crec, kS0, lc, q, ey, ez);
             RowSums rs;
             row_zero(rs);
 #pragma unroll
@@ -962,8 +969,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 if (FULL || j < bp.nb) {
                     const Real gt = pg[jj], ht = ph[jj];
                     const double x = sm.x1[bp.ix0 + j];
-                    Real gb, hb;
-                    shk_relax<D, Real>(cs, Real(x), pe[jj], gt, ht, K3D, c0h, gb, hb);
+                    double gb, hb;
+                    shk_relax<D, double>(cs, x, pe[jj], double(gt), double(ht), K3D, c0h, gb, hb);
                     const Real* Fg = sm.Fg + j * kSI;
                     const Real* Fh = sm.Fh + j * kSI;
                     Real sg = 0, sh = 0;
@@ -980,8 +987,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             sh += e > 0 ? Fh[i] : -Fh[i];
                         }
                     }
-                    const Real g_new = fma(Real(-1.0 / 3), gt, fma(Real(4.0 / 3), gb, sg * dtV));
-                    const Real h_new = fma(Real(-1.0 / 3), ht, fma(Real(4.0 / 3), hb, sh * dtV));
+                    // the update in FP64, one rounding to the storage type
+                    const Real g_new = Real(fma(-1.0 / 3, double(gt), fma(4.0 / 3, gb, double(sg) * dtV)));
+                    const Real h_new = Real(fma(-1.0 / 3, double(ht), fma(4.0 / 3, hb, double(sh) * dtV)));
                     const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
                     gn[idx] = g_new;
                     hn[idx] = h_new;
