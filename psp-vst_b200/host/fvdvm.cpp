@@ -1,0 +1,77 @@
+// dugks_host::FvDVM (see fvdvm.hpp).
+#include "fvdvm.hpp"
+
+namespace dugks_host {
+
+FvDVM::FvDVM(const Case& c, int precision, int device) : case_(c), flat_(flatten(c)) {
+    const FlatMesh& f = flat_;
+    dugks_mesh mesh{f.n_cells,     f.n_internal,  f.n_boundary,
+                    f.D,           f.owner.data(), f.neighbour.data(),
+                    f.C.data(),    f.V.data(),    f.Cf.data(),
+                    f.Sf.data(),   static_cast<int32_t>(f.patch_type.size()), f.patch_start.data()};
+    dugks_dv_set dv{static_cast<int32_t>(case_.xis.size()), case_.xis.data(), case_.weights.data(), case_.xi_max};
+    dugks_gas gas{case_.R, case_.omega, case_.Tref, case_.mu_ref, case_.Pr, case_.K_inner};
+    dugks_bc bc{f.patch_type.data(), f.rho_b.data(), f.U_b.data(), f.T_b.data()};
+    dugks_options opt;
+    dugks_default_options(&opt);
+    opt.precision = precision;
+    opt.device = device;
+    const int st = dugks_create(&mesh, &dv, &gas, &bc, &opt, &h_);
+    if (st != DUGKS_OK) {
+        const std::string msg = h_ ? dugks_last_error(h_) : "dugks_create failed";
+        if (h_) dugks_destroy(h_);
+        h_ = nullptr;
+        throw FvDVMError(st, msg);
+    }
+    n_xi_ = dugks_n_dv(h_);
+    check(dugks_set_macros(h_, case_.rho0.data(), case_.U0.data(), case_.T0.data()), "dugks_set_macros");
+    rho_ = case_.rho0;
+    U_ = case_.U0;
+    T_ = case_.T0;
+    q_.assign(3 * static_cast<size_t>(f.n_cells), 0.0);
+}
+
+FvDVM::~FvDVM() {
+    if (h_) dugks_destroy(h_);
+}
+
+void FvDVM::check(int st, const char* what) const {
+    if (st != DUGKS_OK) throw FvDVMError(st, std::string(what) + ": " + dugks_last_error(h_));
+}
+
+void FvDVM::refresh() {
+    check(dugks_get_macros(h_, rho_.data(), U_.data(), T_.data(), q_.data()), "dugks_get_macros");
+}
+
+void FvDVM::evolution(double dt) {
+    check(dugks_step(h_, 1, &dt), "dugks_step");
+    refresh();
+}
+
+void FvDVM::getCoNum(double dt, double& maxCo, double& meanCo) const {
+    check(dugks_co_num(h_, dt, &maxCo, &meanCo), "dugks_co_num");
+}
+
+void FvDVM::surfMacros(std::vector<double>& rho, std::vector<double>& U, std::vector<double>& T,
+                       std::vector<double>& q) const {
+    const size_t nF = static_cast<size_t>(flat_.n_internal) + flat_.n_boundary;
+    rho.assign(nF, 0.0);
+    T.assign(nF, 0.0);
+    U.assign(3 * nF, 0.0);
+    q.assign(3 * nF, 0.0);
+    check(dugks_get_face_macros(h_, rho.data(), U.data(), T.data(), q.data()), "dugks_get_face_macros");
+}
+
+std::vector<double> FvDVM::boundaryRho() const {
+    std::vector<double> r(static_cast<size_t>(flat_.n_boundary), 0.0);
+    check(dugks_get_boundary_rho(h_, r.data()), "dugks_get_boundary_rho");
+    return r;
+}
+
+void FvDVM::dfOnCells(const std::vector<int32_t>& cells, std::vector<double>& g, std::vector<double>& h) const {
+    g.assign(cells.size() * static_cast<size_t>(n_xi_), 0.0);
+    h.assign(cells.size() * static_cast<size_t>(n_xi_), 0.0);
+    check(dugks_get_df(h_, cells.data(), static_cast<int32_t>(cells.size()), g.data(), h.data()), "dugks_get_df");
+}
+
+}  // namespace dugks_host

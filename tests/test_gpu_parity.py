@@ -113,6 +113,21 @@ def test_fp32c_ball():
     _run(c, 6, tol=TOL32, check_faces=False, floor=1e-2, precision=dl.FP32C)
 
 
+@pytest.mark.parametrize("steps", [200])
+def test_fp32c_long_run_within_1e6_of_fp64(steps):
+    # FP32 storage with the equilibrium and the relaxation in FP64: after
+    # hundreds of steps the macros stay within 1e-6 (plain relative L2, no
+    # floor) of the FP64 path on a far-field flow past a sphere
+    c = cs.ball_case(6, 6, 1.12, 8, kn=0.1, mach=0.5)
+    f64, f32 = dl.Solver(c), dl.Solver(c, precision=dl.FP32C)
+    f64.step(steps, c.dt)
+    f32.step(steps, c.dt)
+    a, b = f32.macros(), f64.macros()
+    for k in ("rho", "U", "T", "q"):
+        err = float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k]))
+        assert err <= 1e-6, (k, err)
+
+
 def test_state_restart_is_exact():
     c = cs.cavity_case(8, 8)
     a = dl.Solver(c)

@@ -1,0 +1,105 @@
+"""The standalone C++ host (psp-vst_b200/host: FoamFile reader, FvDVM over
+the C ABI, dugks_run driver) against the Python host path on the same case
+files.  Without a GPU: the case reader and the mesh flattening
+(`dugks_run --check`).  With a GPU: steps through the driver give the same
+fields as the Python Solver."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import case_writer
+import golden_cases
+from dugks_b200 import case as cs
+from dugks_b200 import foamio
+from dugks_b200 import lib as dl
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HOST = os.path.join(ROOT, "psp-vst_b200", "host")
+DRIVER = os.path.join(HOST, "bin", "dugks_run")
+
+
+@pytest.fixture(scope="module")
+def driver():
+    dl.load()   # the library the driver links
+    subprocess.run(["make", "-s", "-C", HOST], check=True)
+    assert os.path.exists(DRIVER)
+    return DRIVER
+
+
+def _run(driver, *args, check=True):
+    r = subprocess.run([driver, *map(str, args)], capture_output=True, text=True, timeout=600)
+    if check:
+        assert r.returncode == 0, r.stderr
+    return r
+
+
+def _summary(r) -> dict:
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_check_demo_cavity(driver, tmp_path):
+    c = golden_cases.demo_cavity()
+    d = case_writer.write_case(c, str(tmp_path / "cavity"))
+    s = _summary(_run(driver, d, "--check"))
+    fl = c.flat
+    assert s["cells"] == c.n_cells == 3600
+    assert s["internal_faces"] == fl["n_internal"] and s["boundary_faces"] == fl["n_boundary"] == 240
+    assert s["D"] == 2 and s["n_dv"] == 28 ** 2
+    assert s["volume"] == pytest.approx(float(np.sum(fl["V"])), rel=1e-14)
+    assert s["mass"] == pytest.approx(float(np.sum(c.rho0 * fl["V"])), rel=1e-14)
+    assert s["xi_max"] == c.xi_max
+    kinds = {p["name"]: p["kind"] for p in s["patches"]}
+    assert kinds == {"movingWall": "maxwellWall", "fixedWalls": "maxwellWall", "frontAndBack": "empty"}
+
+
+def test_check_ball_far_field(driver, tmp_path):
+    c = cs.ball_case(4, 4, 1.12, 6, kn=0.1, mach=0.5)
+    d = case_writer.write_case(c, str(tmp_path / "ball"))
+    s = _summary(_run(driver, d, "--check"))
+    assert s["cells"] == c.n_cells and s["D"] == 3 and s["n_dv"] == 216
+    assert s["boundary_faces"] == c.flat["n_boundary"]
+    kinds = {p["name"]: p["kind"] for p in s["patches"]}
+    assert kinds == {"wall": "maxwellWall", "farField": "farField"}
+    assert s["volume"] == pytest.approx(float(np.sum(c.flat["V"])), rel=1e-14)
+
+
+def test_unsupported_patch_type_is_an_error(driver, tmp_path):
+    c = cs.cavity_case(4, 6)
+    d = case_writer.write_case(c, str(tmp_path / "bad"), rho_patch_type={"movingWall": "zeroGradient"})
+    r = _run(driver, d, "--check", check=False)
+    assert r.returncode == 1 and "zeroGradient" in r.stderr
+
+
+def test_missing_case_is_an_error(driver, tmp_path):
+    r = _run(driver, str(tmp_path / "nothing"), "--check", check=False)
+    assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_steps_match_python_solver(driver, tmp_path):
+    c = golden_cases.demo_cavity()
+    d = case_writer.write_case(c, str(tmp_path / "cavity"))
+    steps = 3
+    s = _summary(_run(driver, d, "--steps", steps, "--dt", repr(c.dt)))
+    assert s["steps"] == steps and s["dt"] == c.dt
+    ref = dl.Solver(c)
+    ref.step(steps, c.dt)
+    m = ref.macros()
+    sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
+    tdir = os.path.join(d, s["time_name"])
+    rho = foamio.read_vol_field(os.path.join(tdir, "rho"), c.n_cells, sizes)
+    U = foamio.read_vol_field(os.path.join(tdir, "U"), c.n_cells, sizes)
+    T = foamio.read_vol_field(os.path.join(tdir, "T"), c.n_cells, sizes)
+    q = foamio.read_vol_field(os.path.join(tdir, "q"), c.n_cells, sizes)
+    # the fields are written with 15 significant digits
+    np.testing.assert_allclose(rho["internal"], m["rho"], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(T["internal"], m["T"], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(U["internal"], m["U"], rtol=1e-14, atol=1e-14 * np.abs(m["U"]).max())
+    np.testing.assert_allclose(q["internal"], m["q"], rtol=1e-14, atol=1e-14 * np.abs(m["q"]).max())
+    assert rho["patches"]["movingWall"]["type"] == "calculatedMaxwell"
+    np.testing.assert_allclose(rho["patches"]["movingWall"]["value"],
+                               ref.boundary_rho()[: sizes["movingWall"]], rtol=1e-14)
+    assert s["mass"] == pytest.approx(float(np.sum(m["rho"] * c.flat["V"])), rel=1e-13)
