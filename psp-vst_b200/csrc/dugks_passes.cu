@@ -244,7 +244,10 @@ struct SmemA {
     double* x1;     // [kMaxN1d] 1-D nodes
     double* w1;     // [kMaxN1d] 1-D weights
     double* crec;   // [CR_N][kSL] records of the local cells
-    double* stgx;   // [2][NB][kSL] staged e_x (double buffer)
+    // e_x of the local cells: when the DV set has at most 2 NB nodes per
+    // dimension, the whole table [n1d][kSL] is loaded once per CTA (e_x does
+    // not depend on the row); otherwise [2][NB][kSL] staged per batch
+    double* stgx;
     double* stgyz;  // [2][2][kSL] staged e_y, e_z
     Real* stg;      // [2][2][NB][kSL] staged g~, h~
     Real* gB;       // [NB][kSL] gbar+
@@ -429,7 +432,8 @@ __device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
                                        const Real* __restrict__ g, const Real* __restrict__ h,
-                                       const double* __restrict__ ctab, int l, int part, int c, bool active) {
+                                       const double* __restrict__ ctab, int l, int part, int c, bool active,
+                                       bool ex_res) {
     if (active) {
         constexpr int H = NB / kPartsL;
         Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
@@ -441,7 +445,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
             if (FULL || j < bp.nb) {
                 cp_async(sg + j * kSL + l, g + static_cast<size_t>(bp.d0 + j) * nC + c);
                 cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
-                cp_async(sx + j * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
+                if (!ex_res) cp_async(sx + j * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
             }
         }
         double* syz = sm.stgyz + buf * 2 * kSL;
@@ -453,7 +457,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
-                                       int l, int part, bool active, double K3D, double c0h) {
+                                       int l, int part, bool active, double K3D, double c0h, bool ex_res) {
     if (!active) return;
     Shk<double> s;
     s.Ux = sm.crec[CR_UX * kSL + l];
@@ -466,7 +470,7 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
                          sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y, q.Z, syz[l],
                          D == 3 ? syz[kSL + l] : 1.0);
     const Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
-    const double* sx = sm.stgx + static_cast<size_t>(buf) * NB * kSL;
+    const double* sx = sm.stgx + (ex_res ? bp.ix0 : buf * NB) * kSL;
     constexpr int H = NB / kPartsL;
 #pragma unroll
     for (int jj = 0; jj < H; ++jj) {
@@ -602,6 +606,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         sm.crec[CR_OMR * kSL + l1] = 1.0 - r;
         sm.crec[CR_R * kSL + l1] = r;
     }
+    const bool ex_res = m.n1d <= 2 * NB;
+    if (ex_res && act1)
+        for (int ix = p1; ix < m.n1d; ix += kPartsL)
+            sm.stgx[ix * kSL + l1] = __ldg(ctab + static_cast<size_t>(ix) * m.nC + c1);
     // gradient stencils of the L0 cells (slot-major tables, -1: none)
     if (threadIdx.x < kS0 && m.nb_max <= kMaxRegStencil) {
         const int l = threadIdx.x;
@@ -626,7 +634,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 
     BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
-    if (nbt > 0) stage0<D, Real, NB, FULL>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+    if (nbt > 0) stage0<D, Real, NB, FULL>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const int buf = k & 1;
         const BatchPos bp = walk.pos();
@@ -634,10 +642,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         __syncthreads();  // batch k staged; the previous batch's stage 3 is done
         if (k + 1 < nbt) {
             ahead.next();
-            stage0<D, Real, NB, FULL>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1);
+            stage0<D, Real, NB, FULL>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
         }
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
-        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h);
+        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res);
         __syncthreads();
         stage2<D, Real, NB, FULL>(m, sm, bp, t);
         __syncthreads();
