@@ -701,19 +701,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     const bool own_up = xs >= kVSmall, nei_up = xs < -kVSmall;
                     const bool up = own_side ? own_up : nei_up;
                     const bool tang = !own_up && !nei_up;
-                    const Real cs = up ? Real(1) : (tang ? Real(0.5) : Real(0));
-                    Real gg, hh;
-                    recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
-                    gg *= cs;
-                    hh *= cs;
-                    row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
+                    // the downwind side contributes nothing; neighbouring
+                    // tile-boundary faces share their orientation, so whole
+                    // warps skip together
                     if (up || tang) {
+                        const Real cs = up ? Real(1) : Real(0.5);
+                        Real gg, hh;
+                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                        gg *= cs;
+                        hh *= cs;
+                        row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
-                    }
-                    if (up) {
-                        og[j * nI] = gg;
-                        oh[j * nI] = hh;
+                        if (up) {
+                            og[j * nI] = gg;
+                            oh[j * nI] = hh;
+                        }
                     }
                 }
             }
