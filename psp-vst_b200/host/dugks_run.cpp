@@ -7,11 +7,13 @@
 // and q into time directories.
 //
 //   dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] [--device D]
-//                  [--write-interval N] [--no-write] [--check]
+//                  [--write-interval N] [--no-write] [--write-state] [--restart TIME] [--check]
 //
 // The time step is --dt, else controlDict deltaT, else the Courant number
 // 0.5 of the initial state (fvDVM::getCoNum).  The step count is --steps,
-// else (endTime - startTime) / dt.  --check reads the case and computes the
+// else (endTime - startTime) / dt.  --write-state adds an exact restart file
+// (dugksState, see fvdvm.hpp) to every written time directory; --restart TIME
+// continues from CASE/TIME/dugksState.  --check reads the case and computes the
 // mesh geometry on the host only (no GPU) and prints a summary.  The last
 // line printed is a JSON summary.
 #include <cmath>
@@ -35,12 +37,15 @@ struct Args {
     int device = 0;
     long write_interval = 0;
     bool write = true;
+    bool write_state = false;
     bool check = false;
+    std::string restart;
 };
 
 [[noreturn]] void usage(const char* msg) {
     std::fprintf(stderr, "dugks_run: %s\nusage: dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] "
-                         "[--device D] [--write-interval N] [--no-write] [--check]\n", msg);
+                         "[--device D] [--write-interval N] [--no-write] [--write-state] [--restart TIME] "
+                         "[--check]\n", msg);
     std::exit(2);
 }
 
@@ -58,6 +63,8 @@ Args parse(int argc, char** argv) {
         else if (s == "--write-interval") a.write_interval = std::atol(val());
         else if (s == "--no-write") a.write = false;
         else if (s == "--check") a.check = true;
+        else if (s == "--write-state") a.write_state = true;
+        else if (s == "--restart") a.restart = val();
         else if (s == "--precision") {
             const std::string p = val();
             if (p == "fp64") a.precision = DUGKS_FP64;
@@ -83,7 +90,8 @@ using PatchValues = std::vector<std::pair<std::string, std::pair<std::string, st
 
 // rho, U, T, q of the current state into CASE/<time>/ (the AUTO_WRITE
 // macro fields of src/createFields.H and fvDVM.C:2016-2105)
-void write_time(const FvDVM& s, const std::string& tname) {
+void write_time(const FvDVM& s, double time, bool state, double dt) {
+    const std::string tname = time_name(time);
     const Case& c = s.caseData();
     const FlatMesh& f = s.mesh();
     std::vector<double> frho, fU, fT, fq;
@@ -116,6 +124,7 @@ void write_time(const FvDVM& s, const std::string& tname) {
     write_vol_field(dir + "/U", "U", 3, s.Uvol(), pU, "[0 1 -1 0 0 0 0]", tname);
     write_vol_field(dir + "/T", "T", 1, s.Tvol(), pT, "[0 0 0 1 0 0 0]", tname);
     write_vol_field(dir + "/q", "q", 3, s.qVol(), pq, "[1 0 -3 0 0 0 0]", tname);
+    if (state) s.writeState(dir + "/dugksState", dt, time);
 }
 
 double total(const std::vector<double>& v, const std::vector<double>& w) {
@@ -156,14 +165,19 @@ int main(int argc, char** argv) {
         if (steps < 0) steps = c.end_time > c.start_time ? std::lround((c.end_time - c.start_time) / dt) : 1;
         long every = a.write_interval;
         if (every <= 0 && c.write_interval > 0 && c.delta_t > 0) every = std::lround(c.write_interval / c.delta_t);
-        double t = c.start_time;
+        double t0 = c.start_time;
+        if (!a.restart.empty()) {
+            double dt_prev = 0;
+            s.readState(c.dir + "/" + a.restart + "/dugksState", dt_prev, t0);
+        }
+        double t = t0;
         for (long n = 1; n <= steps; ++n) {
             s.evolution(dt);
-            t = c.start_time + n * dt;
+            t = t0 + n * dt;
             std::printf("Time = %s\n", time_name(t).c_str());
-            if (a.write && every > 0 && n % every == 0 && n != steps) write_time(s, time_name(t));
+            if (a.write && every > 0 && n % every == 0 && n != steps) write_time(s, t, a.write_state, dt);
         }
-        if (a.write && steps > 0) write_time(s, time_name(t));
+        if (a.write && steps > 0) write_time(s, t, a.write_state, dt);
         double co_max = 0, co_mean = 0;
         s.getCoNum(dt, co_max, co_mean);
         std::printf("{\"steps\": %ld, \"dt\": %.17g, \"time\": %.17g, \"time_name\": \"%s\", \"mass\": %.17g, "

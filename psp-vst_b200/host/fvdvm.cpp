@@ -1,6 +1,9 @@
 // dugks_host::FvDVM (see fvdvm.hpp).
 #include "fvdvm.hpp"
 
+#include <cstdio>
+#include <cstring>
+
 namespace dugks_host {
 
 FvDVM::FvDVM(const Case& c, int precision, int device) : case_(c), flat_(flatten(c)) {
@@ -72,6 +75,54 @@ void FvDVM::dfOnCells(const std::vector<int32_t>& cells, std::vector<double>& g,
     g.assign(cells.size() * static_cast<size_t>(n_xi_), 0.0);
     h.assign(cells.size() * static_cast<size_t>(n_xi_), 0.0);
     check(dugks_get_df(h_, cells.data(), static_cast<int32_t>(cells.size()), g.data(), h.data()), "dugks_get_df");
+}
+
+namespace {
+constexpr char kStateMagic[8] = {'D', 'U', 'G', 'K', 'S', 'S', 'T', '1'};
+}
+
+void FvDVM::writeState(const std::string& path, double dt_prev, double time) const {
+    const size_t n = static_cast<size_t>(n_xi_) * flat_.n_cells;
+    std::vector<double> g(n), h(n);
+    check(dugks_get_state(h_, g.data(), h.data()), "dugks_get_state");
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw FvDVMError(DUGKS_ERR_ARG, "cannot write " + path);
+    const int32_t D = flat_.D, n1d = nXiPerDim();
+    const int64_t nc = flat_.n_cells, nv = n_xi_;
+    bool ok = std::fwrite(kStateMagic, 1, 8, f) == 8 && std::fwrite(&D, sizeof D, 1, f) == 1 &&
+              std::fwrite(&n1d, sizeof n1d, 1, f) == 1 && std::fwrite(&nc, sizeof nc, 1, f) == 1 &&
+              std::fwrite(&nv, sizeof nv, 1, f) == 1 && std::fwrite(&dt_prev, sizeof dt_prev, 1, f) == 1 &&
+              std::fwrite(&time, sizeof time, 1, f) == 1 && std::fwrite(g.data(), sizeof(double), n, f) == n &&
+              std::fwrite(h.data(), sizeof(double), n, f) == n;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) throw FvDVMError(DUGKS_ERR_ARG, "error writing " + path);
+}
+
+void FvDVM::readState(const std::string& path, double& dt_prev, double& time) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw FvDVMError(DUGKS_ERR_ARG, "cannot open " + path);
+    char magic[8];
+    int32_t D = 0, n1d = 0;
+    int64_t nc = 0, nv = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::fread(&D, sizeof D, 1, f) == 1 &&
+              std::fread(&n1d, sizeof n1d, 1, f) == 1 && std::fread(&nc, sizeof nc, 1, f) == 1 &&
+              std::fread(&nv, sizeof nv, 1, f) == 1 && std::fread(&dt_prev, sizeof dt_prev, 1, f) == 1 &&
+              std::fread(&time, sizeof time, 1, f) == 1;
+    if (!ok || std::memcmp(magic, kStateMagic, 8) != 0) {
+        std::fclose(f);
+        throw FvDVMError(DUGKS_ERR_ARG, path + ": not a DUGKS state file");
+    }
+    if (D != flat_.D || n1d != nXiPerDim() || nc != flat_.n_cells || nv != n_xi_) {
+        std::fclose(f);
+        throw FvDVMError(DUGKS_ERR_ARG, path + ": state of another mesh or DV set");
+    }
+    const size_t n = static_cast<size_t>(nv) * static_cast<size_t>(nc);
+    std::vector<double> g(n), h(n);
+    ok = std::fread(g.data(), sizeof(double), n, f) == n && std::fread(h.data(), sizeof(double), n, f) == n;
+    std::fclose(f);
+    if (!ok) throw FvDVMError(DUGKS_ERR_ARG, path + ": truncated state file");
+    check(dugks_set_state(h_, g.data(), h.data(), dt_prev), "dugks_set_state");
+    refresh();
 }
 
 }  // namespace dugks_host

@@ -52,6 +52,17 @@ public:
     // g~ and h~ of the given cells, [cells][nXi] (fvDVM::writeDFonCell)
     void dfOnCells(const std::vector<int32_t>& cells, std::vector<double>& g, std::vector<double>& h) const;
 
+    // Exact restart file (no reference counterpart: dugksFoam re-initialises
+    // the DFs to the Maxwellian of the written macros, fvDVM.C:414-426).
+    // Binary, native byte order: the 8 bytes "DUGKSST1", int32 D, int32 n1d,
+    // int64 n_cells, int64 n_dv, double dt_prev, double time, then g~ and h~
+    // as DV-major [n_dv][n_cells] doubles in the case's cell numbering.
+    // dt_prev is the step that produced the state (it enters the cell heat
+    // flux); readState restores the state and the cell macros and returns
+    // dt_prev and time.
+    void writeState(const std::string& path, double dt_prev, double time) const;
+    void readState(const std::string& path, double& dt_prev, double& time);
+
     int nXi() const { return n_xi_; }
     int nXiPerDim() const { return static_cast<int>(case_.xis.size()); }
     const FlatMesh& mesh() const { return flat_; }

@@ -103,3 +103,32 @@ def test_driver_steps_match_python_solver(driver, tmp_path):
     np.testing.assert_allclose(rho["patches"]["movingWall"]["value"],
                                ref.boundary_rho()[: sizes["movingWall"]], rtol=1e-14)
     assert s["mass"] == pytest.approx(float(np.sum(m["rho"] * c.flat["V"])), rel=1e-13)
+
+
+@pytest.mark.gpu
+def test_restart_file_continues_exactly(driver, tmp_path):
+    # 4 steps straight vs 2 steps, an exact restart file, then 2 more steps:
+    # the written fields are identical, byte for byte
+    c = cs.cavity_case(12, 8)
+    a = case_writer.write_case(c, str(tmp_path / "straight"))
+    b = case_writer.write_case(c, str(tmp_path / "restarted"))
+    sa = _summary(_run(driver, a, "--steps", 4, "--dt", repr(c.dt)))
+    s1 = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--write-state"))
+    assert os.path.getsize(os.path.join(b, s1["time_name"], "dugksState")) == 8 + 4 + 4 + 8 + 8 + 8 + 8 + 2 * 8 * c.n_cells * 64
+    sb = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--restart", s1["time_name"]))
+    assert sa["time_name"] == sb["time_name"]
+    for name in ("rho", "U", "T", "q"):
+        with open(os.path.join(a, sa["time_name"], name)) as fa, open(os.path.join(b, sb["time_name"], name)) as fb:
+            assert fa.read() == fb.read(), name
+
+
+@pytest.mark.gpu
+def test_restart_rejects_another_mesh(driver, tmp_path):
+    c = cs.cavity_case(12, 8)
+    b = case_writer.write_case(c, str(tmp_path / "one"))
+    s1 = _summary(_run(driver, b, "--steps", 1, "--dt", repr(c.dt), "--write-state"))
+    other = case_writer.write_case(cs.cavity_case(10, 8), str(tmp_path / "two"))
+    os.makedirs(os.path.join(other, s1["time_name"]))
+    os.replace(os.path.join(b, s1["time_name"], "dugksState"), os.path.join(other, s1["time_name"], "dugksState"))
+    r = _run(driver, other, "--steps", 1, "--dt", repr(c.dt), "--restart", s1["time_name"], check=False)
+    assert r.returncode == 1 and "another mesh" in r.stderr
