@@ -165,6 +165,25 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
  * dt[0..n_steps-1]. */
 int dugks_step(dugks_handle* h, int32_t n_steps, const double* dt);
 
+/* Adjustable time step (controlDict adjustTimeStep yes): maxCo and
+ * maxDeltaT as src/readTimeControlsExplicit.H:39-46 reads them. */
+typedef struct dugks_adapt {
+    double max_co;
+    double max_delta_t;
+} dugks_adapt;
+
+/* n_steps iterations of the solver loop with an adjustable time step
+ * (src/dugksFoam.C:71-80: CourantNo, setDeltaTvar, evolution).  Before each
+ * step dt <- min(f dt, maxDeltaT), f = min(min(F, 1 + 0.1 F), 1.2),
+ * F = maxCo / (CoNum + 1e-15), CoNum the Courant number of the current face
+ * velocities at dt (src/setDeltaTvar.H:34-48, fvDVM.C:2177-2185).  The time
+ * step is kept and updated on the device, so the call does not wait for
+ * the host between steps.  *dt: in, the time step of the last step taken
+ * (runTime.deltaTValue(), e.g. controlDict deltaT); out, the time step of
+ * the last of these steps.  dt_history (may be NULL) receives the n_steps
+ * time steps used. */
+int dugks_step_adaptive(dugks_handle* h, int32_t n_steps, const dugks_adapt* adapt, double* dt, double* dt_history);
+
 /* fvDVM::getCoNum (fvDVM.C:2177-2185) for time step dt, from the current
  * face velocities. */
 int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean);
@@ -192,6 +211,18 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
  * the time step that produced them (it enters the heat-flux correction). */
 int dugks_get_state(dugks_handle* h, double* g, double* hh);
 int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double dt_prev);
+
+/* The record the next step starts from besides g~, h~: per cell (in the
+ * mesh's cell order) rho, U[3], T, q[3], tau as the last step's moment sums
+ * gave them, then the largest and the summed |U_f| + sqrt(D) xi_max over
+ * delta_f of the internal faces (Courant number per unit time step).
+ * dugks_set_state recomputes these from the DFs in another summation order,
+ * which differs in the last bits; setting the saved record after it makes a
+ * restart continue bit for bit.  Length: dugks_step_record_size doubles
+ * (9 n_cells + 2).  dugks_set_step_record requires rho, T, tau > 0. */
+int64_t dugks_step_record_size(const dugks_handle* h);
+int dugks_get_step_record(dugks_handle* h, double* rec);
+int dugks_set_step_record(dugks_handle* h, const double* rec);
 
 /* Number of discrete velocities (nDV^D). */
 int32_t dugks_n_dv(const dugks_handle* h);

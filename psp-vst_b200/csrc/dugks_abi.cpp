@@ -314,7 +314,7 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
         (st = dev_alloc(h, &ds.brec, nBF)) || (st = dev_alloc(h, &ds.bmom_in, static_cast<size_t>(nBF) * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.cm, static_cast<size_t>(nC) * 9)) ||
         (st = dev_alloc(h, &ds.fm, static_cast<size_t>(nF) * 9)) || (st = dev_alloc(h, &ds.co, 2)) ||
-        (st = dev_alloc(h, &ds.err, 4))) {
+        (st = dev_alloc(h, &ds.err, 4)) || (st = dev_alloc(h, &h->d_dt, 2))) {
         *out = h;
         return st;
     }
@@ -474,6 +474,59 @@ int dugks_step_timed(dugks_handle* h, int32_t n_steps, const double* dt, double*
     return run_steps(h, n_steps, dt, stage_ms);
 }
 
+int dugks_step_adaptive(dugks_handle* h, int32_t n_steps, const dugks_adapt* adapt, double* dt, double* dt_history) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_step_adaptive before dugks_set_macros");
+    if (n_steps < 0 || !adapt || !dt || !(*dt > 0) || !std::isfinite(*dt) || !(adapt->max_co > 0) ||
+        !(adapt->max_delta_t > 0))
+        return set_error(h, DUGKS_ERR_ARG, "dugks_step_adaptive: bad arguments");
+    if (n_steps == 0) return DUGKS_OK;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (n_steps > h->hist_cap) {
+        int st = dev_alloc(h, &h->d_hist, static_cast<size_t>(n_steps));
+        if (st) return st;
+        h->hist_cap = n_steps;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_dt, dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    // step k (1-based) runs with slot k & 1 and writes the next dt to the other
+    // slot after its face combine; step 1's dt comes from the current faces
+    auto slot = [&](int k) { return h->d_dt + (k & 1); };
+    int launches = 0;
+    dugks::StepArgs a = make_args(h, 0.0, 0.0);
+    CUDA_TRY(h, dugks::launch_adapt(a, h->d_dt, slot(1), h->d_hist, adapt->max_co, adapt->max_delta_t, h->stream));
+    a.dtp = slot(1);
+    CUDA_TRY(h, dugks::launch_cell_prep(a, h->stream));
+    launches += 2;
+    for (int k = 1; k <= n_steps; ++k) {
+        a = make_args(h, 0.0, 0.0);
+        a.dtp = slot(k);
+        a.dtnp = slot(k + 1);
+        CUDA_TRY(h, cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream));
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_A, h->stream, &launches));
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_FACE_COMBINE, h->stream, &launches));
+        CUDA_TRY(h, dugks::launch_adapt(a, slot(k), slot(k + 1), k < n_steps ? h->d_hist + k : nullptr,
+                                        adapt->max_co, adapt->max_delta_t, h->stream));
+        ++launches;
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, &launches));
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, &launches));
+        h->ds.cur = 1 - h->ds.cur;
+        h->steps_done++;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(dt, slot(n_steps), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (dt_history)
+        CUDA_TRY(h, cudaMemcpyAsync(dt_history, h->d_hist, static_cast<size_t>(n_steps) * sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->stream));
+    h->launches += launches;
+    h->cellrec_dt = 0.0;   // the records hold the next adaptive dt; a fixed step rebuilds them
+    int st = check_device_errors(h);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_step_ms = ms;
+    return st;
+}
+
 int64_t dugks_kernel_launches(const dugks_handle* h) { return h ? h->launches : 0; }
 
 int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean) {
@@ -487,6 +540,49 @@ int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean) {
     *co_max = mx * dt;
     *co_mean = h->nIF > 0 ? co[1] / h->nIF * dt : 0.0;
     return DUGKS_OK;
+}
+
+int64_t dugks_step_record_size(const dugks_handle* h) { return h ? 9 * static_cast<int64_t>(h->nC) + 2 : 0; }
+
+int dugks_get_step_record(dugks_handle* h, double* rec) {
+    if (!h || !rec) return set_error(h, DUGKS_ERR_ARG, "dugks_get_step_record: null argument");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_step_record before dugks_set_macros");
+    const int nC = h->nC;
+    std::vector<double> cm(static_cast<size_t>(nC) * 9);
+    CUDA_TRY(h, cudaMemcpyAsync(cm.data(), h->ds.cm, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(rec + cm.size(), h->ds.co, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const std::vector<int32_t>& perm = h->tiling.perm;
+    for (int c = 0; c < nC; ++c) std::memcpy(rec + 9 * static_cast<size_t>(perm[c]), &cm[9 * static_cast<size_t>(c)],
+                                             9 * sizeof(double));
+    return DUGKS_OK;
+}
+
+int dugks_set_step_record(dugks_handle* h, const double* rec) {
+    if (!h || !rec) return set_error(h, DUGKS_ERR_ARG, "dugks_set_step_record: null argument");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_set_step_record before dugks_set_macros");
+    const int nC = h->nC;
+    std::vector<double> cm(static_cast<size_t>(nC) * 9);
+    const std::vector<int32_t>& perm = h->tiling.perm;
+    for (int c = 0; c < nC; ++c) {
+        const double* r = rec + 9 * static_cast<size_t>(perm[c]);
+        bool ok = r[0] > 0 && r[4] > 0 && r[8] > 0;
+        for (int j = 0; j < 9; ++j) ok = ok && std::isfinite(r[j]);
+        if (!ok) return set_error(h, DUGKS_ERR_ARG, "dugks_set_step_record: bad record of cell " + std::to_string(perm[c]));
+        std::memcpy(&cm[9 * static_cast<size_t>(c)], r, 9 * sizeof(double));
+    }
+    const double* co = rec + cm.size();
+    double co_max;
+    std::memcpy(&co_max, &co[0], sizeof co_max);
+    if (!(co_max >= 0) || !std::isfinite(co_max) || !(co[1] >= 0) || !std::isfinite(co[1]))
+        return set_error(h, DUGKS_ERR_ARG, "dugks_set_step_record: bad Courant sums");
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.cm, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.co, co, 2 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, dugks::launch_cell_records(make_args(h, 0.0, 0.0), h->stream));
+    h->launches += 1;
+    h->cellrec_dt = 0;   // the next step sets the relax factors for its dt
+    return check_device_errors(h);
 }
 
 int dugks_get_macros(dugks_handle* h, double* rho, double* U, double* T, double* q) {

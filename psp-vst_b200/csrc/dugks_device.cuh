@@ -11,6 +11,9 @@ struct Consts {
     int D;
 };
 
+// this step's time step (device-resident when adaptive)
+__device__ __forceinline__ double step_dt(const StepArgs& a) { return a.dtp ? *a.dtp : a.dt; }
+
 inline Consts make_consts(const DevMesh& m, double dt) {
     Consts k;
     k.dt = dt;

@@ -179,6 +179,9 @@ struct dugks_handle {
     dugks::DevState ds{};
     std::vector<void*> allocations;
     int32_t* d_chunk_begin = nullptr;
+    double* d_dt = nullptr;         // [2] device time steps of adaptive stepping (ping-pong)
+    double* d_hist = nullptr;       // time steps of the last adaptive call
+    int32_t hist_cap = 0;
     bool initialised = false;
     double cellrec_dt = 0;          // time step the cell records' relax factors were built for
     long steps_done = 0;

@@ -86,7 +86,8 @@ __device__ __forceinline__ void write_face(const StepArgs& a, const Consts& k, i
     }
 }
 
-__global__ void k_face_combine_internal(const StepArgs a, const Consts k) {
+__global__ void k_face_combine_internal(const StepArgs a, Consts k) {
+    k.dt = step_dt(a);
     const DevMesh& m = a.dm;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     double co = 0.0;
@@ -128,7 +129,8 @@ __global__ void k_face_combine_internal(const StepArgs a, const Consts k) {
     }
 }
 
-__global__ void k_face_combine_boundary(const StepArgs a, const Consts k) {
+__global__ void k_face_combine_boundary(const StepArgs a, Consts k) {
+    k.dt = step_dt(a);
     const DevMesh& m = a.dm;
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.nBF) return;
@@ -172,7 +174,9 @@ __device__ __forceinline__ void write_cellrec(const StepArgs& a, const Consts& k
     write_maxwell_tables(a.dm, a.ds.ctab, n, c, U, 1.0 / RT, rho * inv_norm(RT, k.D));
 }
 
-__global__ void k_cell_combine(const StepArgs a, const Consts k, double dt_next) {
+__global__ void k_cell_combine(const StepArgs a, Consts k, double dt_next) {
+    k.dt = step_dt(a);
+    if (a.dtnp) dt_next = *a.dtnp;
     const DevMesh& m = a.dm;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nC) return;
@@ -200,6 +204,16 @@ __global__ void k_cell_combine(const StepArgs a, const Consts k, double dt_next)
     write_cellrec(a, k, c, rho, U, T, q, tau, dt_next);
 }
 
+// cell records and Maxwellian tables from the cell macros in cm (a restored
+// step record); the relax factor is left to k_cell_prep
+__global__ void k_cell_records(const StepArgs a, Consts k) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.dm.nC) return;
+    const double* cm = a.ds.cm + static_cast<size_t>(c) * 9;
+    const double U[3] = {cm[1], cm[2], cm[3]}, q[3] = {cm[5], cm[6], cm[7]};
+    write_cellrec(a, k, c, cm[0], U, cm[4], q, cm[8], 0.0);
+}
+
 // Maxwellian tables of every cell from its record (after the host wrote
 // the records at initialisation)
 __global__ void k_cell_tables(const StepArgs a) {
@@ -217,7 +231,8 @@ __global__ void k_cell_prep(const StepArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.dm.nC) return;
     const double tau = a.ds.cm[static_cast<size_t>(c) * 9 + 8];
-    a.ds.cellrec[REC_R * static_cast<size_t>(a.dm.nC) + c] = 1.5 * a.dt / (2.0 * tau + a.dt);
+    const double dt = step_dt(a);
+    a.ds.cellrec[REC_R * static_cast<size_t>(a.dm.nC) + c] = 1.5 * dt / (2.0 * tau + dt);
 }
 
 // initial Maxwellian state (fvDVM.C:414-426), DV-major
@@ -281,6 +296,25 @@ __global__ void k_init_wall(const StepArgs a) {
         for (int j = 0; j < 15; ++j) mi[j] = s[j];
         br->inByRho = si;
     }
+}
+
+// adjustable time step of src/setDeltaTvar.H:34-48 from the Courant number
+// CoNum = max_f dc_f (|U_f| + sqrt(D) xiMax) dt (fvDVM::getCoNum) of the
+// faces in co[0] (the maximum per unit dt, as double bits): F = maxCo /
+// (CoNum + SMALL), f = min(min(F, 1 + 0.1 F), 1.2), dt_out = min(f dt, maxDeltaT);
+// SMALL = 1e-15 (OpenFOAM's double SMALL).  Unfused operations, so that
+// the host evaluation of the same formula gives the same bits.
+__global__ void k_adapt(const double* co, const double* dt_in, double* dt_out, double* hist, double max_co,
+                        double max_dt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double per_dt = __longlong_as_double(*reinterpret_cast<const long long*>(co));
+    const double dt = *dt_in;
+    const double co_num = __dmul_rn(per_dt, dt);
+    const double F = max_co / __dadd_rn(co_num, 1.0e-15);
+    const double f = fmin(fmin(F, __dadd_rn(1.0, __dmul_rn(0.1, F))), 1.2);
+    const double dtn = fmin(__dmul_rn(f, dt), max_dt);
+    *dt_out = dtn;
+    if (hist) *hist = dtn;
 }
 
 // raw cell moments of the current state, one thread per cell looping over
@@ -364,6 +398,17 @@ cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s
     one.chunks = 1;
     const Consts k = make_consts(a.dm, a.dt);
     k_cell_combine<<<(a.dm.nC + 255) / 256, 256, 0, s>>>(one, k, 0.0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_records(const StepArgs& a, cudaStream_t s) {
+    k_cell_records<<<(a.dm.nC + 255) / 256, 256, 0, s>>>(a, make_consts(a.dm, a.dt));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adapt(const StepArgs& a, const double* dt_in, double* dt_out, double* hist, double max_co,
+                         double max_dt, cudaStream_t s) {
+    k_adapt<<<1, 32, 0, s>>>(a.ds.co, dt_in, dt_out, hist, max_co, max_dt);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,11 @@ struct StepArgs {
     int chunks;
     const int32_t* chunk_begin;  // [chunks+1] DV rows
     double dt_next;              // time step of the following step (0 = unknown)
+    // device-resident time steps (adaptive stepping): when set, the kernels
+    // read this step's dt from *dtp and the next step's from *dtnp instead of
+    // dt and dt_next
+    const double* dtp;
+    const double* dtnp;
     int wideA, wideB;            // batch width of each pass: 1 wide, 0 narrow
     int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
@@ -30,6 +35,13 @@ cudaError_t launch_init(const StepArgs& a, int precision, cudaStream_t s);
 // cell macros from the current state (raw moments over all DVs, then the
 // cell combine with time step dt for the heat-flux correction)
 cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s);
+// dt of the next step from the Courant number of this step's faces (in
+// ds.co) and dt_in, as src/setDeltaTvar.H:34-48 adjusts it; also stored to
+// *hist when hist is not null
+// cell records and Maxwellian tables rebuilt from the cell macros
+cudaError_t launch_cell_records(const StepArgs& a, cudaStream_t s);
+cudaError_t launch_adapt(const StepArgs& a, const double* dt_in, double* dt_out, double* hist, double max_co,
+                         double max_dt, cudaStream_t s);
 // one of the two tile passes (dugks_passes.cu)
 cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s);
 // batch widths and dynamic shared memory of the passes for a DV set of n1d

@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     Real* const fvg = reinterpret_cast<Real*>(a.ds.fvg);
     Real* const fvh = reinterpret_cast<Real*>(a.ds.fvh);
     const double K3D = m.K + 3.0 - m.D, c0h = -(m.D * (m.K + 3.0 - m.D) + 2.0 * m.K);
-    const Real hdt = Real(0.5 * a.dt);
+    const Real hdt = Real(0.5 * step_dt(a));
     const size_t nI = static_cast<size_t>(m.n_items);
 
     // CTA set-up: DV tables, records of the local cells, this thread's cell
@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const bool has_cell = lc < t.n0;
     const int c = t.b + (has_cell ? lc : 0);
     if (has_cell && part == 0) stash_rec(sm.crec, kS0, lc, a.ds.cellrec, nC, c);
-    const double dtV = has_cell ? a.dt * __ldg(m.dtV + c) : 0.0;
+    const double dtV = has_cell ? step_dt(a) * __ldg(m.dtV + c) : 0.0;
     // flux list of the cell: item slot and sign (owner side: outflow, negated
     // by flipping the sign bit); absent entries read the zero slot kSI - 1,
     // which no item uses

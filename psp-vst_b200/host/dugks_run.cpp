@@ -8,10 +8,17 @@
 //
 //   dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] [--device D]
 //                  [--write-interval N] [--no-write] [--write-state] [--restart TIME] [--check]
+//                  [--max-co C] [--max-delta-t DT] [--fixed-dt]
 //
 // The time step is --dt, else controlDict deltaT, else the Courant number
-// 0.5 of the initial state (fvDVM::getCoNum).  The step count is --steps,
-// else (endTime - startTime) / dt.  --write-state adds an exact restart file
+// 0.5 of the initial state (fvDVM::getCoNum).  With controlDict
+// adjustTimeStep on, or --max-co given, every step first adjusts it to hold
+// the Courant number at maxCo (CourantNo.H + setDeltaTvar.H, on the device);
+// --fixed-dt turns that off.  The step count is --steps, else the steps that
+// reach endTime (Time::run: time < endTime - dt/2).  Fixed steps write every
+// --write-interval steps, else every writeInterval / deltaT steps; adjusted
+// steps write when the time passes a multiple of writeInterval (the time step
+// is not shortened to land on it).  --write-state adds an exact restart file
 // (dugksState, see fvdvm.hpp) to every written time directory; --restart TIME
 // continues from CASE/TIME/dugksState.  --check reads the case and computes the
 // mesh geometry on the host only (no GPU) and prints a summary.  The last
@@ -39,13 +46,15 @@ struct Args {
     bool write = true;
     bool write_state = false;
     bool check = false;
+    bool fixed_dt = false;
+    double max_co = 0, max_delta_t = 0;
     std::string restart;
 };
 
 [[noreturn]] void usage(const char* msg) {
     std::fprintf(stderr, "dugks_run: %s\nusage: dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] "
                          "[--device D] [--write-interval N] [--no-write] [--write-state] [--restart TIME] "
-                         "[--check]\n", msg);
+                         "[--check] [--max-co C] [--max-delta-t DT] [--fixed-dt]\n", msg);
     std::exit(2);
 }
 
@@ -65,6 +74,9 @@ Args parse(int argc, char** argv) {
         else if (s == "--check") a.check = true;
         else if (s == "--write-state") a.write_state = true;
         else if (s == "--restart") a.restart = val();
+        else if (s == "--max-co") a.max_co = std::atof(val());
+        else if (s == "--max-delta-t") a.max_delta_t = std::atof(val());
+        else if (s == "--fixed-dt") a.fixed_dt = true;
         else if (s == "--precision") {
             const std::string p = val();
             if (p == "fp64") a.precision = DUGKS_FP64;
@@ -144,9 +156,11 @@ int main(int argc, char** argv) {
             double vol = 0;
             for (double v : f.V) vol += v;
             std::printf("{\"cells\": %d, \"internal_faces\": %d, \"boundary_faces\": %d, \"D\": %d, "
-                        "\"n_dv\": %.0f, \"volume\": %.17g, \"mass\": %.17g, \"xi_max\": %.17g, \"patches\": [",
+                        "\"n_dv\": %.0f, \"volume\": %.17g, \"mass\": %.17g, \"xi_max\": %.17g, "
+                        "\"adjust_time_step\": %s, \"max_co\": %.17g, \"max_delta_t\": %.17g, \"patches\": [",
                         f.n_cells, f.n_internal, f.n_boundary, f.D, std::pow(double(c.xis.size()), f.D), vol,
-                        total(c.rho0, f.V), c.xi_max);
+                        total(c.rho0, f.V), c.xi_max, c.adjust_time_step ? "true" : "false", c.max_co,
+                        c.max_delta_t);
             for (size_t p = 0; p < c.mesh.patches.size(); ++p)
                 std::printf("%s{\"name\": \"%s\", \"kind\": \"%s\", \"faces\": %lld}", p ? ", " : "",
                             c.mesh.patches[p].name.c_str(), kind_name(c.kinds[p]),
@@ -161,28 +175,47 @@ int main(int argc, char** argv) {
             s.getCoNum(1.0, co_max, co_mean);   // Courant number per unit time step
             dt = 0.5 / co_max;
         }
-        long steps = a.steps;
-        if (steps < 0) steps = c.end_time > c.start_time ? std::lround((c.end_time - c.start_time) / dt) : 1;
-        long every = a.write_interval;
-        if (every <= 0 && c.write_interval > 0 && c.delta_t > 0) every = std::lround(c.write_interval / c.delta_t);
+        const bool adjust = !a.fixed_dt && (c.adjust_time_step || a.max_co > 0);
+        const double max_co = a.max_co > 0 ? a.max_co : c.max_co;
+        const double max_dt = a.max_delta_t > 0 ? a.max_delta_t : c.max_delta_t;
         double t0 = c.start_time;
         if (!a.restart.empty()) {
             double dt_prev = 0;
             s.readState(c.dir + "/" + a.restart + "/dugksState", dt_prev, t0);
         }
+        long steps = a.steps;
+        if (steps < 0 && !adjust) steps = c.end_time > t0 ? std::lround((c.end_time - t0) / dt) : 1;
+        if (steps < 0 && !(c.end_time > t0)) steps = 1;
+        long every = a.write_interval;
+        if (every <= 0 && !adjust && c.write_interval > 0 && c.delta_t > 0)
+            every = std::lround(c.write_interval / c.delta_t);
+        const bool by_time = adjust && a.write_interval <= 0 && c.write_interval > 0;
+        long write_index = 0;
         double t = t0;
-        for (long n = 1; n <= steps; ++n) {
-            s.evolution(dt);
-            t = t0 + n * dt;
+        long n = 0;
+        bool written = false;
+        while (steps >= 0 ? n < steps : t < c.end_time - 0.5 * dt) {
+            if (adjust) s.evolutionAdjustable(dt, max_co, max_dt);
+            else s.evolution(dt);
+            ++n;
+            t = adjust ? t + dt : t0 + n * dt;
             std::printf("Time = %s\n", time_name(t).c_str());
-            if (a.write && every > 0 && n % every == 0 && n != steps) write_time(s, t, a.write_state, dt);
+            bool due = every > 0 && n % every == 0;
+            if (by_time) {   // Time::writeTime for adjustableRunTime
+                const long idx = static_cast<long>(std::floor((t - t0 + 0.5 * dt) / c.write_interval));
+                due = idx > write_index;
+                if (due) write_index = idx;
+            }
+            written = a.write && due;
+            if (written) write_time(s, t, a.write_state, dt);
         }
-        if (a.write && steps > 0) write_time(s, t, a.write_state, dt);
+        const long done = n;
+        if (a.write && done > 0 && !written) write_time(s, t, a.write_state, dt);
         double co_max = 0, co_mean = 0;
         s.getCoNum(dt, co_max, co_mean);
         std::printf("{\"steps\": %ld, \"dt\": %.17g, \"time\": %.17g, \"time_name\": \"%s\", \"mass\": %.17g, "
                     "\"co_max\": %.17g, \"co_mean\": %.17g, \"n_dv\": %d}\n",
-                    steps, dt, t, time_name(t).c_str(), total(s.rhoVol(), s.mesh().V), co_max, co_mean, s.nXi());
+                    done, dt, t, time_name(t).c_str(), total(s.rhoVol(), s.mesh().V), co_max, co_mean, s.nXi());
         return 0;
     } catch (const FvDVMError& e) {
         std::fprintf(stderr, "dugks_run: %s (status %d)\n", e.what(), e.status);

@@ -253,6 +253,15 @@ void make_dirs(const std::string& path) {
         if (k == path.size() || path[k] == '/') mkdir(path.substr(0, k).c_str(), 0755);
 }
 
+// an OpenFOAM Switch entry (yes/no, on/off, true/false, y/n, t/f, none)
+bool switch_value(const FoamValue& v) {
+    if (v.kind != FoamValue::Word) throw FoamError("entry is not a switch");
+    const std::string& w = v.word;
+    if (w == "yes" || w == "on" || w == "true" || w == "y" || w == "t") return true;
+    if (w == "no" || w == "off" || w == "false" || w == "n" || w == "f" || w == "none") return false;
+    throw FoamError("bad switch value '" + w + "'");
+}
+
 }  // namespace
 
 const FoamValue* FoamValue::find(const std::string& key) const {
@@ -454,6 +463,9 @@ Case read_case(const std::string& dir) {
         if (const FoamValue* v = d.find("endTime")) c.end_time = v->number();
         if (const FoamValue* v = d.find("deltaT")) c.delta_t = v->number();
         if (const FoamValue* v = d.find("writeInterval")) c.write_interval = v->number();
+        if (const FoamValue* v = d.find("adjustTimeStep")) c.adjust_time_step = switch_value(*v);
+        if (const FoamValue* v = d.find("maxCo")) c.max_co = v->number();
+        if (const FoamValue* v = d.find("maxDeltaT")) c.max_delta_t = v->number();
     }
     return c;
 }

@@ -95,6 +95,10 @@ struct Case {
     std::vector<double> rho0, U0, T0;   // initial cell fields
     // system/controlDict (0 when absent)
     double start_time = 0, end_time = 0, delta_t = 0, write_interval = 0;
+    // adjustable time step (src/readTimeControlsExplicit.H:39-46, OpenFOAM's
+    // GREAT = 1e15 as the maxDeltaT default)
+    bool adjust_time_step = false;
+    double max_co = 1.0, max_delta_t = 1.0e15;
 };
 Case read_case(const std::string& dir);
 

@@ -51,6 +51,12 @@ void FvDVM::evolution(double dt) {
     refresh();
 }
 
+void FvDVM::evolutionAdjustable(double& dt, double maxCo, double maxDeltaT) {
+    const dugks_adapt ad{maxCo, maxDeltaT};
+    check(dugks_step_adaptive(h_, 1, &ad, &dt, nullptr), "dugks_step_adaptive");
+    refresh();
+}
+
 void FvDVM::getCoNum(double dt, double& maxCo, double& meanCo) const {
     check(dugks_co_num(h_, dt, &maxCo, &meanCo), "dugks_co_num");
 }
@@ -78,13 +84,15 @@ void FvDVM::dfOnCells(const std::vector<int32_t>& cells, std::vector<double>& g,
 }
 
 namespace {
-constexpr char kStateMagic[8] = {'D', 'U', 'G', 'K', 'S', 'S', 'T', '1'};
+constexpr char kStateMagic[8] = {'D', 'U', 'G', 'K', 'S', 'S', 'T', '2'};
 }
 
 void FvDVM::writeState(const std::string& path, double dt_prev, double time) const {
     const size_t n = static_cast<size_t>(n_xi_) * flat_.n_cells;
     std::vector<double> g(n), h(n);
     check(dugks_get_state(h_, g.data(), h.data()), "dugks_get_state");
+    std::vector<double> rec(static_cast<size_t>(dugks_step_record_size(h_)));
+    check(dugks_get_step_record(h_, rec.data()), "dugks_get_step_record");
     std::FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) throw FvDVMError(DUGKS_ERR_ARG, "cannot write " + path);
     const int32_t D = flat_.D, n1d = nXiPerDim();
@@ -93,7 +101,8 @@ void FvDVM::writeState(const std::string& path, double dt_prev, double time) con
               std::fwrite(&n1d, sizeof n1d, 1, f) == 1 && std::fwrite(&nc, sizeof nc, 1, f) == 1 &&
               std::fwrite(&nv, sizeof nv, 1, f) == 1 && std::fwrite(&dt_prev, sizeof dt_prev, 1, f) == 1 &&
               std::fwrite(&time, sizeof time, 1, f) == 1 && std::fwrite(g.data(), sizeof(double), n, f) == n &&
-              std::fwrite(h.data(), sizeof(double), n, f) == n;
+              std::fwrite(h.data(), sizeof(double), n, f) == n &&
+              std::fwrite(rec.data(), sizeof(double), rec.size(), f) == rec.size();
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) throw FvDVMError(DUGKS_ERR_ARG, "error writing " + path);
 }
@@ -117,11 +126,13 @@ void FvDVM::readState(const std::string& path, double& dt_prev, double& time) {
         throw FvDVMError(DUGKS_ERR_ARG, path + ": state of another mesh or DV set");
     }
     const size_t n = static_cast<size_t>(nv) * static_cast<size_t>(nc);
-    std::vector<double> g(n), h(n);
-    ok = std::fread(g.data(), sizeof(double), n, f) == n && std::fread(h.data(), sizeof(double), n, f) == n;
+    std::vector<double> g(n), h(n), rec(static_cast<size_t>(dugks_step_record_size(h_)));
+    ok = std::fread(g.data(), sizeof(double), n, f) == n && std::fread(h.data(), sizeof(double), n, f) == n &&
+         std::fread(rec.data(), sizeof(double), rec.size(), f) == rec.size();
     std::fclose(f);
     if (!ok) throw FvDVMError(DUGKS_ERR_ARG, path + ": truncated state file");
     check(dugks_set_state(h_, g.data(), h.data(), dt_prev), "dugks_set_state");
+    check(dugks_set_step_record(h_, rec.data()), "dugks_set_step_record");
     refresh();
 }
 

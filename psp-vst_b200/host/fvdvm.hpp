@@ -38,6 +38,10 @@ public:
 
     // one DUGKS step of size dt; refreshes the host macro fields
     void evolution(double dt);
+    // CourantNo.H + setDeltaTvar.H + evolution() (src/dugksFoam.C:65-75):
+    // dt (the previous step's) is adjusted on the device to hold maxCo and
+    // returned as the step taken
+    void evolutionAdjustable(double& dt, double maxCo, double maxDeltaT);
     void getCoNum(double dt, double& maxCo, double& meanCo) const;
 
     const std::vector<double>& rhoVol() const { return rho_; }
@@ -54,11 +58,13 @@ public:
 
     // Exact restart file (no reference counterpart: dugksFoam re-initialises
     // the DFs to the Maxwellian of the written macros, fvDVM.C:414-426).
-    // Binary, native byte order: the 8 bytes "DUGKSST1", int32 D, int32 n1d,
+    // Binary, native byte order: the 8 bytes "DUGKSST2", int32 D, int32 n1d,
     // int64 n_cells, int64 n_dv, double dt_prev, double time, then g~ and h~
-    // as DV-major [n_dv][n_cells] doubles in the case's cell numbering.
+    // as DV-major [n_dv][n_cells] doubles in the case's cell numbering, then
+    // the step record (dugks_get_step_record: 9 n_cells + 2 doubles).
     // dt_prev is the step that produced the state (it enters the cell heat
-    // flux); readState restores the state and the cell macros and returns
+    // flux); readState restores the state, the cell macros and the Courant
+    // sums exactly, so that the run continues bit for bit, and returns
     // dt_prev and time.
     void writeState(const std::string& path, double dt_prev, double time) const;
     void readState(const std::string& path, double& dt_prev, double& time);

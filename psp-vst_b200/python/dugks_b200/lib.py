@@ -57,6 +57,10 @@ class BC(C.Structure):
     _fields_ = [("patch_type", _i32p), ("rho", _dp), ("U", _dp), ("T", _dp)]
 
 
+class Adapt(C.Structure):
+    _fields_ = [("max_co", C.c_double), ("max_delta_t", C.c_double)]
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("ls_weighting", C.c_int32), ("device", C.c_int32),
                 ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("reserved", C.c_int32 * 11)]
@@ -73,12 +77,16 @@ SIGNATURES = {
     "dugks_set_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "dugks_step": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "dugks_co_num": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp]),
+    "dugks_step_adaptive": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Adapt), _dp, _dp]),
     "dugks_get_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "dugks_get_face_macros": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "dugks_get_boundary_rho": (C.c_int, [C.c_void_p, _dp]),
     "dugks_get_df": (C.c_int, [C.c_void_p, _i32p, C.c_int32, _dp, _dp]),
     "dugks_get_state": (C.c_int, [C.c_void_p, _dp, _dp]),
     "dugks_set_state": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double]),
+    "dugks_step_record_size": (C.c_int64, [C.c_void_p]),
+    "dugks_get_step_record": (C.c_int, [C.c_void_p, _dp]),
+    "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_last_step_ms": (C.c_int, [C.c_void_p, _dp]),
     "dugks_step_timed": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
@@ -207,6 +215,15 @@ class Solver:
         dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (n,)))
         self._check(self.lib.dugks_step(self.h, n, ptr(dts)))
 
+    def step_adaptive(self, n: int, dt: float, max_co: float, max_delta_t: float = 1e300):
+        """n steps with the adjustable time step (setDeltaTvar); dt is the
+        last step's time step.  Returns (last dt, array of the n dts)."""
+        ad = Adapt(max_co, max_delta_t)
+        d = C.c_double(dt)
+        hist = np.zeros(max(n, 1))
+        self._check(self.lib.dugks_step_adaptive(self.h, n, C.byref(ad), C.byref(d), ptr(hist)))
+        return d.value, hist[:n]
+
     def step_timed(self, n: int, dt) -> np.ndarray:
         """n steps with CUDA events around every stage: [passA, face combine,
         passB, cell combine, total] milliseconds summed over the steps."""
@@ -260,10 +277,24 @@ class Solver:
         self._check(self.lib.dugks_get_state(self.h, ptr(g), ptr(hh)))
         return g, hh
 
-    def set_state(self, g, hh, dt_prev: float):
+    def set_state(self, g, hh, dt_prev: float, record=None):
+        """Load g~, h~; with the step record of the run that produced them
+        the next steps continue bit for bit."""
         g = np.ascontiguousarray(g, dtype=np.float64)
         hh = np.ascontiguousarray(hh, dtype=np.float64)
         self._check(self.lib.dugks_set_state(self.h, ptr(g), ptr(hh), dt_prev))
+        if record is not None:
+            rec = np.ascontiguousarray(record, dtype=np.float64)
+            if rec.size != self.lib.dugks_step_record_size(self.h):
+                raise ValueError("step record of another mesh")
+            self._check(self.lib.dugks_set_step_record(self.h, ptr(rec)))
+
+    def step_record(self) -> np.ndarray:
+        """Per-cell rho, U, T, q, tau and the Courant sums of the last step
+        (dugks_get_step_record)."""
+        rec = np.zeros(self.lib.dugks_step_record_size(self.h))
+        self._check(self.lib.dugks_get_step_record(self.h, ptr(rec)))
+        return rec
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

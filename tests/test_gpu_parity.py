@@ -133,19 +133,31 @@ def test_fp32c_long_run_within_1e6_of_fp64(steps):
 
 
 def test_state_restart_is_exact():
+    # the DFs alone give the macros to rounding (another summation order);
+    # with the step record the run continues bit for bit, adaptive steps too
     c = cs.cavity_case(8, 8)
     a = dl.Solver(c)
     a.step(5, c.dt)
     g, h = a.state()
+    rec = a.step_record()
     b = dl.Solver(c)
     b.set_state(g, h, c.dt)
     errs = ob.macro_errors(b.macros(), a.macros(), c.gas["R"])
     assert max(errs.values()) <= 1e-13, errs
+    b.set_state(g, h, c.dt, rec)
+    assert np.array_equal(b.step_record(), rec)
     a.step(3, c.dt)
     b.step(3, c.dt)
+    da, ha = a.step_adaptive(3, c.dt, 0.5)
+    db, hb = b.step_adaptive(3, c.dt, 0.5)
+    assert da == db and np.array_equal(ha, hb)
     ga, _ = a.state()
     gb, _ = b.state()
-    assert ob.rel_l2(gb, ga) <= 1e-13
+    assert np.array_equal(ga, gb)
+    bad = rec.copy()
+    bad[0] = -1.0
+    with pytest.raises(dl.DugksError):
+        b.set_state(g, h, c.dt, bad)
 
 
 def test_df_output_matches_state():
@@ -169,6 +181,72 @@ def test_multi_step_call_equals_single_steps():
     ga, _ = a.state()
     gb, _ = b.state()
     assert np.array_equal(ga, gb)
+
+
+def _oracle_adaptive(orc, n, dt, max_co, max_dt):
+    """The reference's time loop with adjustTimeStep on (src/dugksFoam.C:63-75:
+    CourantNo.H, setDeltaTvar.H:34-48 with SMALL = 1e-15, then evolution)."""
+    hist = []
+    for _ in range(n):
+        co = orc.get_co_num(dt)[0]
+        F = max_co / (co + 1e-15)
+        f = min(min(F, 1.0 + 0.1 * F), 1.2)
+        dt = min(f * dt, max_dt)
+        hist.append(dt)
+        orc.evolution(dt)
+    return dt, np.array(hist)
+
+
+@pytest.mark.parametrize("max_dt", [1e300, None])
+def test_adaptive_time_step_matches_oracle(max_dt):
+    # the case's dt sits at Co 0.5; starting from a quarter of it, the step
+    # grows by 1.2 per step until the Courant limit (or maxDeltaT) holds it
+    c = cs.cavity_case(8, 8)
+    dt0 = 0.25 * c.dt
+    if max_dt is None:
+        max_dt = 0.5 * c.dt
+    gpu, orc = _pair(c)
+    dg, hg = gpu.step_adaptive(16, dt0, 0.5, max_dt)
+    do, ho = _oracle_adaptive(orc, 16, dt0, 0.5, max_dt)
+    assert np.max(np.abs(hg - ho) / ho) <= 1e-12, (hg, ho)
+    assert dg == hg[-1]
+    errs = ob.macro_errors(gpu.macros(), orc.macros(), c.gas["R"])
+    assert max(errs.values()) <= TOL64, errs
+    if max_dt < 1e300:
+        assert np.max(hg) == max_dt
+
+
+def test_adaptive_time_step_ball_far_field():
+    c = cs.ball_case(6, 6, 1.12, 8)
+    gpu, orc = _pair(c)
+    _, hg = gpu.step_adaptive(8, c.dt, 0.4)
+    _, ho = _oracle_adaptive(orc, 8, c.dt, 0.4, 1e300)
+    assert np.max(np.abs(hg - ho) / ho) <= 1e-12, (hg, ho)
+    errs = ob.macro_errors(gpu.macros(), orc.macros(), c.gas["R"])
+    assert max(errs.values()) <= TOL64, errs
+
+
+def test_adaptive_calls_chain_exactly():
+    # one call of n adaptive steps equals n calls of one step, and a fixed
+    # step after an adaptive call rebuilds its relax factors
+    c = cs.cavity_case(8, 8)
+    a, b = dl.Solver(c), dl.Solver(c)
+    da, ha = a.step_adaptive(6, c.dt, 0.5)
+    db, hb = c.dt, []
+    for _ in range(6):
+        db, h1 = b.step_adaptive(1, db, 0.5)
+        hb.append(h1[0])
+    assert da == db and np.array_equal(ha, np.array(hb))
+    ga, _ = a.state()
+    gb, _ = b.state()
+    assert np.array_equal(ga, gb)
+    orc = ob.Oracle(c)
+    _oracle_adaptive(orc, 6, c.dt, 0.5, 1e300)
+    a.step(2, 0.7 * da)
+    orc.evolution(0.7 * da)
+    orc.evolution(0.7 * da)
+    errs = ob.macro_errors(a.macros(), orc.macros(), c.gas["R"])
+    assert max(errs.values()) <= TOL64, errs
 
 
 def test_errors_are_reported_not_fatal():

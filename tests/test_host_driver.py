@@ -66,6 +66,21 @@ def test_check_ball_far_field(driver, tmp_path):
     assert s["volume"] == pytest.approx(float(np.sum(c.flat["V"])), rel=1e-14)
 
 
+def test_check_reads_time_controls(driver, tmp_path):
+    # readTimeControlsExplicit.H: adjustTimeStep (a Switch), maxCo, maxDeltaT
+    c = cs.cavity_case(4, 6)
+    d = case_writer.write_case(c, str(tmp_path / "a"), control={"deltaT": 1e-5, "adjustTimeStep": "on",
+                                                                "maxCo": 0.7, "maxDeltaT": 2e-5})
+    s = _summary(_run(driver, d, "--check"))
+    assert s["adjust_time_step"] is True and s["max_co"] == 0.7 and s["max_delta_t"] == 2e-5
+    d = case_writer.write_case(c, str(tmp_path / "b"), control={"deltaT": 1e-5})
+    s = _summary(_run(driver, d, "--check"))
+    assert s["adjust_time_step"] is False and s["max_co"] == 1.0 and s["max_delta_t"] == 1e15
+    d = case_writer.write_case(c, str(tmp_path / "c"), control={"adjustTimeStep": "maybe"})
+    r = _run(driver, d, "--check", check=False)
+    assert r.returncode == 1 and "maybe" in r.stderr
+
+
 def test_unsupported_patch_type_is_an_error(driver, tmp_path):
     c = cs.cavity_case(4, 6)
     d = case_writer.write_case(c, str(tmp_path / "bad"), rho_patch_type={"movingWall": "zeroGradient"})
@@ -114,7 +129,8 @@ def test_restart_file_continues_exactly(driver, tmp_path):
     b = case_writer.write_case(c, str(tmp_path / "restarted"))
     sa = _summary(_run(driver, a, "--steps", 4, "--dt", repr(c.dt)))
     s1 = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--write-state"))
-    assert os.path.getsize(os.path.join(b, s1["time_name"], "dugksState")) == 8 + 4 + 4 + 8 + 8 + 8 + 8 + 2 * 8 * c.n_cells * 64
+    header, dfs, record = 8 + 4 + 4 + 8 + 8 + 8 + 8, 2 * 8 * c.n_cells * 64, 8 * (9 * c.n_cells + 2)
+    assert os.path.getsize(os.path.join(b, s1["time_name"], "dugksState")) == header + dfs + record
     sb = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--restart", s1["time_name"]))
     assert sa["time_name"] == sb["time_name"]
     for name in ("rho", "U", "T", "q"):
@@ -132,3 +148,28 @@ def test_restart_rejects_another_mesh(driver, tmp_path):
     os.replace(os.path.join(b, s1["time_name"], "dugksState"), os.path.join(other, s1["time_name"], "dugksState"))
     r = _run(driver, other, "--steps", 1, "--dt", repr(c.dt), "--restart", s1["time_name"], check=False)
     assert r.returncode == 1 and "another mesh" in r.stderr
+
+
+@pytest.mark.gpu
+def test_adjustable_time_step_from_control_dict(driver, tmp_path):
+    # adjustTimeStep yes: each step runs CourantNo.H + setDeltaTvar.H on the
+    # device; the driver's steps equal Solver.step_adaptive's, and the run
+    # stops at endTime as Time::run does
+    c = cs.cavity_case(12, 8)
+    dt0 = 0.3 * c.dt
+    end = 6.0 * c.dt
+    control = {"startTime": 0.0, "endTime": end, "deltaT": dt0, "writeInterval": 1.0,
+               "adjustTimeStep": "yes", "maxCo": 0.5}
+    d = case_writer.write_case(c, str(tmp_path / "adjust"), control=control)
+    s = _summary(_run(driver, d))
+    ref = dl.Solver(c)
+    t, dt, n = 0.0, dt0, 0
+    while t < end - 0.5 * dt:
+        dt, _ = ref.step_adaptive(1, dt, 0.5, 1e15)
+        t += dt
+        n += 1
+    assert s["steps"] == n and s["dt"] == dt and s["time"] == t
+    m = ref.macros()
+    sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
+    rho = foamio.read_vol_field(os.path.join(d, s["time_name"], "rho"), c.n_cells, sizes)
+    np.testing.assert_allclose(rho["internal"], m["rho"], rtol=1e-14, atol=0)
