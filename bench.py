@@ -7,9 +7,13 @@ wall; FP64.  Synthetic mesh and initial state (uniform free stream).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One JSON line on rank 0.  Multi-GPU: replicas only (every rank advances
-its own copy of the workload; the step has no cross-rank exchange), so
-value = all ranks' cell-DV updates / the slowest rank's time, weak scaling.
+One JSON line on rank 0.  Multi-GPU, by default replicas (every rank
+advances its own copy of the workload; the step has no cross-rank
+exchange), so value = all ranks' cell-DV updates / the slowest rank's time,
+weak scaling.  --dv-shard splits one workload's DV rows over the ranks
+instead (NCCL all-reduce of the raw face and cell moments, two per step):
+value = the workload's cell-DV updates / the slowest rank's time, strong
+scaling.
 """
 from __future__ import annotations
 
@@ -44,6 +48,8 @@ def parse():
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
+    p.add_argument("--dv-shard", action="store_true",
+                   help="N>1: shard the DV rows of one workload over the ranks (NCCL) instead of replicas")
     return p.parse_args()
 
 
@@ -231,8 +237,16 @@ def main():
     from dugks_b200 import lib as dl
     case, cfg = build_case(args.workload, args.ndv1d)
     prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
-    solver = dl.Solver(case, precision=prec, device=local)
+    shard = None
+    if world > 1 and args.dv_shard:
+        from dugks_b200 import shard as sh
+        shard = sh.init_nccl_shard(rank, world)
+    solver = dl.Solver(case, precision=prec, device=local, shard=shard)
     nv, nc = solver.n_dv, case.n_cells
+    nv_loc = solver.n_dv_local
+    # whole-job rate: replicas each advance the whole workload; shards share one
+    job_rate = (lambda k, sec: nc * nv * k / sec) if shard is not None else \
+        (lambda k, sec: replica_rate(world, nc, nv, k, sec))
     K, W = args.steps, max(3, args.warmup)
 
     def barrier():
@@ -254,7 +268,7 @@ def main():
     barrier()
     clocks = sampler.stop() if sampler else None
     t_ms = max_over_ranks(float(stage[4]), dist)
-    value = replica_rate(world, nc, nv, K, t_ms / 1e3)
+    value = job_rate(K, t_ms / 1e3)
 
     # end to end through the public API with host buffers: each step is
     # fvDVM::evolution (dt passed by value) followed by the copy of the
@@ -265,26 +279,30 @@ def main():
         solver.step(1, case.dt)
         solver.macros()
     te = max_over_ranks(time.perf_counter() - te0, dist)
-    e2e = replica_rate(world, nc, nv, K, te)
+    e2e = job_rate(K, te)
 
     rs = 8 if prec == dl.FP64 else 4
     peak, peak_kind = measured_peaks()
     a_ms, b_ms = stage[0] / K, stage[2] / K
+    # per-launch figures of this rank's kernels (its DV block)
     if b_ms >= a_ms:
-        kname, kbytes, kms = "pass B (face relaxation, flux, update, cell moments)", 4 * rs * nc * nv, b_ms
+        kname, kbytes, kms = "pass B (face relaxation, flux, update, cell moments)", 4 * rs * nc * nv_loc, b_ms
         tpu = profiled_traffic("k_pass_b", args.precision) if args.workload == "ball" else None
     else:
-        kname, kbytes, kms = "pass A (reconstruction, face moments)", 2 * rs * nc * nv, a_ms
+        kname, kbytes, kms = "pass A (reconstruction, face moments)", 2 * rs * nc * nv_loc, a_ms
         tpu = profiled_traffic("k_pass_a", args.precision) if args.workload == "ball" else None
     achieved = kbytes / (kms / 1e3) / 1e9
-    traffic = tpu * nc * nv if tpu is not None else None
-    step_bytes = 6 * rs * nc * nv
+    traffic = tpu * nc * nv_loc if tpu is not None else None
+    step_bytes = 6 * rs * nc * nv_loc
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "strong" if shard is not None else "weak",
+        "vs_baseline": None,
         "dtype": "f64" if prec == dl.FP64 else "f32 storage / f64 moments", "data": "synthetic",
-        "config": dict(cfg, precision=args.precision, parallelism=f"replicas x{world}",
-                       l2="inputs larger than L2 (state %.2f GB)" % (4 * rs * nc * nv / 1e9)),
+        "config": dict(cfg, precision=args.precision,
+                       parallelism=f"dv-shard x{world} (NCCL all-reduce of raw moments)" if shard is not None
+                       else f"replicas x{world}",
+                       l2="inputs larger than L2 (state %.2f GB per GPU)" % (4 * rs * nc * nv_loc / 1e9)),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 72 * nc + 16},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -156,6 +156,50 @@ int dugks_mesh_geometry(int32_t n_points, const double* points, int32_t n_faces,
 int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas,
                  const dugks_bc* bc, const dugks_options* opt, dugks_handle** out);
 
+/* Velocity-space sharding (the reference's -dvParallel with fieldMPIreducer,
+ * fvDVM.C:381-383 and the reduceField calls of fvDVM.C:1241-1245,
+ * :1547-1552, :1738-1740).  Rank r of world W owns a contiguous block of DV
+ * rows (n_dv_1d DVs along x at fixed y, z): rows*r/W .. rows*(r+1)/W.  Its
+ * g~, h~ and face values cover those DVs only; the raw face moments (after
+ * the face reconstruction) and the raw cell moments (after the update) are
+ * summed over all ranks, so every rank holds the same macros, which equal
+ * the unsharded step's up to the summation order.  (The reference's own DV
+ * decomposition leaves the face heat flux unreduced, fvDVM.C:1353-1356; it
+ * is not followed there.)
+ *   use_nccl != 0: the library all-reduces with NCCL on its own stream inside
+ *       dugks_step, dugks_step_adaptive and dugks_set_state.  nccl_id is the
+ *       NCCL unique id rank 0 made with dugks_nccl_unique_id and the host
+ *       sent to every rank; dugks_create_sharded is collective (every rank
+ *       calls it) and each rank drives its own GPU.  NCCL is loaded at this
+ *       call (libnccl.so.2); without it the call fails with DUGKS_ERR_UNSUPPORTED.
+ *   use_nccl == 0: the host reduces, through dugks_shard_phase. */
+typedef struct dugks_dv_shard {
+    int32_t rank;
+    int32_t world;
+    int32_t use_nccl;
+    unsigned char nccl_id[128];
+} dugks_dv_shard;
+
+int dugks_nccl_unique_id(unsigned char id[128]);
+int dugks_create_sharded(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas,
+                         const dugks_bc* bc, const dugks_options* opt, const dugks_dv_shard* shard,
+                         dugks_handle** out);
+
+/* First global DV index and number of DVs this handle holds (all of them
+ * unless sharded).  dugks_get_state, dugks_set_state and dugks_get_df work
+ * on these DVs only; macros and face values are global on every rank. */
+int dugks_dv_range(const dugks_handle* h, int32_t* first_dv, int32_t* n_dv_local);
+
+/* One step of a sharded handle with host-side reduction, in three calls:
+ *   phase 0 (dt): face reconstruction and raw face moments of this shard;
+ *   phase 1: face macros, face relaxation, update, raw cell moments;
+ *   phase 2: cell macros; the step is complete.
+ * After phases 0 and 1, *part / *n_part are a DEVICE buffer of doubles that
+ * the host replaces, in place, by its sum over all shards before the next
+ * phase (the stream is synchronised at the end of each phase).  Every shard
+ * runs the same phases with the same dt. */
+int dugks_shard_phase(dugks_handle* h, int32_t phase, double dt, double** part, int64_t* n_part);
+
 /* fvDVM::fvDVM, second half: g~ = Maxwellian(rho,U,T), h~ = (K+3-D)RT g~,
  * wall inComingByRho, tau, q = 0, linear face velocity.
  * fvDVM.C:414-426, :578-624, :2115-2116.  U is [n_cells*3]. */

@@ -1,8 +1,12 @@
 // C ABI of the B200 DUGKS step (declarations and reference mapping in
 // include/dugks.h).  Owns the device layout and drives the kernels.
+#include <dlfcn.h>
+#include <nccl.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -63,6 +67,55 @@ dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
     return a;
 }
 
+// NCCL, opened on first use so that the library does not depend on it (and
+// does not clash with another NCCL a host process has loaded: dlopen of the
+// same soname returns that one)
+struct NcclApi {
+    ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
+    ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+    ncclResult_t (*all_reduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                               cudaStream_t) = nullptr;
+    ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+    const char* (*error_string)(ncclResult_t) = nullptr;
+    std::string error;
+};
+
+const NcclApi& nccl_api() {
+    static NcclApi api;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!lib) lib = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+        if (!lib) {
+            const char* e = dlerror();
+            api.error = std::string("cannot load NCCL: ") + (e ? e : "libnccl.so.2 not found");
+            return;
+        }
+        api.get_unique_id = reinterpret_cast<decltype(api.get_unique_id)>(dlsym(lib, "ncclGetUniqueId"));
+        api.comm_init_rank = reinterpret_cast<decltype(api.comm_init_rank)>(dlsym(lib, "ncclCommInitRank"));
+        api.all_reduce = reinterpret_cast<decltype(api.all_reduce)>(dlsym(lib, "ncclAllReduce"));
+        api.comm_destroy = reinterpret_cast<decltype(api.comm_destroy)>(dlsym(lib, "ncclCommDestroy"));
+        api.error_string = reinterpret_cast<decltype(api.error_string)>(dlsym(lib, "ncclGetErrorString"));
+        if (!api.get_unique_id || !api.comm_init_rank || !api.all_reduce || !api.comm_destroy || !api.error_string) {
+            api.error = "NCCL library lacks a needed symbol";
+            api.get_unique_id = nullptr;
+        }
+    });
+    return api;
+}
+
+// the sum over all shards of n doubles at buf (device), on the handle's stream
+int shard_allreduce(dugks_handle* h, double* buf, size_t n) {
+    if (!h->shard_nccl || n == 0) return DUGKS_OK;
+    const NcclApi& api = nccl_api();
+    const ncclResult_t r = api.all_reduce(buf, buf, n, ncclDouble, ncclSum, static_cast<ncclComm_t>(h->nccl_comm),
+                                          h->stream);
+    if (r != ncclSuccess) return set_error(h, DUGKS_ERR_CUDA, std::string("ncclAllReduce: ") + api.error_string(r));
+    return DUGKS_OK;
+}
+
+bool sharded(const dugks_handle* h) { return h->shard_world > 1 || h->shard_nccl; }
+
 int check_device_errors(dugks_handle* h) {
     int err[4] = {0, 0, 0, 0};
     CUDA_TRY(h, cudaMemcpyAsync(err, h->ds.err, sizeof err, cudaMemcpyDeviceToHost, h->stream));
@@ -85,8 +138,8 @@ void dugks_default_options(dugks_options* opt) {
     opt->ls_weighting = DUGKS_LS_MAGSF;
 }
 
-int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
-                 const dugks_options* opt_in, dugks_handle** out) {
+static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
+                       const dugks_options* opt_in, const dugks_dv_shard* shard, dugks_handle** out) {
     if (!out) return DUGKS_ERR_ARG;
     *out = nullptr;
     if (!mesh || !dv || !gas || !bc) return DUGKS_ERR_ARG;
@@ -205,12 +258,25 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     // whole DV rows (n1d DVs along x at fixed y, z): the passes walk a row in
     // batches and factor the x direction out of their sums
     const int rows = h->nv / h->n1d;
+    // velocity-space shard: this device's block of DV rows
+    int row0 = 0, row1 = rows;
+    if (shard) {
+        if (shard->world < 1 || shard->rank < 0 || shard->rank >= shard->world)
+            return fail(DUGKS_ERR_ARG, "dugks_create_sharded: bad rank or world");
+        if (shard->world > rows)
+            return fail(DUGKS_ERR_ARG, "dugks_create_sharded: more shards than DV rows (" + std::to_string(rows) + ")");
+        h->shard_rank = shard->rank;
+        h->shard_world = shard->world;
+        row0 = static_cast<int>(static_cast<int64_t>(rows) * shard->rank / shard->world);
+        row1 = static_cast<int>(static_cast<int64_t>(rows) * (shard->rank + 1) / shard->world);
+    }
+    const int rows_loc = row1 - row0;
     int chunks = opt.dv_chunks > 0 ? opt.dv_chunks : (2 * sms + h->tiling.n_tiles - 1) / h->tiling.n_tiles;
-    chunks = std::max(1, std::min(chunks, rows));
+    chunks = std::max(1, std::min(chunks, rows_loc));
     h->chunks = chunks;
     h->chunk_begin.resize(chunks + 1);
     for (int c = 0; c <= chunks; ++c)
-        h->chunk_begin[c] = static_cast<int32_t>((static_cast<int64_t>(rows) * c) / chunks);
+        h->chunk_begin[c] = row0 + static_cast<int32_t>((static_cast<int64_t>(rows_loc) * c) / chunks);
 
     // ---- device layout ----
     const dugks::Tiling& t = h->tiling;
@@ -226,6 +292,9 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dm.nIF = nIF;
     dm.nBF = nBF;
     dm.nv = h->nv;
+    dm.row_base = row0;
+    dm.dv_base = row0 * h->n1d;
+    dm.nv_loc = rows_loc * h->n1d;
     dm.prec = h->precision;
     dm.n1d = h->n1d;
     dm.n_tiles = t.n_tiles;
@@ -291,8 +360,8 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dm.bS = d_bS;
     dugks::DevState& ds = h->ds;
     const size_t rs = real_size(h);
-    const size_t nvc = static_cast<size_t>(h->nv) * nC;
-    const size_t nfv = static_cast<size_t>(h->nv) * std::max(dm.n_items, 1);
+    const size_t nvc = static_cast<size_t>(dm.nv_loc) * nC;
+    const size_t nfv = static_cast<size_t>(dm.nv_loc) * std::max(dm.n_items, 1);
     unsigned char* p;
     for (int i = 0; i < 2; ++i) {
         if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
@@ -325,7 +394,51 @@ int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas
     dugks::StepArgs a = make_args(h, 0.0, 0.0);
     ce = dugks::configure_kernels(h->precision, a);
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, std::string("configure kernels: ") + cudaGetErrorString(ce));
+    if (shard && shard->use_nccl) {
+        // collective: every rank of the shard set makes this call
+        const NcclApi& api = nccl_api();
+        if (!api.get_unique_id) return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_sharded: " + api.error);
+        ncclUniqueId id;
+        static_assert(sizeof id == sizeof shard->nccl_id, "NCCL unique id size");
+        std::memcpy(&id, shard->nccl_id, sizeof id);
+        ncclComm_t comm = nullptr;
+        const ncclResult_t r = api.comm_init_rank(&comm, shard->world, id, shard->rank);
+        if (r != ncclSuccess) return fail(DUGKS_ERR_CUDA, std::string("ncclCommInitRank: ") + api.error_string(r));
+        h->nccl_comm = comm;
+        h->shard_nccl = true;
+    }
     *out = h;
+    return DUGKS_OK;
+}
+
+int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
+                 const dugks_options* opt, dugks_handle** out) {
+    return create_impl(mesh, dv, gas, bc, opt, nullptr, out);
+}
+
+int dugks_create_sharded(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
+                         const dugks_options* opt, const dugks_dv_shard* shard, dugks_handle** out) {
+    if (!shard) {
+        if (out) *out = nullptr;
+        return DUGKS_ERR_ARG;
+    }
+    return create_impl(mesh, dv, gas, bc, opt, shard, out);
+}
+
+int dugks_nccl_unique_id(unsigned char id[128]) {
+    if (!id) return DUGKS_ERR_ARG;
+    const NcclApi& api = nccl_api();
+    if (!api.get_unique_id) return DUGKS_ERR_UNSUPPORTED;
+    ncclUniqueId u;
+    if (api.get_unique_id(&u) != ncclSuccess) return DUGKS_ERR_CUDA;
+    std::memcpy(id, &u, sizeof u);
+    return DUGKS_OK;
+}
+
+int dugks_dv_range(const dugks_handle* h, int32_t* first_dv, int32_t* n_dv_local) {
+    if (!h || !first_dv || !n_dv_local) return DUGKS_ERR_ARG;
+    *first_dv = h->dm.dv_base;
+    *n_dv_local = h->dm.nv_loc;
     return DUGKS_OK;
 }
 
@@ -412,9 +525,65 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     return DUGKS_OK;
 }
 
+// the adaptive time step between the face combine and pass B
+struct AdaptCall {
+    const double* dt_in;
+    double* dt_out;
+    double* hist;
+    double max_co, max_dt;
+};
+
+// One step's stages on the handle's stream.  A sharded handle sums its DV
+// chunks and all-reduces the raw moments before each combine, which then
+// read one chunk.  sev (5 events, or null) are recorded before pass A and
+// after each stage; adapt (or null) runs after the face combine.
+static int enqueue_step(dugks_handle* h, const dugks::StepArgs& a, cudaEvent_t* sev, int* launches,
+                        const AdaptCall* adapt) {
+    const bool sh = sharded(h);
+    dugks::StepArgs one = a;
+    if (sh) one.chunks = 1;
+    if (sev) CUDA_TRY(h, cudaEventRecord(sev[0], h->stream));
+    CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_A, h->stream, launches));
+    if (sev) CUDA_TRY(h, cudaEventRecord(sev[1], h->stream));
+    if (sh) {
+        const size_t n = static_cast<size_t>(h->dm.n_items) * dugks::kNM;
+        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partF, h->chunks, n, h->stream));
+        if (h->chunks > 1) ++*launches;
+        const int st = shard_allreduce(h, h->ds.partF, n);
+        if (st) return st;
+    }
+    CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_FACE_COMBINE, h->stream, launches));
+    if (adapt) {
+        CUDA_TRY(h, dugks::launch_adapt(a, adapt->dt_in, adapt->dt_out, adapt->hist, adapt->max_co, adapt->max_dt,
+                                        h->stream));
+        ++*launches;
+    }
+    if (sev) CUDA_TRY(h, cudaEventRecord(sev[2], h->stream));
+    CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, launches));
+    if (sev) CUDA_TRY(h, cudaEventRecord(sev[3], h->stream));
+    if (sh) {
+        const size_t n = static_cast<size_t>(h->nC) * dugks::kNM;
+        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partC, h->chunks, n, h->stream));
+        if (h->chunks > 1) ++*launches;
+        const int st = shard_allreduce(h, h->ds.partC, n);
+        if (st) return st;
+    }
+    CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, launches));
+    if (sev) CUDA_TRY(h, cudaEventRecord(sev[4], h->stream));
+    return DUGKS_OK;
+}
+
+static int require_internal_reduction(dugks_handle* h, const char* what) {
+    if (sharded(h) && !h->shard_nccl)
+        return set_error(h, DUGKS_ERR_STATE,
+                         std::string(what) + ": a handle sharded without NCCL steps through dugks_shard_phase");
+    return DUGKS_OK;
+}
+
 static int run_steps(dugks_handle* h, int32_t n_steps, const double* dt, double* stage_ms) {
     if (!h) return DUGKS_ERR_ARG;
     if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_step before dugks_set_macros");
+    if (int st = require_internal_reduction(h, "dugks_step")) return st;
     if (n_steps < 0 || (n_steps > 0 && !dt)) return set_error(h, DUGKS_ERR_ARG, "dugks_step: bad arguments");
     for (int i = 0; i < n_steps; ++i)
         if (!(dt[i] > 0) || !std::isfinite(dt[i])) return set_error(h, DUGKS_ERR_ARG, "dugks_step: dt must be > 0");
@@ -435,14 +604,8 @@ static int run_steps(dugks_handle* h, int32_t n_steps, const double* dt, double*
             ++launches;
         }
         CUDA_TRY(h, cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream));
-        if (!stage_ms) {
-            CUDA_TRY(h, dugks::launch_step(a, h->precision, h->stream, &launches));
-        } else {
-            CUDA_TRY(h, cudaEventRecord(sev[0], h->stream));
-            for (int stg = 0; stg < 4; ++stg) {
-                CUDA_TRY(h, dugks::launch_stage(a, h->precision, stg, h->stream, &launches));
-                CUDA_TRY(h, cudaEventRecord(sev[stg + 1], h->stream));
-            }
+        if (const int st = enqueue_step(h, a, stage_ms ? sev : nullptr, &launches, nullptr)) return st;
+        if (stage_ms) {
             CUDA_TRY(h, cudaEventSynchronize(sev[4]));
             for (int stg = 0; stg < 4; ++stg) {
                 float ms = 0;
@@ -477,6 +640,7 @@ int dugks_step_timed(dugks_handle* h, int32_t n_steps, const double* dt, double*
 int dugks_step_adaptive(dugks_handle* h, int32_t n_steps, const dugks_adapt* adapt, double* dt, double* dt_history) {
     if (!h) return DUGKS_ERR_ARG;
     if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_step_adaptive before dugks_set_macros");
+    if (int st = require_internal_reduction(h, "dugks_step_adaptive")) return st;
     if (n_steps < 0 || !adapt || !dt || !(*dt > 0) || !std::isfinite(*dt) || !(adapt->max_co > 0) ||
         !(adapt->max_delta_t > 0))
         return set_error(h, DUGKS_ERR_ARG, "dugks_step_adaptive: bad arguments");
@@ -503,13 +667,9 @@ int dugks_step_adaptive(dugks_handle* h, int32_t n_steps, const dugks_adapt* ada
         a.dtp = slot(k);
         a.dtnp = slot(k + 1);
         CUDA_TRY(h, cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream));
-        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_A, h->stream, &launches));
-        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_FACE_COMBINE, h->stream, &launches));
-        CUDA_TRY(h, dugks::launch_adapt(a, slot(k), slot(k + 1), k < n_steps ? h->d_hist + k : nullptr,
-                                        adapt->max_co, adapt->max_delta_t, h->stream));
-        ++launches;
-        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, &launches));
-        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, &launches));
+        const AdaptCall ac{slot(k), slot(k + 1), k < n_steps ? h->d_hist + k : nullptr, adapt->max_co,
+                           adapt->max_delta_t};
+        if (const int st = enqueue_step(h, a, nullptr, &launches, &ac)) return st;
         h->ds.cur = 1 - h->ds.cur;
         h->steps_done++;
     }
@@ -525,6 +685,55 @@ int dugks_step_adaptive(dugks_handle* h, int32_t n_steps, const dugks_adapt* ada
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->last_step_ms = ms;
     return st;
+}
+
+int dugks_shard_phase(dugks_handle* h, int32_t phase, double dt, double** part, int64_t* n_part) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_shard_phase before dugks_set_macros");
+    if (h->shard_nccl) return set_error(h, DUGKS_ERR_STATE, "dugks_shard_phase: the handle reduces with NCCL");
+    if (phase != h->shard_phase_next)
+        return set_error(h, DUGKS_ERR_STATE, "dugks_shard_phase: expected phase " + std::to_string(h->shard_phase_next));
+    if (phase < 2 && (!part || !n_part)) return set_error(h, DUGKS_ERR_ARG, "dugks_shard_phase: null output");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    int launches = 0;
+    if (phase == 0) {
+        if (!(dt > 0) || !std::isfinite(dt)) return set_error(h, DUGKS_ERR_ARG, "dugks_shard_phase: dt must be > 0");
+        h->shard_dt = dt;
+        const dugks::StepArgs a = make_args(h, dt, 0.0);
+        if (h->cellrec_dt != dt) {
+            CUDA_TRY(h, dugks::launch_cell_prep(a, h->stream));
+            ++launches;
+        }
+        CUDA_TRY(h, cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream));
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_A, h->stream, &launches));
+        const size_t n = static_cast<size_t>(h->dm.n_items) * dugks::kNM;
+        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partF, h->chunks, n, h->stream));
+        if (h->chunks > 1) ++launches;
+        *part = h->ds.partF;
+        *n_part = static_cast<int64_t>(n);
+    } else if (phase == 1) {
+        const dugks::StepArgs a = make_args(h, h->shard_dt, 0.0);
+        dugks::StepArgs one = a;
+        one.chunks = 1;
+        CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_FACE_COMBINE, h->stream, &launches));
+        CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, &launches));
+        const size_t n = static_cast<size_t>(h->nC) * dugks::kNM;
+        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partC, h->chunks, n, h->stream));
+        if (h->chunks > 1) ++launches;
+        *part = h->ds.partC;
+        *n_part = static_cast<int64_t>(n);
+    } else {
+        dugks::StepArgs one = make_args(h, h->shard_dt, 0.0);
+        one.chunks = 1;
+        CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, &launches));
+        h->cellrec_dt = 0.0;   // the next phase 0 sets the relax factors for its dt
+        h->ds.cur = 1 - h->ds.cur;
+        h->steps_done++;
+    }
+    h->launches += launches;
+    h->shard_phase_next = (phase + 1) % 3;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return phase == 2 ? check_device_errors(h) : DUGKS_OK;
 }
 
 int64_t dugks_kernel_launches(const dugks_handle* h) { return h ? h->launches : 0; }
@@ -642,7 +851,7 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
     if (!h || (n > 0 && (!cells || !g_out))) return set_error(h, DUGKS_ERR_ARG, "dugks_get_df: bad arguments");
     if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_df before dugks_set_macros");
     const size_t rs = real_size(h);
-    std::vector<unsigned char> col(static_cast<size_t>(h->nv) * rs);
+    std::vector<unsigned char> col(static_cast<size_t>(h->dm.nv_loc) * rs);
     for (int i = 0; i < n; ++i) {
         if (cells[i] < 0 || cells[i] >= h->nC) return set_error(h, DUGKS_ERR_ARG, "dugks_get_df: cell out of range");
         const int c = h->tiling.iperm[cells[i]];
@@ -651,10 +860,10 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
             if (!dst) continue;
             const unsigned char* src =
                 static_cast<const unsigned char*>(which == 0 ? h->ds.g[h->ds.cur] : h->ds.h[h->ds.cur]) + c * rs;
-            CUDA_TRY(h, cudaMemcpy2DAsync(col.data(), rs, src, static_cast<size_t>(h->nC) * rs, rs, h->nv,
+            CUDA_TRY(h, cudaMemcpy2DAsync(col.data(), rs, src, static_cast<size_t>(h->nC) * rs, rs, h->dm.nv_loc,
                                           cudaMemcpyDeviceToHost, h->stream));
             CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            for (int d = 0; d < h->nv; ++d) {
+            for (int d = 0; d < h->dm.nv_loc; ++d) {
                 double v;
                 if (rs == sizeof(double)) std::memcpy(&v, &col[d * rs], sizeof v);
                 else {
@@ -662,7 +871,7 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
                     std::memcpy(&fv, &col[d * rs], sizeof fv);
                     v = fv;
                 }
-                dst[static_cast<size_t>(i) * h->nv + d] = v;
+                dst[static_cast<size_t>(i) * h->dm.nv_loc + d] = v;
             }
         }
     }
@@ -673,7 +882,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
     if (!h) return DUGKS_ERR_ARG;
     if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "state access before dugks_set_macros");
     const size_t rs = real_size(h);
-    const size_t nvc = static_cast<size_t>(h->nv) * h->nC;
+    const size_t nvc = static_cast<size_t>(h->dm.nv_loc) * h->nC;
     std::vector<unsigned char> buf(nvc * rs);
     const std::vector<int32_t>& perm = h->tiling.perm;
     for (int which = 0; which < 2; ++which) {
@@ -682,7 +891,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
             double* dst = which == 0 ? g : hh;
             if (!dst) continue;
             CUDA_TRY(h, cudaMemcpy(buf.data(), dev, nvc * rs, cudaMemcpyDeviceToHost));
-            for (int d = 0; d < h->nv; ++d)
+            for (int d = 0; d < h->dm.nv_loc; ++d)
                 for (int c = 0; c < h->nC; ++c) {
                     const size_t s = static_cast<size_t>(d) * h->nC + c;
                     const size_t o = static_cast<size_t>(d) * h->nC + perm[c];
@@ -696,7 +905,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
         } else {
             const double* src = which == 0 ? gi : hi;
             if (!src) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: null array");
-            for (int d = 0; d < h->nv; ++d)
+            for (int d = 0; d < h->dm.nv_loc; ++d)
                 for (int c = 0; c < h->nC; ++c) {
                     const size_t s = static_cast<size_t>(d) * h->nC + c;
                     const size_t o = static_cast<size_t>(d) * h->nC + perm[c];
@@ -715,11 +924,15 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
 int dugks_get_state(dugks_handle* h, double* g, double* hh) { return state_io(h, g, hh, nullptr, nullptr, true); }
 
 int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double dt_prev) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (int st = require_internal_reduction(h, "dugks_set_state")) return st;
     int st = state_io(h, nullptr, nullptr, g, hh, false);
     if (st) return st;
     if (!(dt_prev > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: dt_prev must be > 0");
     dugks::StepArgs a = make_args(h, dt_prev, 0.0);
-    CUDA_TRY(h, dugks::launch_state_macros(a, h->precision, h->stream));
+    CUDA_TRY(h, dugks::launch_state_moments(a, h->precision, h->stream));
+    if ((st = shard_allreduce(h, h->ds.partC, static_cast<size_t>(h->nC) * dugks::kNM))) return st;
+    CUDA_TRY(h, dugks::launch_cell_combine_one(a, 0.0, h->stream));
     h->launches += 2;
     h->cellrec_dt = 0;
     return check_device_errors(h);
@@ -739,6 +952,7 @@ void dugks_destroy(dugks_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->nccl_comm) nccl_api().comm_destroy(static_cast<ncclComm_t>(h->nccl_comm));
     for (void* p : h->allocations) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);

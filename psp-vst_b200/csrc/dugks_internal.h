@@ -69,6 +69,9 @@ struct DevMesh {
     int D, K;
     double R, Pr, omega, Tref, muRef;
     int nC, nIF, nBF, nv, n_tiles;
+    // DVs this device holds: global DVs dv_base .. dv_base + nv_loc - 1, the
+    // DV rows row_base ..; the state and face-value arrays are [nv_loc][..]
+    int nv_loc, dv_base, row_base;
     int prec;              // dugks_precision of the state and tables
     // DV set
     const double* xi;      // [nv*3]
@@ -171,7 +174,13 @@ struct dugks_handle {
     std::vector<double> C, V, Cf, Sf, weights, dc, lsP, lsN, lsB;
     dugks::Tiling tiling;
     int chunks = 1;
-    std::vector<int32_t> chunk_begin;   // DV chunk boundaries in DV rows [chunks+1]
+    std::vector<int32_t> chunk_begin;   // DV chunk boundaries in global DV rows [chunks+1]
+    // velocity-space shard (world 1: the whole DV set)
+    int shard_rank = 0, shard_world = 1;
+    bool shard_nccl = false;
+    void* nccl_comm = nullptr;          // ncclComm_t
+    int shard_phase_next = 0;           // dugks_shard_phase: the phase expected next
+    double shard_dt = 0;                // dugks_shard_phase: dt of the step in progress
     // device
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -9,6 +9,8 @@
 //   cell combine  cell macros and the next step's cell coefficients
 // The state g~, h~ is DV-major [dv][cell] (cells renumbered along a Morton
 // curve), double-buffered between steps.
+#include <algorithm>
+
 #include "dugks_device.cuh"
 
 namespace dugks {
@@ -239,11 +241,11 @@ __global__ void k_cell_prep(const StepArgs a) {
 template <typename Real>
 __global__ void k_init_state(const StepArgs a) {
     const DevMesh& m = a.dm;
-    const size_t n = static_cast<size_t>(m.nv) * m.nC;
+    const size_t n = static_cast<size_t>(m.nv_loc) * m.nC;
     const double K3D = m.K + 3.0 - m.D;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int d = static_cast<int>(i / m.nC), c = static_cast<int>(i % m.nC);
+        const int d = m.dv_base + static_cast<int>(i / m.nC), c = static_cast<int>(i % m.nC);
         const double* cm = a.ds.cm + static_cast<size_t>(c) * 9;
         const double RT = m.R * cm[4];
         const double cx = cm[1] - m.xi[3 * d], cy = cm[2] - m.xi[3 * d + 1], cz = cm[3] - m.xi[3 * d + 2];
@@ -318,7 +320,7 @@ __global__ void k_adapt(const double* co, const double* dt_in, double* dt_out, d
 }
 
 // raw cell moments of the current state, one thread per cell looping over
-// all DVs (rows are contiguous in cells, so a warp reads coalesced)
+// this device's DVs (rows are contiguous in cells, so a warp reads coalesced)
 template <int D, typename Real>
 __global__ void k_state_moments(const StepArgs a) {
     const DevMesh& m = a.dm;
@@ -328,14 +330,26 @@ __global__ void k_state_moments(const StepArgs a) {
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
     double acc[15];
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
-    for (int d = 0; d < m.nv; ++d) {
+    for (int dl = 0; dl < m.nv_loc; ++dl) {
+        const int d = m.dv_base + dl;
         const double xi[3] = {__ldg(m.xi + 3 * d), __ldg(m.xi + 3 * d + 1), __ldg(m.xi + 3 * d + 2)};
         const double xi2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
-        const size_t idx = static_cast<size_t>(d) * m.nC + c;
+        const size_t idx = static_cast<size_t>(dl) * m.nC + c;
         accum<D>(acc, __ldg(m.w + d), xi, xi2, double(g[idx]), double(h[idx]));
     }
     double* p = a.ds.partC + static_cast<size_t>(c) * kNM;
     for (int j = 0; j < 15; ++j) p[j] = acc[j];
+}
+
+// part[0][i] = sum over chunks of part[ch][i], in chunk order (the order the
+// combine kernels sum them in), for the cross-shard reduction
+__global__ void k_sum_chunks(double* part, int chunks, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        double v = part[i];
+        for (int ch = 1; ch < chunks; ++ch) v += part[static_cast<size_t>(ch) * n + i];
+        part[i] = v;
+    }
 }
 
 }  // namespace
@@ -385,7 +399,7 @@ cudaError_t launch_step(const StepArgs& a, int precision, cudaStream_t s, int* l
     return cudaSuccess;
 }
 
-cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s) {
+cudaError_t launch_state_moments(const StepArgs& a, int precision, cudaStream_t s) {
     const int tb = 128, nb = (a.dm.nC + tb - 1) / tb;
     if (precision == DUGKS_FP64) {
         if (a.dm.D == 3) k_state_moments<3, double><<<nb, tb, 0, s>>>(a);
@@ -394,10 +408,27 @@ cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s
         if (a.dm.D == 3) k_state_moments<3, float><<<nb, tb, 0, s>>>(a);
         else k_state_moments<2, float><<<nb, tb, 0, s>>>(a);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_combine_one(const StepArgs& a, double dt_next, cudaStream_t s) {
     StepArgs one = a;
     one.chunks = 1;
     const Consts k = make_consts(a.dm, a.dt);
-    k_cell_combine<<<(a.dm.nC + 255) / 256, 256, 0, s>>>(one, k, 0.0);
+    k_cell_combine<<<(a.dm.nC + 255) / 256, 256, 0, s>>>(one, k, dt_next);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s) {
+    cudaError_t e = launch_state_moments(a, precision, s);
+    return e != cudaSuccess ? e : launch_cell_combine_one(a, 0.0, s);
+}
+
+cudaError_t launch_sum_chunks(double* part, int chunks, size_t n, cudaStream_t s) {
+    if (chunks <= 1 || n == 0) return cudaSuccess;
+    const int tb = 256;
+    const int nb = static_cast<int>(std::min<size_t>((n + tb - 1) / tb, 148 * 16));
+    k_sum_chunks<<<nb, tb, 0, s>>>(part, chunks, n);
     return cudaGetLastError();
 }
 

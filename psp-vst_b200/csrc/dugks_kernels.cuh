@@ -38,6 +38,12 @@ cudaError_t launch_state_macros(const StepArgs& a, int precision, cudaStream_t s
 // dt of the next step from the Courant number of this step's faces (in
 // ds.co) and dt_in, as src/setDeltaTvar.H:34-48 adjusts it; also stored to
 // *hist when hist is not null
+// raw cell moments of the state (this device's DVs) into partC chunk 0, and
+// the cell macros and records from partC chunk 0
+cudaError_t launch_state_moments(const StepArgs& a, int precision, cudaStream_t s);
+cudaError_t launch_cell_combine_one(const StepArgs& a, double dt_next, cudaStream_t s);
+// partial moments of all chunks summed into chunk 0 (n doubles per chunk)
+cudaError_t launch_sum_chunks(double* part, int chunks, size_t n, cudaStream_t s);
 // cell records and Maxwellian tables rebuilt from the cell macros
 cudaError_t launch_cell_records(const StepArgs& a, cudaStream_t s);
 cudaError_t launch_adapt(const StepArgs& a, const double* dt_in, double* dt_out, double* hist, double max_co,

@@ -88,7 +88,8 @@ __device__ __forceinline__ TileRange tile_range(const DevMesh& m, const int32_t*
     return t;
 }
 
-// position of batch k of a chunk: first x index, width, first DV, row indices
+// position of batch k of a chunk: first x index, width, first DV of this
+// device's DV block (the state and face-value row), row indices
 struct BatchPos {
     int ix0, nb, d0, iy, iz;
 };
@@ -97,8 +98,10 @@ struct BatchPos {
 // then the next row) without integer divisions per batch
 template <int D, int NB>
 struct BatchWalk {
-    int row, iy, iz, kb, nbr, n1d;
-    __device__ __forceinline__ BatchWalk(int r0, int n) : row(r0), kb(0), nbr((n + NB - 1) / NB), n1d(n) {
+    int row, iy, iz, kb, nbr, n1d, rb;
+    // r0: first global row of the chunk; base: first global row this device holds
+    __device__ __forceinline__ BatchWalk(int r0, int n, int base)
+        : row(r0), kb(0), nbr((n + NB - 1) / NB), n1d(n), rb(base) {
         iy = D == 3 ? r0 % n : r0;
         iz = D == 3 ? r0 / n : 0;
     }
@@ -106,7 +109,7 @@ struct BatchWalk {
         BatchPos p;
         p.ix0 = kb * NB;
         p.nb = min(NB, n1d - p.ix0);
-        p.d0 = row * n1d + p.ix0;
+        p.d0 = (row - rb) * n1d + p.ix0;
         p.iy = iy;
         p.iz = iz;
         return p;
@@ -632,7 +635,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
 
-    BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
+    BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) stage0<D, Real, NB, FULL>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
     for (int k = 0; k < nbt; ++k, walk.next()) {
@@ -880,7 +883,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     constexpr int H = (NB + kParts0 - 1) / kParts0;
     Real pg[H], ph[H];
     double pe[H];
-    BatchWalk<D, NB> walk(t.r0, m.n1d), ahead(t.r0, m.n1d);
+    BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
         if (has_item) stage_items<Real, NB, FULL>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);

@@ -61,6 +61,47 @@ class Adapt(C.Structure):
     _fields_ = [("max_co", C.c_double), ("max_delta_t", C.c_double)]
 
 
+class Shard(C.Structure):
+    """Velocity-space shard of a solver (dugks_dv_shard): rank of world;
+    use_nccl with the NCCL unique id rank 0 made (nccl_unique_id())."""
+    _fields_ = [("rank", C.c_int32), ("world", C.c_int32), ("use_nccl", C.c_int32), ("nccl_id", C.c_ubyte * 128)]
+
+
+def shard(rank: int, world: int, nccl_id: bytes | None = None) -> Shard:
+    s = Shard(rank, world, 1 if nccl_id is not None else 0)
+    if nccl_id is not None:
+        if len(nccl_id) != 128:
+            raise ValueError("an NCCL unique id is 128 bytes")
+        C.memmove(s.nccl_id, nccl_id, 128)
+    return s
+
+
+def _load_torch_nccl() -> None:
+    # The library opens libnccl.so.2 by soname when a shard uses NCCL; load
+    # torch (and with it the NCCL it was built with) first, so that the
+    # process holds one NCCL and torch.distributed can still start.
+    try:
+        import torch  # noqa: F401
+    except ImportError:
+        pass
+
+
+def nccl_unique_id() -> bytes:
+    """A new NCCL unique id (rank 0 makes it and sends it to the other ranks)."""
+    _load_torch_nccl()
+    buf = (C.c_ubyte * 128)()
+    st = load().dugks_nccl_unique_id(buf)
+    if st != 0:
+        raise DugksError(st, "ncclGetUniqueId failed or NCCL is not available")
+    return bytes(buf)
+
+
+def dv_rows(n_rows: int, rank: int, world: int) -> tuple[int, int]:
+    """The DV rows rank owns: rows*rank/world .. rows*(rank+1)/world, as
+    dugks_create_sharded assigns them."""
+    return n_rows * rank // world, n_rows * (rank + 1) // world
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("ls_weighting", C.c_int32), ("device", C.c_int32),
                 ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("reserved", C.c_int32 * 11)]
@@ -88,6 +129,11 @@ SIGNATURES = {
     "dugks_get_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
+    "dugks_nccl_unique_id": (C.c_int, [C.POINTER(C.c_ubyte)]),
+    "dugks_create_sharded": (C.c_int, [C.POINTER(Mesh), C.POINTER(DVSet), C.POINTER(Gas), C.POINTER(BC),
+                                       C.POINTER(Options), C.POINTER(Shard), C.POINTER(C.c_void_p)]),
+    "dugks_dv_range": (C.c_int, [C.c_void_p, _i32p, _i32p]),
+    "dugks_shard_phase": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.POINTER(_dp), _i64p]),
     "dugks_last_step_ms": (C.c_int, [C.c_void_p, _dp]),
     "dugks_step_timed": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "dugks_kernel_launches": (C.c_int64, [C.c_void_p]),
@@ -149,7 +195,7 @@ class Solver:
     """fvDVM-shaped wrapper over one dugks_handle."""
 
     def __init__(self, case, precision: int = FP64, ls_weighting: int = LS_MAGSF, device: int = 0,
-                 tile_cells: int = 0, dv_chunks: int = 0):
+                 tile_cells: int = 0, dv_chunks: int = 0, shard: Shard | None = None):
         self.lib = load()
         self.case = case
         fc = case.flat
@@ -188,14 +234,23 @@ class Solver:
         opt.tile_cells = tile_cells
         opt.dv_chunks = dv_chunks
         h = C.c_void_p()
-        st = self.lib.dugks_create(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas), C.byref(self.bc),
-                                   C.byref(opt), C.byref(h))
+        if shard is None:
+            st = self.lib.dugks_create(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas), C.byref(self.bc),
+                                       C.byref(opt), C.byref(h))
+        else:
+            if shard.use_nccl:
+                _load_torch_nccl()
+            st = self.lib.dugks_create_sharded(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas),
+                                               C.byref(self.bc), C.byref(opt), C.byref(shard), C.byref(h))
         self.h = h
         if st != 0:
             msg = self.lib.dugks_last_error(h).decode() if h.value else "dugks_create failed"
             self.close()
             raise DugksError(st, msg)
         self.n_dv = self.lib.dugks_n_dv(self.h)
+        first, nloc = C.c_int32(), C.c_int32()
+        self._check(self.lib.dugks_dv_range(self.h, C.byref(first), C.byref(nloc)))
+        self.dv_first, self.n_dv_local = first.value, nloc.value
         self.set_macros(case.rho0, case.U0, case.T0)
 
     def _check(self, st):
@@ -223,6 +278,13 @@ class Solver:
         hist = np.zeros(max(n, 1))
         self._check(self.lib.dugks_step_adaptive(self.h, n, C.byref(ad), C.byref(d), ptr(hist)))
         return d.value, hist[:n]
+
+    def shard_phase(self, phase: int, dt: float = 0.0) -> tuple[int, int]:
+        """dugks_shard_phase: (device address, count) of the doubles the host
+        sums over all shards after phases 0 and 1; (0, 0) after phase 2."""
+        p, n = _dp(), C.c_int64()
+        self._check(self.lib.dugks_shard_phase(self.h, phase, dt, C.byref(p), C.byref(n)))
+        return (C.cast(p, C.c_void_p).value or 0, n.value) if phase < 2 else (0, 0)
 
     def step_timed(self, n: int, dt) -> np.ndarray:
         """n steps with CUDA events around every stage: [passA, face combine,
@@ -266,14 +328,14 @@ class Solver:
 
     def df(self, cells) -> tuple[np.ndarray, np.ndarray]:
         cells = np.ascontiguousarray(cells, dtype=np.int32)
-        g = np.zeros((len(cells), self.n_dv))
-        hh = np.zeros((len(cells), self.n_dv))
+        g = np.zeros((len(cells), self.n_dv_local))
+        hh = np.zeros((len(cells), self.n_dv_local))
         self._check(self.lib.dugks_get_df(self.h, ptr(cells, C.c_int32), len(cells), ptr(g), ptr(hh)))
         return g, hh
 
     def state(self) -> tuple[np.ndarray, np.ndarray]:
-        g = np.zeros((self.n_dv, self.case.n_cells))
-        hh = np.zeros((self.n_dv, self.case.n_cells))
+        g = np.zeros((self.n_dv_local, self.case.n_cells))
+        hh = np.zeros((self.n_dv_local, self.case.n_cells))
         self._check(self.lib.dugks_get_state(self.h, ptr(g), ptr(hh)))
         return g, hh
 
