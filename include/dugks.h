@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define DUGKS_ABI_VERSION 1
+#define DUGKS_ABI_VERSION 2
 
 typedef enum dugks_status {
     DUGKS_OK = 0,
@@ -53,12 +53,34 @@ typedef enum dugks_status {
 
 /* Boundary patch types.  The reference selects the g/h surface patch type
  * from the rho patch type (discreteVelocity::setBCtype,
- * src/fvDVM/discreteVelocity/discreteVelocity.C:188-195):
- *   rho calculatedMaxwell -> maxwellWall  (diffuse Maxwell wall)
- *   rho farField          -> farField     (equilibrium inflow, upwind outflow) */
+ * src/fvDVM/discreteVelocity/discreteVelocity.C:188-195); the g/h
+ * surface values per type are those of fvDVM::updateGHbarSurf
+ * (fvDVM.C:866-1027), their relaxation fvDVM.C:1429-1453:
+ *   rho calculatedMaxwell -> maxwellWall  diffuse Maxwell wall
+ *   rho farField          -> farField     incoming rho_b M(U_owner, T_b), outgoing upwind
+ *   rho zeroGradient      -> zeroGradient every DV takes the owner cell's gbar+
+ *   rho fixedValue        -> mixed        incoming keep the Maxwellian of the patch rho,
+ *                                         U, T set at start (discreteVelocity.C:226-258)
+ *   symmetryPlane         -> symmetryPlane incoming DV = the face value of its mirror DV
+ *                                         (discreteVelocity.C:745-771)
+ *   rho symmetryMod       -> DVMsymmetry  the same, and every DV relaxed once more
+ *   rho pressureIn        -> farField     and after each step rho_b = p/(R T_b)
+ *   rho pressureOut       -> farField     and after each step rho_b, T_b from the owner
+ *                                         cell and p (fvDVM::updatePressureInOutBC,
+ *                                         fvDVM.C:1745-1821)
+ * Symmetry patches must be planar and normal to a coordinate axis (the
+ * reference mirrors by the patch's first face normal); they are not
+ * supported on a DV-sharded handle (the mirror DV can live on another
+ * shard). */
 typedef enum dugks_patch_type {
     DUGKS_PATCH_MAXWELL_WALL = 1,
-    DUGKS_PATCH_FAR_FIELD = 2
+    DUGKS_PATCH_FAR_FIELD = 2,
+    DUGKS_PATCH_ZERO_GRADIENT = 3,
+    DUGKS_PATCH_MIXED = 4,
+    DUGKS_PATCH_SYMMETRY = 5,
+    DUGKS_PATCH_DVM_SYMMETRY = 6,
+    DUGKS_PATCH_PRESSURE_IN = 7,
+    DUGKS_PATCH_PRESSURE_OUT = 8
 } dugks_patch_type;
 
 typedef enum dugks_precision {
@@ -117,12 +139,17 @@ typedef struct dugks_gas {
  * faces rho is ignored (computed each step from the outgoing flux,
  * calculatedMaxwellFvPatchField.C:140-164); for farField faces rho and T
  * stay at these values (farFieldFvPatchField.H assignment operators are
- * no-ops) and U is not used (the owner-cell velocity is, fvDVM.C:929-934). */
+ * no-ops) and U is not used (the owner-cell velocity is, fvDVM.C:929-934).
+ * pressureIn / pressureOut faces start from these rho and T (the reference's
+ * patch constructors set rho to 1, pressureInFvPatchField.C:72-75) and p is
+ * their pressureIn / pressureOut value.  p may be NULL without pressure
+ * patches; zeroGradient and symmetry faces use no values. */
 typedef struct dugks_bc {
     const int32_t* patch_type;      /* [n_patches] dugks_patch_type */
     const double* rho;              /* [n_boundary_faces] */
     const double* U;                /* [n_boundary_faces*3] */
     const double* T;                /* [n_boundary_faces] */
+    const double* p;                /* [n_boundary_faces] or NULL */
 } dugks_bc;
 
 typedef struct dugks_options {
@@ -259,11 +286,13 @@ int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double d
 /* The record the next step starts from besides g~, h~: per cell (in the
  * mesh's cell order) rho, U[3], T, q[3], tau as the last step's moment sums
  * gave them, then the largest and the summed |U_f| + sqrt(D) xi_max over
- * delta_f of the internal faces (Courant number per unit time step).
- * dugks_set_state recomputes these from the DFs in another summation order,
- * which differs in the last bits; setting the saved record after it makes a
- * restart continue bit for bit.  Length: dugks_step_record_size doubles
- * (9 n_cells + 2).  dugks_set_step_record requires rho, T, tau > 0. */
+ * delta_f of the internal faces (Courant number per unit time step), then
+ * rho_b, T_b per boundary face (the pressure patches carry them from step
+ * to step; T_b is restored on those faces only).  dugks_set_state recomputes the
+ * cell part from the DFs in another summation order, which differs in the
+ * last bits; setting the saved record after it makes a restart continue bit
+ * for bit.  Length: dugks_step_record_size doubles (9 n_cells + 2 +
+ * 2 n_boundary_faces).  dugks_set_step_record requires rho, T, tau > 0. */
 int64_t dugks_step_record_size(const dugks_handle* h);
 int dugks_get_step_record(dugks_handle* h, double* rec);
 int dugks_set_step_record(dugks_handle* h, const double* rec);

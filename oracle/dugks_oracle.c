@@ -9,6 +9,9 @@
  *   src/fvDVM/discreteVelocity/discreteVelocity.C equilibria, BC-type map
  *   src/fvDVM/BCs/calculatedMaxwellFvPatchField/calculatedMaxwellFvPatchField.C
  *   src/fvDVM/BCs/farFieldFvPatchField/farFieldFvPatchField.H (no-op assignment)
+ *   src/fvDVM/BCs/pressureInFvPatchField, pressureOutFvPatchField,
+ *   symmetryModFvPatchField (their value starts at one: the dictionary
+ *       constructors assign pTraits<Type>::one)
  *   src/fvDVM/zeroBoundaryGrad/zeroBoundaryVectors.C, zeroBoundaryGrad.C
  *       (least squares; the commented boundary terms restored = stock
  *        leastSquares, which the cases select in system/fvSchemes)
@@ -33,6 +36,8 @@ struct oracle_state {
     double *lsP, *lsN, *lsB;
     int *ptype, *pstart, *bf_patch, *bf_local;
     double *rho_b, *U_b, *T_b;      /* rho patch values (farField keeps them), U/T patch values */
+    double *p_b;                    /* pressureIn / pressureOut values */
+    int n1d;                        /* DV nodes per dimension (symmetry targets) */
     double *inByRho, *outGoing;     /* calculatedMaxwell patch members */
     int nv;
     double *xi, *wv, xi_max;
@@ -331,6 +336,7 @@ oracle_state* oracle_create(int D, int K_inner, double R, double omega, double T
     s->rho_b = dup(rho_b, n_boundary);
     s->U_b = dup(U_b, 3 * (size_t)n_boundary);
     s->T_b = dup(T_b, n_boundary);
+    s->p_b = dup(NULL, n_boundary);
     s->inByRho = dup(NULL, n_boundary);
     s->outGoing = dup(NULL, n_boundary);
     s->nv = n_dv;
@@ -368,7 +374,7 @@ void oracle_destroy(oracle_state* s) {
     void* ptrs[] = {s->own, s->nei, s->C, s->V, s->Cf, s->Sf, s->magSf, s->w, s->dc, s->lsP, s->lsN, s->lsB,
                     s->ptype, s->pstart, s->bf_patch, s->bf_local, s->rho_b, s->U_b, s->T_b, s->inByRho,
                     s->outGoing, s->xi, s->wv, s->gT, s->hT, s->gBP, s->hBP, s->gS, s->hS, s->gSb, s->hSb,
-                    s->rho, s->U, s->T, s->q, s->tau, s->rhoF, s->UF, s->TF, s->qF, s->tauF};
+                    s->rho, s->U, s->T, s->q, s->tau, s->rhoF, s->UF, s->TF, s->qF, s->tauF, s->p_b};
     for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; ++i) free(ptrs[i]);
     free(s);
 }
@@ -382,6 +388,32 @@ static inline double eq_by_rho(const oracle_state* s, const double* xi, const do
 /* fvDVM::updateTau (fvDVM.C:1823-1832) */
 static inline double tau_of(const oracle_state* s, double T, double rho) {
     return s->muRef * exp(s->omega * log(T / s->Tref)) / rho / T / s->R;
+}
+
+void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b) {
+    s->n1d = n_dv_1d;
+    if (p_b) memcpy(s->p_b, p_b, sizeof(double) * s->nBF);
+}
+
+/* the DV a symmetry patch mirrors DV d into: round(|n . (symmX, symmY,
+ * symmZ)(d)|) with n the unit normal of the patch's first face
+ * (discreteVelocity.C:735-738, :762-764; target ids fvDVM.C:300-372) */
+static int sym_target(const oracle_state* s, int patch, int d) {
+    const int n = s->n1d, D = s->D;
+    const int ix = d % n, iy = D >= 2 ? (d / n) % n : 0, iz = D == 3 ? d / (n * n) : 0;
+    double tx, ty, tz;
+    if (D == 3) {
+        tx = iz * n * n + iy * n + (n - ix - 1);
+        ty = iz * n * n + (n - iy - 1) * n + ix;
+        tz = (n - iz - 1) * n * n + iy * n + ix;
+    } else {
+        tx = iy * n + (n - ix - 1);
+        ty = (n - iy - 1) * n + ix;
+        tz = 0;
+    }
+    const double* S = s->Sf + 3 * (s->nIF + s->pstart[patch]);
+    const double m = sqrt(magsqr3(S));
+    return (int)round(fabs(S[0] / m * tx + S[1] / m * ty + S[2] / m * tz));
 }
 
 void oracle_set_macros(oracle_state* s, const double* rho, const double* U, const double* T) {
@@ -415,6 +447,20 @@ void oracle_set_macros(oracle_state* s, const double* rho, const double* U, cons
         }
         s->inByRho[b] = acc;
         s->outGoing[b] = 0.0;
+    }
+    /* mixed (rho fixedValue) patches: g/h = equilibriumMaxwell of the patch
+     * rho, U, T for every DV (discreteVelocity::initBoundaryField,
+     * discreteVelocity.C:226-258, :1010-1024); the incoming DVs keep it */
+    for (int b = 0; b < s->nBF; ++b) {
+        if (s->ptype[s->bf_patch[b]] != ORACLE_PATCH_MIXED) continue;
+        const double Tb = s->T_b[b];
+        for (int i = 0; i < s->nv; ++i) {
+            const double* xi = s->xi + 3 * i;
+            double d[3] = {s->U_b[3 * b] - xi[0], s->U_b[3 * b + 1] - xi[1], s->U_b[3 * b + 2] - xi[2]};
+            size_t id = (size_t)i * s->nBF + b;
+            s->gSb[id] = s->rho_b[b] / pow(sqrt(2.0 * M_PI * R * Tb), D) * exp(-magsqr3(d) / (2.0 * R * Tb));
+            s->hSb[id] = (s->K + 3 - D) * R * Tb * s->gSb[id];
+        }
     }
     for (int c = 0; c < s->nC; ++c) s->tau[c] = tau_of(s, s->T[c], s->rho[c]);
     /* Usurf = linear interpolate(Uvol) (fvDVM.C:2116), for the first CFL */
@@ -526,7 +572,25 @@ void oracle_evolve(oracle_state* s, double dt) {
                 const double* S = s->Sf + 3 * f;
                 double xs = dot3(xi, S);
                 int type = s->ptype[s->bf_patch[b]];
-                if (type == ORACLE_PATCH_FAR_FIELD) {
+                if (type == ORACLE_PATCH_ZERO_GRADIENT) {
+                    /* gSurf == gBarPvol patchInternalField, every DV (fvDVM.C:887-891) */
+                    gSb[b] = g[o];
+                    hSb[b] = h[o];
+                } else if (type == ORACLE_PATCH_MIXED) {
+                    /* outgoing upwind; incoming keep the initial Maxwellian (fvDVM.C:892-909) */
+                    if (xs > 0) {
+                        gSb[b] = recon(g[o], Gg + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
+                        hSb[b] = recon(h[o], Gh + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
+                    }
+                } else if (type == ORACLE_PATCH_SYMMETRY || type == ORACLE_PATCH_DVM_SYMMETRY) {
+                    /* outgoing and tangential upwind; incoming from the mirror DV below
+                     * (fvDVM.C:1009-1025) */
+                    if (xs > -VSMALL) {
+                        gSb[b] = recon(g[o], Gg + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
+                        hSb[b] = recon(h[o], Gh + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
+                    }
+                } else if (type == ORACLE_PATCH_FAR_FIELD || type == ORACLE_PATCH_PRESSURE_IN ||
+                           type == ORACLE_PATCH_PRESSURE_OUT) {
                     if (xs > 0) {
                         gSb[b] = recon(g[o], Gg + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
                         hSb[b] = recon(h[o], Gh + 3 * o, s->Cf + 3 * f, s->C + 3 * o, xi, dt);
@@ -575,6 +639,21 @@ void oracle_evolve(oracle_state* s, double dt) {
                 s->gSb[id] = s->rho_b[b] * eq_by_rho(s, xi, s->U_b + 3 * b, s->T_b[b]);
                 s->hSb[id] = s->gSb[id] * (R * s->T_b[b]) * (double)(K + 3 - D);
             }
+        }
+    }
+
+    /* 7. updateGHbarSurfSymmetryIn (fvDVM.C:1100-1179, discreteVelocity.C:691-773):
+     *    incoming DVs (xi . S_first <= 0) take the mirror DV's face value, DVs
+     *    in ascending order */
+    for (int b = 0; b < nBF; ++b) {
+        const int p = s->bf_patch[b], type = s->ptype[p];
+        if (type != ORACLE_PATCH_SYMMETRY && type != ORACLE_PATCH_DVM_SYMMETRY) continue;
+        const double* S0 = s->Sf + 3 * (nIF + s->pstart[p]);
+        for (int dvi = 0; dvi < nv; ++dvi) {
+            if (dot3(s->xi + 3 * dvi, S0) > 0) continue;
+            const int t = sym_target(s, p, dvi);
+            s->gSb[(size_t)dvi * nBF + b] = s->gSb[(size_t)t * nBF + b];
+            s->hSb[(size_t)dvi * nBF + b] = s->hSb[(size_t)t * nBF + b];
         }
     }
 
@@ -641,7 +720,9 @@ void oracle_evolve(oracle_state* s, double dt) {
         double* hSb = s->hSb + (size_t)dvi * nBF;
         for (int b = 0; b < nBF; ++b) {
             int f = nIF + b;
-            if (!(dot3(xi, s->Sf + 3 * f) > 0)) continue;
+            const int dvm_sym = s->ptype[s->bf_patch[b]] == ORACLE_PATCH_DVM_SYMMETRY;
+            const int out = dot3(xi, s->Sf + 3 * f) > 0;
+            if (!out && !dvm_sym) continue;
             const double *U = s->UF + 3 * f, *q = s->qF + 3 * f;
             double T = s->TF[f], rho = s->rhoF[f];
             double um[3] = {U[0] - xi[0], U[1] - xi[1], U[2] - xi[2]};
@@ -656,8 +737,15 @@ void oracle_evolve(oracle_state* s, double dt) {
             double hEq = ((K + 3.0 - D) + (1.0 - Pr) * cqBy5pRT * ((cSqrByRT - D) * (K + 3.0 - D) - 2 * K)) *
                          gEqBGK * R * Tint;
             double r = 0.5 * dt / (2.0 * s->tauF[f] + 0.5 * dt);
-            gSb[b] = (1.0 - r) * gSb[b] + r * gEq;
-            hSb[b] = (1.0 - r) * hSb[b] + r * hEq;
+            if (out) {
+                gSb[b] = (1.0 - r) * gSb[b] + r * gEq;
+                hSb[b] = (1.0 - r) * hSb[b] + r * hEq;
+            }
+            if (dvm_sym) {
+                /* DVMsymmetry: every DV relaxed (again), fvDVM.C:1445-1453 */
+                gSb[b] = (1.0 - r) * gSb[b] + r * gEq;
+                hSb[b] = (1.0 - r) * hSb[b] + r * hEq;
+            }
         }
     }
 
@@ -724,6 +812,33 @@ void oracle_evolve(oracle_state* s, double dt) {
             s->U[3 * c + k] = U[k];
             s->q[3 * c + k] = fac * q[k];
         }
+    }
+
+    /* 12. updatePressureInOutBC (fvDVM.C:1745-1821): the pressureIn rho and
+     *     the pressureOut rho and T patch values from the owner cell (the
+     *     next step's far-field incoming DFs read them); U patch values by
+     *     the characteristics, kept for output */
+    for (int b = 0; b < nBF; ++b) {
+        const int type = s->ptype[s->bf_patch[b]];
+        if (type != ORACLE_PATCH_PRESSURE_IN && type != ORACLE_PATCH_PRESSURE_OUT) continue;
+        const int64_t o = s->own[nIF + b];
+        const double* Sf = s->Sf + 3 * (nIF + b);
+        const double magSf = s->magSf[nIF + b];
+        const double* Ui = s->U + 3 * o;
+        const double Ti = s->T[o], rhoi = s->rho[o], p = s->p_b[b];
+        const double ai = sqrt(R * Ti * (K + 5) / (K + 3));
+        double n[3] = {Sf[0] / magSf, Sf[1] / magSf, Sf[2] / magSf};
+        const double Un = dot3(Ui, n);
+        double UnIn;
+        if (type == ORACLE_PATCH_PRESSURE_IN) {
+            s->rho_b[b] = p / R / s->T_b[b];
+            UnIn = Un + (p - rhoi * R * Ti) / rhoi / ai;
+        } else {
+            s->rho_b[b] = rhoi + (p - rhoi * R * Ti) / ai / ai;
+            s->T_b[b] = p / (R * rhoi);
+            UnIn = Un + (rhoi * R * Ti - p) / rhoi / ai;
+        }
+        for (int k = 0; k < 3; ++k) s->U_b[3 * b + k] = UnIn * n[k] + (Ui[k] - Un * n[k]);
     }
 }
 

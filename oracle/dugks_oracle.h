@@ -21,7 +21,21 @@
 extern "C" {
 #endif
 
-enum { ORACLE_PATCH_MAXWELL_WALL = 1, ORACLE_PATCH_FAR_FIELD = 2 };
+/* patch types by the rho patch type (discreteVelocity::setBCtype,
+ * discreteVelocity.C:188-195): calculatedMaxwell -> maxwellWall, farField,
+ * zeroGradient, fixedValue -> mixed, symmetryPlane, symmetryMod ->
+ * DVMsymmetry, pressureIn / pressureOut -> farField plus the macro update of
+ * fvDVM::updatePressureInOutBC */
+enum {
+    ORACLE_PATCH_MAXWELL_WALL = 1,
+    ORACLE_PATCH_FAR_FIELD = 2,
+    ORACLE_PATCH_ZERO_GRADIENT = 3,
+    ORACLE_PATCH_MIXED = 4,
+    ORACLE_PATCH_SYMMETRY = 5,
+    ORACLE_PATCH_DVM_SYMMETRY = 6,
+    ORACLE_PATCH_PRESSURE_IN = 7,
+    ORACLE_PATCH_PRESSURE_OUT = 8
+};
 enum { ORACLE_LS_MAGSF = 0, ORACLE_LS_INVDIST = 1, ORACLE_LS_UNWEIGHTED = 2 };
 
 typedef struct oracle_state oracle_state;
@@ -44,6 +58,12 @@ oracle_state* oracle_create(int D, int K_inner, double R, double omega, double T
                             const double* U_b, const double* T_b, int n_dv, const double* xi,
                             const double* w, double xi_max, int ls_weighting, int n_threads);
 void oracle_destroy(oracle_state* s);
+
+/* Per-face pressure of pressureIn/pressureOut faces (the patch dictionary's
+ * pressureIn / pressureOut entry; others ignored) and the DV count per
+ * dimension (symmetry targets, fvDVM.C:300-372).  Call before
+ * oracle_set_macros when the mesh has such patches. */
+void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b);
 
 /* fvDVM ctor tail: initialiseDV (Maxwellian g/h), setCalculatedMaxwellRhoBC,
  * updateTau, linear Usurf (fvDVM.C:2110-2116). */

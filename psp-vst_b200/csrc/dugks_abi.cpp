@@ -197,9 +197,13 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     h->patch_type.assign(bc->patch_type, bc->patch_type + h->nP);
     h->bface_ptype.assign(nBF, 0);
     h->bface_patch_local.assign(nBF, 0);
+    bool any_pressure = false, any_symmetry = false;
     for (int p = 0; p < h->nP; ++p) {
-        if (h->patch_type[p] != DUGKS_PATCH_MAXWELL_WALL && h->patch_type[p] != DUGKS_PATCH_FAR_FIELD)
-            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: unsupported patch type");
+        const int pt = h->patch_type[p];
+        if (pt < DUGKS_PATCH_MAXWELL_WALL || pt > DUGKS_PATCH_PRESSURE_OUT)
+            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: unsupported patch type " + std::to_string(pt));
+        any_pressure = any_pressure || pt == DUGKS_PATCH_PRESSURE_IN || pt == DUGKS_PATCH_PRESSURE_OUT;
+        any_symmetry = any_symmetry || pt == DUGKS_PATCH_SYMMETRY || pt == DUGKS_PATCH_DVM_SYMMETRY;
         if (h->patch_start[p + 1] < h->patch_start[p]) return fail(DUGKS_ERR_ARG, "dugks_create: bad patch_start");
         for (int b = h->patch_start[p]; b < h->patch_start[p + 1]; ++b) {
             h->bface_ptype[b] = h->patch_type[p];
@@ -210,6 +214,19 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     h->bc_rho.assign(bc->rho, bc->rho + nBF);
     h->bc_U.assign(bc->U, bc->U + 3 * static_cast<size_t>(nBF));
     h->bc_T.assign(bc->T, bc->T + nBF);
+    h->bc_p.assign(nBF, 0.0);
+    if (any_pressure) {
+        if (!bc->p) return fail(DUGKS_ERR_ARG, "dugks_create: pressure patches need bc->p");
+        h->bc_p.assign(bc->p, bc->p + nBF);
+        for (int b = 0; b < nBF; ++b) {
+            const int pt = h->bface_ptype[b];
+            if ((pt == DUGKS_PATCH_PRESSURE_IN || pt == DUGKS_PATCH_PRESSURE_OUT) &&
+                (!(h->bc_p[b] > 0) || !std::isfinite(h->bc_p[b])))
+                return fail(DUGKS_ERR_ARG, "dugks_create: pressure must be > 0");
+        }
+    }
+    if (any_symmetry && shard && shard->world > 1)
+        return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_sharded: symmetry patches need the whole DV set on one handle");
     // tensor-product DV set, x fastest (fvDVM.C:293-374)
     const int n = dv->n_per_dim;
     h->n1d = n;
@@ -228,6 +245,41 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
             }
     }
     h->nv = static_cast<int>(h->w.size());
+    // symmetry patches: the reference mirrors incoming DV d into DV
+    // round(|n . (symmX, symmY, symmZ)(d)|), n the unit normal of the patch's
+    // first face (discreteVelocity.C:735-738, :762-764; ids fvDVM.C:300-372).
+    // That is the mirror along one axis when n is (nearly) a coordinate axis;
+    // other planes are rejected.
+    h->bface_mirror.assign(nBF, -1);
+    for (int p = 0; p < h->nP; ++p) {
+        const int pt = h->patch_type[p];
+        if (pt != DUGKS_PATCH_SYMMETRY && pt != DUGKS_PATCH_DVM_SYMMETRY) continue;
+        if (h->patch_start[p + 1] == h->patch_start[p]) continue;
+        const double* S = &h->Sf[3 * static_cast<size_t>(nIF + h->patch_start[p])];
+        const double mS = std::sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+        int axis = -1;
+        for (int k = 0; k < h->D && axis < 0; ++k) {
+            bool all = true;
+            for (int d = 0; d < h->nv && all; ++d) {
+                const int ix = d % n, iy = (d / n) % n, iz = h->D == 3 ? d / (n * n) : 0;
+                double t[3];
+                if (h->D == 3) {
+                    t[0] = iz * n * n + iy * n + (n - ix - 1);
+                    t[1] = iz * n * n + (n - iy - 1) * n + ix;
+                    t[2] = (n - iz - 1) * n * n + iy * n + ix;
+                } else {
+                    t[0] = iy * n + (n - ix - 1);
+                    t[1] = (n - iy - 1) * n + ix;
+                    t[2] = 0;
+                }
+                const double target = std::round(std::fabs(S[0] / mS * t[0] + S[1] / mS * t[1] + S[2] / mS * t[2]));
+                all = target == t[k];
+            }
+            if (all) axis = k;
+        }
+        if (axis < 0) return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: symmetry patch not normal to a coordinate axis");
+        for (int b = h->patch_start[p]; b < h->patch_start[p + 1]; ++b) h->bface_mirror[b] = axis;
+    }
     if (opt.ls_weighting < 0 || opt.ls_weighting > 2) return fail(DUGKS_ERR_ARG, "dugks_create: bad ls_weighting");
     dugks::compute_weights_and_ls(h, opt.ls_weighting);
     for (double x : h->lsP)
@@ -309,7 +361,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     cudaEventCreate(&h->ev1);
     double *d_xi, *d_w, *d_grad_ls, *d_dtV, *d_dc, *d_bS, *d_geo;
     int32_t *d_tb, *d_tlo, *d_lc, *d_tio, *d_gnb, *d_cfi, *d_fi, *d_bpl, *d_bpt, *d_bown;
-    int32_t *d_meta, *d_loc, *d_face, *d_other;
+    int32_t *d_meta, *d_loc, *d_face, *d_other, *d_bmir;
     std::vector<double> dtV(nC);
     for (int c = 0; c < nC; ++c) dtV[c] = 1.0 / h->V[t.perm[c]];
     std::vector<double> bS(3 * static_cast<size_t>(nBF));
@@ -331,6 +383,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         (st = upload(h, &d_cfi, t.cf_item)) || (st = upload(h, &d_dtV, dtV)) || (st = upload(h, &d_fi, t.face_items)) ||
         (st = upload(h, &d_bpl, h->bface_patch_local)) || (st = upload(h, &d_bpt, h->bface_ptype)) ||
         (st = upload(h, &d_bown, bown)) || (st = upload(h, &d_dc, h->dc)) || (st = upload(h, &d_bS, bS)) ||
+        (st = upload(h, &d_bmir, h->bface_mirror)) ||
         (st = upload(h, &h->d_chunk_begin, h->chunk_begin))) {
         *out = h;
         return st;
@@ -356,6 +409,13 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     dm.bface_patch_local = d_bpl;
     dm.bface_ptype = d_bpt;
     dm.bface_owner = d_bown;
+    dm.bface_mirror = d_bmir;
+    dm.n_sym_faces = dm.n_pressure_faces = 0;
+    for (int b = 0; b < nBF; ++b) {
+        const int pt = h->bface_ptype[b];
+        if (pt == DUGKS_PATCH_SYMMETRY || pt == DUGKS_PATCH_DVM_SYMMETRY) ++dm.n_sym_faces;
+        if (pt == DUGKS_PATCH_PRESSURE_IN || pt == DUGKS_PATCH_PRESSURE_OUT) ++dm.n_pressure_faces;
+    }
     dm.dc = d_dc;
     dm.bS = d_bS;
     dugks::DevState& ds = h->ds;
@@ -476,7 +536,11 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     const double K3D = h->gas.K_inner + 3.0 - D;
     std::vector<dugks::BRec> br(nBF);
     for (int b = 0; b < nBF; ++b) {
-        const double RT = R * h->bc_T[b];
+        const int pt = h->bface_ptype[b];
+        // zeroGradient and symmetry faces take no patch values
+        const bool uses_values = pt != DUGKS_PATCH_ZERO_GRADIENT && pt != DUGKS_PATCH_SYMMETRY &&
+                                 pt != DUGKS_PATCH_DVM_SYMMETRY;
+        const double RT = uses_values ? R * h->bc_T[b] : R * h->gas.Tref;
         if (!(RT > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: boundary T must be > 0");
         br[b].U[0] = h->bc_U[3 * b];
         br[b].U[1] = h->bc_U[3 * b + 1];
@@ -484,8 +548,10 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
         br[b].K_in = inv_norm_host(RT, D);
         br[b].invRT_in = 1.0 / RT;
         br[b].hfac = RT * K3D;
-        br[b].rho_in = h->bface_ptype[b] == DUGKS_PATCH_FAR_FIELD ? h->bc_rho[b] : 1.0;
+        br[b].rho_in = h->bface_ptype[b] == DUGKS_PATCH_MAXWELL_WALL ? 1.0 : h->bc_rho[b];
         br[b].inByRho = 0.0;
+        br[b].T = h->bc_T[b];
+        br[b].p = h->bc_p[b];
     }
     // face velocity for the first Courant number: linear interpolation
     // (fvDVM.C:2116), U_f = w (U_own - U_nei) + U_nei
@@ -751,7 +817,9 @@ int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean) {
     return DUGKS_OK;
 }
 
-int64_t dugks_step_record_size(const dugks_handle* h) { return h ? 9 * static_cast<int64_t>(h->nC) + 2 : 0; }
+int64_t dugks_step_record_size(const dugks_handle* h) {
+    return h ? 9 * static_cast<int64_t>(h->nC) + 2 + 2 * static_cast<int64_t>(h->nBF) : 0;
+}
 
 int dugks_get_step_record(dugks_handle* h, double* rec) {
     if (!h || !rec) return set_error(h, DUGKS_ERR_ARG, "dugks_get_step_record: null argument");
@@ -760,10 +828,19 @@ int dugks_get_step_record(dugks_handle* h, double* rec) {
     std::vector<double> cm(static_cast<size_t>(nC) * 9);
     CUDA_TRY(h, cudaMemcpyAsync(cm.data(), h->ds.cm, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(rec + cm.size(), h->ds.co, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<dugks::BRec> br(h->nBF);
+    if (h->nBF > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(br.data(), h->ds.brec, br.size() * sizeof(dugks::BRec), cudaMemcpyDeviceToHost,
+                                    h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     const std::vector<int32_t>& perm = h->tiling.perm;
     for (int c = 0; c < nC; ++c) std::memcpy(rec + 9 * static_cast<size_t>(perm[c]), &cm[9 * static_cast<size_t>(c)],
                                              9 * sizeof(double));
+    double* rb = rec + cm.size() + 2;
+    for (int b = 0; b < h->nBF; ++b) {
+        rb[2 * b] = br[b].rho_in;
+        rb[2 * b + 1] = br[b].T;
+    }
     return DUGKS_OK;
 }
 
@@ -785,7 +862,31 @@ int dugks_set_step_record(dugks_handle* h, const double* rec) {
     std::memcpy(&co_max, &co[0], sizeof co_max);
     if (!(co_max >= 0) || !std::isfinite(co_max) || !(co[1] >= 0) || !std::isfinite(co[1]))
         return set_error(h, DUGKS_ERR_ARG, "dugks_set_step_record: bad Courant sums");
+    // boundary rho and T: the pressure patches carry them from step to step
+    std::vector<dugks::BRec> br(h->nBF);
+    if (h->nBF > 0)
+        CUDA_TRY(h, cudaMemcpy(br.data(), h->ds.brec, br.size() * sizeof(dugks::BRec), cudaMemcpyDeviceToHost));
+    const double* rb = co + 2;
+    const double K3D = h->gas.K_inner + 3.0 - h->D;
+    for (int b = 0; b < h->nBF; ++b) {
+        // rho_b of every face (walls: the last step's rho_w, an output);
+        // T_b and its factors on the pressure faces, the only ones it changes on
+        br[b].rho_in = rb[2 * b];
+        const int pt = h->bface_ptype[b];
+        if (pt != DUGKS_PATCH_PRESSURE_IN && pt != DUGKS_PATCH_PRESSURE_OUT) continue;
+        const double rho_b = rb[2 * b], T_b = rb[2 * b + 1];
+        if (!(rho_b > 0) || !(T_b > 0) || !std::isfinite(rho_b + T_b))
+            return set_error(h, DUGKS_ERR_ARG, "dugks_set_step_record: bad boundary record");
+        const double RT = h->gas.R * T_b;
+        br[b].T = T_b;
+        br[b].K_in = inv_norm_host(RT, h->D);
+        br[b].invRT_in = 1.0 / RT;
+        br[b].hfac = RT * K3D;
+    }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (h->nBF > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(h->ds.brec, br.data(), br.size() * sizeof(dugks::BRec), cudaMemcpyHostToDevice,
+                                    h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->ds.cm, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->ds.co, co, 2 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, dugks::launch_cell_records(make_args(h, 0.0, 0.0), h->stream));

@@ -56,12 +56,15 @@ enum {
 // Incoming-DF parameters of a mesh-boundary face: g_in = rho_in K_in exp(-|U_in - xi|^2 invRT_in / 2),
 // h_in = g_in * hfac (fvDVM.C:926-938, :1079-1092).
 struct __align__(16) BRec {
-    double U[3];       // wall velocity (farField: unused, the owner-cell U is taken)
+    double U[3];       // wall and mixed: patch velocity (farField: the owner-cell U is taken)
     double K_in;       // (2 pi R T_in)^(-D/2)
     double invRT_in;
     double hfac;       // R T_in (K+3-D)
-    double rho_in;     // farField: fixed patch rho; wall: rho_w of the current step
+    double rho_in;     // farField, mixed: fixed patch rho; wall: rho_w of the current step;
+                       // pressureIn/Out: updated after each step
     double inByRho;    // wall: inComingByRho
+    double T;          // T_in
+    double p;          // pressureIn / pressureOut value
 };
 
 // Device-side view of everything the kernels read.
@@ -101,6 +104,8 @@ struct DevMesh {
     const int32_t* bface_patch_local;  // [nBF] index within its patch
     const int32_t* bface_ptype;    // [nBF]
     const int32_t* bface_owner;    // [nBF] renumbered owner cell
+    const int32_t* bface_mirror;   // [nBF] symmetry faces: mirrored DV axis 0..2; -1 otherwise
+    int n_sym_faces, n_pressure_faces;
     const double* dc;              // [nIF] deltaCoeffs
     const double* bS;              // [nBF*3] boundary face area vectors
     int n_items;
@@ -166,7 +171,8 @@ struct dugks_handle {
     double xi_max = 0;
     std::vector<int32_t> patch_type, patch_start;
     std::vector<int32_t> bface_ptype, bface_patch_local;
-    std::vector<double> bc_rho, bc_U, bc_T;
+    std::vector<double> bc_rho, bc_U, bc_T, bc_p;
+    std::vector<int32_t> bface_mirror;   // symmetry faces: mirrored DV axis; -1 otherwise
     std::vector<double> xi, w;      // tensor-product DV set
     std::vector<double> X1, W1;     // one-dimensional nodes and weights
     // geometry (original numbering)

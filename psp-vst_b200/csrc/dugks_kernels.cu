@@ -341,6 +341,85 @@ __global__ void k_state_moments(const StepArgs a) {
     for (int j = 0; j < 15; ++j) p[j] = acc[j];
 }
 
+// Symmetry patches, after pass A (updateGHbarSurfSymmetryIn, fvDVM.C:1100-1179,
+// discreteVelocity.C:691-773): every DV d incoming through the patch's first
+// face (xi.S <= 0) takes the face value of its mirror DV along the patch's
+// axis, and the face's raw moments gain it.  Pass A reconstructed the DVs
+// with xi.S > -VSMALL through the face's own area vector and summed them; a
+// mirror DV that is the DV itself changes nothing.  One thread per boundary
+// face, DVs in ascending order.
+template <int D, typename Real>
+__global__ void k_symmetry_in(const StepArgs a) {
+    const DevMesh& m = a.dm;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.nBF) return;
+    const int axis = __ldg(m.bface_mirror + b);
+    if (axis < 0) return;
+    const int it = __ldg(m.face_items + 2 * (m.nIF + b));
+    const int b0 = b - __ldg(m.bface_patch_local + b);
+    const double S0[3] = {__ldg(m.bS + 3 * b0), __ldg(m.bS + 3 * b0 + 1), __ldg(m.bS + 3 * b0 + 2)};
+    const double S[3] = {__ldg(m.bS + 3 * b), __ldg(m.bS + 3 * b + 1), __ldg(m.bS + 3 * b + 2)};
+    Real* fg = reinterpret_cast<Real*>(a.ds.fvg);
+    Real* fh = reinterpret_cast<Real*>(a.ds.fvh);
+    const size_t nI = static_cast<size_t>(m.n_items);
+    const int n = m.n1d;
+    double acc[15];
+    for (int j = 0; j < 15; ++j) acc[j] = 0.0;
+    for (int d = 0; d < m.nv; ++d) {
+        const double xi[3] = {__ldg(m.xi + 3 * d), __ldg(m.xi + 3 * d + 1), __ldg(m.xi + 3 * d + 2)};
+        if (xi_dot_s(xi, S0) > 0) continue;
+        const int ix = d % n, iy = (d / n) % n, iz = D == 3 ? d / (n * n) : 0;
+        const int t = axis == 0 ? d + (n - 1 - 2 * ix) : (axis == 1 ? d + (n - 1 - 2 * iy) * n
+                                                                     : d + (n - 1 - 2 * iz) * n * n);
+        if (t == d) continue;
+        const double w = __ldg(m.w + d), xi2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+        const size_t sd = static_cast<size_t>(d) * nI + it, st = static_cast<size_t>(t) * nI + it;
+        if (xi_dot_s(xi, S) > -kVSmall) accum<D>(acc, -w, xi, xi2, double(fg[sd]), double(fh[sd]));
+        fg[sd] = fg[st];
+        fh[sd] = fh[st];
+        accum<D>(acc, w, xi, xi2, double(fg[sd]), double(fh[sd]));
+    }
+    double* p = a.ds.partF + static_cast<size_t>(it) * kNM;
+    for (int j = 0; j < 14; ++j) p[j] += acc[j];
+}
+
+// pressureIn / pressureOut faces after the cell macros (updatePressureInOutBC,
+// fvDVM.C:1745-1821): the next step's incoming far-field DFs take
+//   pressureIn:  rho_b = p / R / T_b
+//   pressureOut: rho_b = rho_i + (p - rho_i R T_i) / a_i / a_i, T_b = p / (R rho_i)
+// from the owner cell i, a_i = sqrt(R T_i (K+5)/(K+3)); the patch velocity
+// follows the characteristics (kept for output).
+__global__ void k_pressure_bc(const StepArgs a) {
+    const DevMesh& m = a.dm;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.nBF) return;
+    const int pt = __ldg(m.bface_ptype + b);
+    if (pt != DUGKS_PATCH_PRESSURE_IN && pt != DUGKS_PATCH_PRESSURE_OUT) return;
+    BRec* br = a.ds.brec + b;
+    const double* cm = a.ds.cm + static_cast<size_t>(__ldg(m.bface_owner + b)) * 9;
+    const double rhoi = cm[0], Ui[3] = {cm[1], cm[2], cm[3]}, Ti = cm[4];
+    const double R = m.R, p = br->p;
+    const double ai = sqrt(R * Ti * (m.K + 5) / (m.K + 3));
+    const double S[3] = {__ldg(m.bS + 3 * b), __ldg(m.bS + 3 * b + 1), __ldg(m.bS + 3 * b + 2)};
+    const double magS = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+    const double nv[3] = {S[0] / magS, S[1] / magS, S[2] / magS};
+    const double Un = Ui[0] * nv[0] + Ui[1] * nv[1] + Ui[2] * nv[2];
+    double UnIn;
+    if (pt == DUGKS_PATCH_PRESSURE_IN) {
+        br->rho_in = p / R / br->T;
+        UnIn = Un + (p - rhoi * R * Ti) / rhoi / ai;
+    } else {
+        br->rho_in = rhoi + (p - rhoi * R * Ti) / ai / ai;
+        br->T = p / (R * rhoi);
+        const double RT = R * br->T;
+        br->K_in = inv_norm(RT, m.D);
+        br->invRT_in = 1.0 / RT;
+        br->hfac = RT * (m.K + 3.0 - m.D);
+        UnIn = Un + (rhoi * R * Ti - p) / rhoi / ai;
+    }
+    for (int k = 0; k < 3; ++k) br->U[k] = UnIn * nv[k] + (Ui[k] - Un * nv[k]);
+}
+
 // part[0][i] = sum over chunks of part[ch][i], in chunk order (the order the
 // combine kernels sum them in), for the cross-shard reduction
 __global__ void k_sum_chunks(double* part, int chunks, size_t n) {
@@ -363,6 +442,18 @@ cudaError_t launch_stage(const StepArgs& a, int precision, int stage, cudaStream
         case STAGE_PASS_A:
             e = launch_pass(a, precision, false, s);
             n = 1;
+            if (e == cudaSuccess && a.dm.n_sym_faces > 0) {
+                const int nb = (a.dm.nBF + 127) / 128;
+                if (precision == DUGKS_FP64) {
+                    if (a.dm.D == 3) k_symmetry_in<3, double><<<nb, 128, 0, s>>>(a);
+                    else k_symmetry_in<2, double><<<nb, 128, 0, s>>>(a);
+                } else {
+                    if (a.dm.D == 3) k_symmetry_in<3, float><<<nb, 128, 0, s>>>(a);
+                    else k_symmetry_in<2, float><<<nb, 128, 0, s>>>(a);
+                }
+                ++n;
+                e = cudaGetLastError();
+            }
             break;
         case STAGE_FACE_COMBINE:
             if (a.dm.nIF > 0) {
@@ -382,6 +473,10 @@ cudaError_t launch_stage(const StepArgs& a, int precision, int stage, cudaStream
         case STAGE_CELL_COMBINE:
             k_cell_combine<<<(a.dm.nC + tb - 1) / tb, tb, 0, s>>>(a, k, a.dt_next);
             n = 1;
+            if (a.dm.n_pressure_faces > 0) {
+                k_pressure_bc<<<(a.dm.nBF + tb - 1) / tb, tb, 0, s>>>(a);
+                ++n;
+            }
             e = cudaGetLastError();
             break;
         default:

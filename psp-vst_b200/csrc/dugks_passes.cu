@@ -724,17 +724,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                 }
             }
         } else {
-            // far-field inflow parameters (read per batch: boundary items are few)
-            const bool wall = v.ptype == DUGKS_PATCH_MAXWELL_WALL;
+            // mesh boundary, by patch type (fvDVM.C:866-1027)
+            const int pt = v.ptype;
+            const bool wall = pt == DUGKS_PATCH_MAXWELL_WALL;
+            const bool zero_grad = pt == DUGKS_PATCH_ZERO_GRADIENT;
+            const bool sym = pt == DUGKS_PATCH_SYMMETRY || pt == DUGKS_PATCH_DVM_SYMMETRY;
+            // incoming DFs computed here: far field and pressure patches
+            // rho_b M(xi; U_owner, T_b) (fvDVM.C:926-938); mixed patches the
+            // Maxwellian of the patch rho, U, T kept from the start
+            // (discreteVelocity.C:226-258)
+            const bool eq_in = !wall && !zero_grad && !sym;
             double bK = 0, bInv = 0, bHf = 0, bU[3] = {0, 0, 0};
-            if (!wall) {
+            if (eq_in) {
                 const BRec* br = a.ds.brec + v.face;
-                const int own = __ldg(m.bface_owner + v.face);
-                const size_t n = static_cast<size_t>(m.nC);
                 bK = __ldg(&br->rho_in) * __ldg(&br->K_in);
                 bInv = __ldg(&br->invRT_in);
                 bHf = __ldg(&br->hfac);
-                for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * n + own);
+                if (pt == DUGKS_PATCH_MIXED) {
+                    for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
+                } else {
+                    const int own = __ldg(m.bface_owner + v.face);
+                    const size_t n = static_cast<size_t>(m.nC);
+                    for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * n + own);
+                }
             }
             const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
 #pragma unroll
@@ -743,21 +755,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const double wx = sm.w1[bp.ix0 + j];
-                    if (xs > 0) {
-                        // outgoing: upwind from the owner (fvDVM.C:916-923, :950-961)
+                    if (zero_grad) {
+                        // every DV: the owner cell's gbar+ (fvDVM.C:887-891)
+                        const Real gg = sm.gB[j * kSL + v.la], hh = sm.hB[j * kSL + v.la];
+                        row_add(rs, wx, x, double(gg), double(hh));
+                        fg[j * nI] = gg;
+                        fh[j * nI] = hh;
+                    } else if (xs > 0 || (sym && xs > -kVSmall)) {
+                        // outgoing (symmetry: and tangential): upwind from the owner
+                        // (fvDVM.C:916-923, :950-961, :1013-1023)
                         Real gg, hh;
                         recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         const double aw = row_add(rs, wx, x, double(gg), double(hh));
                         if (wall) rs.O = fma(aw, xs, rs.O);
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
-                    } else if (!wall) {
-                        // incoming far field: rho_b M(xi; U_owner, T_b) (fvDVM.C:926-938);
-                        // incoming wall DFs enter through rho_w in the face combine
+                    } else if (eq_in) {
                         const double cx = x - bU[0];
                         const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
                         row_add(rs, wx, x, double(Real(ge)), double(Real(ge * bHf)));
                     }
+                    // incoming wall DFs enter through rho_w in the face combine;
+                    // incoming symmetry DFs are the mirror DVs' values, added by
+                    // the symmetry pass after this one
                 }
             }
         }
@@ -927,16 +947,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     }
                 }
             } else {
-                // incoming DFs, never relaxed: wall rho_w M(U_w, T_w)
-                // (fvDVM.C:1079-1092), far field rho_b M(U_owner, T_b)
-                // (fvDVM.C:926-938); read per batch, boundary items are few
+                // mesh boundary, by patch type.  Outgoing DFs are relaxed with
+                // the boundary face's record, whose h uses the internal-face T
+                // at the patch-local index (fvDVM.C:1367, :1413, :1429-1444).
+                // Incoming ones are not relaxed: wall rho_w M(U_w, T_w)
+                // (fvDVM.C:1079-1092), far field and pressure rho_b M(U_owner,
+                // T_b) (fvDVM.C:926-938) and mixed rho_b M(U_b, T_b) computed
+                // here; zero-gradient and symmetry ones come from the face-value
+                // buffer.  DVMsymmetry relaxes every DV once more
+                // (fvDVM.C:1445-1453).  Read per batch: boundary items are few.
                 const int face = __ldg(m.it_face + gi);
-                const bool wall = (__ldg(m.it_meta + gi) >> 4) == DUGKS_PATCH_MAXWELL_WALL;
+                const int pt = __ldg(m.it_meta + gi) >> 4;
+                const bool stored_in = pt == DUGKS_PATCH_ZERO_GRADIENT || pt == DUGKS_PATCH_SYMMETRY ||
+                                       pt == DUGKS_PATCH_DVM_SYMMETRY;
+                const bool again = pt == DUGKS_PATCH_DVM_SYMMETRY;
                 const BRec* br = a.ds.brec + face;
                 const double bK = br->rho_in * __ldg(&br->K_in);
                 const double bInv = __ldg(&br->invRT_in), bHf = __ldg(&br->hfac);
                 double bU[3];
-                if (wall) {
+                if (pt == DUGKS_PATCH_MAXWELL_WALL || pt == DUGKS_PATCH_MIXED) {
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
                 } else {
                     const int own = __ldg(m.bface_owner + face);
@@ -949,12 +978,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
                         double gf, hf;
-                        if (xs > 0) {
-                            // outgoing: relaxed with the boundary face's record,
-                            // whose h uses the internal-face T at the patch-local
-                            // index (fvDVM.C:1367, :1413, :1429-1444)
-                            shk_relax<D, double>(fs, x, sx[j * kSI], double(sg[j * kSI]), double(sg[(NB + j) * kSI]),
-                                                 K3D, c0h, gf, hf);
+                        if (xs > 0 || stored_in) {
+                            gf = double(sg[j * kSI]);
+                            hf = double(sg[(NB + j) * kSI]);
+                            if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
+                            if (again) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                         } else {
                             const double cx = x - bU[0];
                             const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);

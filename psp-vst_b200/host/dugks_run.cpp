@@ -94,10 +94,6 @@ Args parse(int argc, char** argv) {
     return a;
 }
 
-const char* kind_name(PatchKind k) {
-    return k == PatchKind::Empty ? "empty" : (k == PatchKind::MaxwellWall ? "maxwellWall" : "farField");
-}
-
 using PatchValues = std::vector<std::pair<std::string, std::pair<std::string, std::vector<double>>>>;
 
 // rho, U, T, q of the current state into CASE/<time>/ (the AUTO_WRITE

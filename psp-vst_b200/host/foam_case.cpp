@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <map>
 #include <sstream>
 #include <sys/stat.h>
 
@@ -396,6 +397,8 @@ VolField read_vol_field(const std::string& path, int64_t n_cells, const std::vec
             for (const PatchInfo& pi : patches)
                 if (pi.name == e.first) size = pi.size;
             if (const FoamValue* v = e.second.find("value")) p.value = field_value(*v, f.ncomp, size);
+            if (const FoamValue* v = e.second.find("pressureIn")) p.pressure = v->number();
+            if (const FoamValue* v = e.second.find("pressureOut")) p.pressure = v->number();
             f.patches[e.first] = p;
         }
     } catch (const FoamError& e) {
@@ -434,12 +437,21 @@ Case read_case(const std::string& dir) {
         auto rt = rho.patches.find(p.name);
         // constraint (empty) patches need no field entry
         const std::string type = rt != rho.patches.end() ? rt->second.type : p.type;
-        PatchKind kind;
-        if (type == "empty") kind = PatchKind::Empty;
-        else if (type == "calculatedMaxwell") kind = PatchKind::MaxwellWall;
-        else if (type == "farField") kind = PatchKind::FarField;
-        else throw FoamError("patch " + p.name + ": rho patch type '" + type + "' is not supported");
+        static const std::map<std::string, PatchKind> by_type = {
+            {"empty", PatchKind::Empty},
+            {"calculatedMaxwell", PatchKind::MaxwellWall},
+            {"farField", PatchKind::FarField},
+            {"zeroGradient", PatchKind::ZeroGradient},
+            {"fixedValue", PatchKind::Mixed},
+            {"symmetryPlane", PatchKind::Symmetry},
+            {"symmetryMod", PatchKind::DVMSymmetry},
+            {"pressureIn", PatchKind::PressureIn},
+            {"pressureOut", PatchKind::PressureOut}};
+        const auto kt = by_type.find(type);
+        if (kt == by_type.end()) throw FoamError("patch " + p.name + ": rho patch type '" + type + "' is not supported");
+        const PatchKind kind = kt->second;
         c.kinds.push_back(kind);
+        c.patch_p.push_back(rt != rho.patches.end() ? rt->second.pressure : 0.0);
         auto first = [&](const VolField& f, int comp, double dflt) {
             auto it = f.patches.find(p.name);
             if (it == f.patches.end() || it->second.value.empty()) return dflt;
@@ -468,6 +480,34 @@ Case read_case(const std::string& dir) {
         if (const FoamValue* v = d.find("maxDeltaT")) c.max_delta_t = v->number();
     }
     return c;
+}
+
+int32_t patch_type_of(PatchKind k) {
+    switch (k) {
+        case PatchKind::MaxwellWall: return DUGKS_PATCH_MAXWELL_WALL;
+        case PatchKind::FarField: return DUGKS_PATCH_FAR_FIELD;
+        case PatchKind::ZeroGradient: return DUGKS_PATCH_ZERO_GRADIENT;
+        case PatchKind::Mixed: return DUGKS_PATCH_MIXED;
+        case PatchKind::Symmetry: return DUGKS_PATCH_SYMMETRY;
+        case PatchKind::DVMSymmetry: return DUGKS_PATCH_DVM_SYMMETRY;
+        case PatchKind::PressureIn: return DUGKS_PATCH_PRESSURE_IN;
+        case PatchKind::PressureOut: return DUGKS_PATCH_PRESSURE_OUT;
+        default: return 0;
+    }
+}
+
+const char* kind_name(PatchKind k) {
+    switch (k) {
+        case PatchKind::Empty: return "empty";
+        case PatchKind::MaxwellWall: return "maxwellWall";
+        case PatchKind::FarField: return "farField";
+        case PatchKind::ZeroGradient: return "zeroGradient";
+        case PatchKind::Mixed: return "mixed";
+        case PatchKind::Symmetry: return "symmetryPlane";
+        case PatchKind::DVMSymmetry: return "DVMsymmetry";
+        case PatchKind::PressureIn: return "pressureIn";
+        default: return "pressureOut";
+    }
 }
 
 FlatMesh flatten(const Case& c) {
@@ -500,11 +540,17 @@ FlatMesh flatten(const Case& c) {
             f.owner.push_back(pm.owner[k]);
             f.Cf.insert(f.Cf.end(), Cf.begin() + 3 * k, Cf.begin() + 3 * k + 3);
             f.Sf.insert(f.Sf.end(), Sf.begin() + 3 * k, Sf.begin() + 3 * k + 3);
-            f.rho_b.push_back(c.patch_rho[p]);
+            // pressureIn/Out and symmetryMod rho patches start at one: their
+            // dictionary constructors read no value and assign pTraits::one
+            // (pressureInFvPatchField.C:72-75, symmetryModFvPatchField.C:72)
+            const bool at_one = c.kinds[p] == PatchKind::PressureIn || c.kinds[p] == PatchKind::PressureOut ||
+                                c.kinds[p] == PatchKind::DVMSymmetry;
+            f.rho_b.push_back(at_one ? 1.0 : c.patch_rho[p]);
             f.U_b.insert(f.U_b.end(), c.patch_U.begin() + 3 * p, c.patch_U.begin() + 3 * p + 3);
             f.T_b.push_back(c.patch_T[p]);
+            f.p_b.push_back(c.patch_p[p]);
         }
-        f.patch_type.push_back(c.kinds[p] == PatchKind::MaxwellWall ? DUGKS_PATCH_MAXWELL_WALL : DUGKS_PATCH_FAR_FIELD);
+        f.patch_type.push_back(patch_type_of(c.kinds[p]));
         f.patch_start.push_back(f.patch_start.back() + static_cast<int32_t>(pi.size));
         f.patch_of.push_back(static_cast<int>(p));
     }

@@ -72,6 +72,7 @@ struct VolField {
     struct Patch {
         std::string type;
         std::vector<double> value;   // [size * ncomp], empty if the entry has none
+        double pressure = 0;         // pressureIn / pressureOut entry of the patch, if any
     };
     std::map<std::string, Patch> patches;
 };
@@ -79,7 +80,13 @@ VolField read_vol_field(const std::string& path, int64_t n_cells, const std::vec
 
 // boundary condition kinds of the rho patch types (discreteVelocity::setBCtype,
 // src/fvDVM/discreteVelocity/discreteVelocity.C:188-195)
-enum class PatchKind { Empty, MaxwellWall, FarField };
+// g/h surface type by the rho patch type (discreteVelocity::setBCtype,
+// discreteVelocity.C:188-195): calculatedMaxwell -> MaxwellWall, farField,
+// zeroGradient, fixedValue -> Mixed, symmetryPlane, symmetryMod ->
+// DVMSymmetry, pressureIn, pressureOut
+enum class PatchKind { Empty, MaxwellWall, FarField, ZeroGradient, Mixed, Symmetry, DVMSymmetry, PressureIn, PressureOut };
+int32_t patch_type_of(PatchKind k);      // dugks_patch_type
+const char* kind_name(PatchKind k);
 
 struct Case {
     std::string dir;
@@ -92,6 +99,7 @@ struct Case {
     std::vector<PatchKind> kinds;       // per mesh patch
     std::vector<std::string> rho_types, U_types, T_types;
     std::vector<double> patch_rho, patch_U, patch_T;   // per mesh patch: first face value
+    std::vector<double> patch_p;                       // per mesh patch: pressureIn / pressureOut
     std::vector<double> rho0, U0, T0;   // initial cell fields
     // system/controlDict (0 when absent)
     double start_time = 0, end_time = 0, delta_t = 0, write_interval = 0;
@@ -110,7 +118,7 @@ struct FlatMesh {
     std::vector<double> C, V, Cf, Sf;
     std::vector<int32_t> patch_type, patch_start;   // non-empty patches
     std::vector<int> patch_of;                      // non-empty patch -> mesh patch index
-    std::vector<double> rho_b, U_b, T_b;            // per boundary face
+    std::vector<double> rho_b, U_b, T_b, p_b;       // per boundary face
 };
 // geometry by the library's dugks_mesh_geometry (OpenFOAM primitiveMesh algorithm)
 FlatMesh flatten(const Case& c);

@@ -14,7 +14,7 @@ FvDVM::FvDVM(const Case& c, int precision, int device) : case_(c), flat_(flatten
                     f.Sf.data(),   static_cast<int32_t>(f.patch_type.size()), f.patch_start.data()};
     dugks_dv_set dv{static_cast<int32_t>(case_.xis.size()), case_.xis.data(), case_.weights.data(), case_.xi_max};
     dugks_gas gas{case_.R, case_.omega, case_.Tref, case_.mu_ref, case_.Pr, case_.K_inner};
-    dugks_bc bc{f.patch_type.data(), f.rho_b.data(), f.U_b.data(), f.T_b.data()};
+    dugks_bc bc{f.patch_type.data(), f.rho_b.data(), f.U_b.data(), f.T_b.data(), f.p_b.data()};
     dugks_options opt;
     dugks_default_options(&opt);
     opt.precision = precision;

@@ -15,6 +15,9 @@ Workloads (synthetic; the reference ships no mesh for them):
 * ``cube_case``        3-D lid-driven cube, n^3 cells.
 * ``ball_case``        flow past a sphere on a cubed-sphere mesh, far field
   at Mach Ma along +x, isothermal diffuse wall.
+* ``channel_case``     2-D channel whose four sides take any patch kind
+  (inlet/outlet/walls/symmetry), for the boundary types of
+  discreteVelocity::setBCtype.
 """
 from __future__ import annotations
 
@@ -44,13 +47,24 @@ def mu_bar(kn: float, omega: float) -> float:
     return 5.0 * (a + 1.0) * (a + 2.0) * math.sqrt(math.pi) * kn / (4.0 * a * (5.0 - 2 * omega) * (7.0 - 2.0 * omega))
 
 
+# patch kind (the g/h surface type discreteVelocity::setBCtype picks from
+# the rho patch type, discreteVelocity.C:188-195) -> dugks_patch_type
+PATCH_TYPES = {"maxwellWall": 1, "farField": 2, "zeroGradient": 3, "mixed": 4, "symmetryPlane": 5,
+               "DVMsymmetry": 6, "pressureIn": 7, "pressureOut": 8}
+# rho patch type in a case's 0/rho -> patch kind
+RHO_PATCH_KINDS = {"calculatedMaxwell": "maxwellWall", "farField": "farField", "zeroGradient": "zeroGradient",
+                   "fixedValue": "mixed", "symmetryPlane": "symmetryPlane", "symmetryMod": "DVMsymmetry",
+                   "pressureIn": "pressureIn", "pressureOut": "pressureOut"}
+
+
 @dataclass
 class Patch:
     name: str
-    kind: str                       # "maxwellWall" | "farField" | "empty"
+    kind: str                       # a PATCH_TYPES key or "empty"
     U: tuple = (0.0, 0.0, 0.0)
     T: float = 273.0
-    rho: float = 0.0                # farField patch density
+    rho: float = 0.0                # farField / mixed patch density
+    p: float = 0.0                  # pressureIn / pressureOut value
 
 
 @dataclass
@@ -90,7 +104,7 @@ class Case:
         by_name = {p.name: p for p in self.patches}
         sel = [np.arange(nIF)]
         ptype, pstart = [], [0]
-        rho_b, U_b, T_b = [], [], []
+        rho_b, U_b, T_b, p_b = [], [], [], []
         for p in pm.patches:
             spec = by_name.get(p["name"])
             if spec is None:
@@ -101,9 +115,16 @@ class Case:
                 continue
             faces = np.arange(p["startFace"], p["startFace"] + p["nFaces"])
             sel.append(faces)
-            ptype.append(1 if spec.kind == "maxwellWall" else 2)
+            if spec.kind not in PATCH_TYPES:
+                raise ValueError(f"unknown patch kind {spec.kind}")
+            ptype.append(PATCH_TYPES[spec.kind])
             pstart.append(pstart[-1] + len(faces))
-            rho_b.append(np.full(len(faces), spec.rho))
+            # pressureIn/Out and symmetryMod rho patches start at one: their
+            # dictionary constructors assign pTraits::one and read no value
+            # (pressureInFvPatchField.C:72-75, symmetryModFvPatchField.C:72)
+            starts_at_one = spec.kind in ("pressureIn", "pressureOut", "DVMsymmetry")
+            rho_b.append(np.full(len(faces), 1.0 if starts_at_one else spec.rho))
+            p_b.append(np.full(len(faces), spec.p))
             U_b.append(np.tile(np.asarray(spec.U, dtype=np.float64), (len(faces), 1)))
             T_b.append(np.full(len(faces), spec.T))
         idx = np.concatenate(sel)
@@ -117,7 +138,7 @@ class Case:
             "Cf": geometry["Cf"][idx], "Sf": geometry["Sf"][idx],
             "patch_type": np.array(ptype, dtype=np.int32),
             "patch_start": np.array(pstart, dtype=np.int32),
-            "rho_b": cat(rho_b, (0,)), "U_b": cat(U_b, (0, 3)), "T_b": cat(T_b, (0,)),
+            "rho_b": cat(rho_b, (0,)), "U_b": cat(U_b, (0, 3)), "T_b": cat(T_b, (0,)), "p_b": cat(p_b, (0,)),
         }
         if self.dt == 0.0:
             self.dt = cfl_dt(self, 0.5)
@@ -169,6 +190,28 @@ def cavity_case(n: int = 61, n_dv: int = 28, kn: float = 0.075, u_lid: float = 5
     return c.flatten(geometry) if flatten else c
 
 
+def channel_case(nx: int = 24, ny: int = 12, n_dv: int = 16, sides: dict | None = None, kn: float = 0.1,
+                 T0: float = 273.0, U0: tuple = (0.0, 0.0, 0.0), flatten: bool = True, geometry=None) -> Case:
+    """2-D channel [0, 2] x [0, 1] of argon at rest (or U0); ``sides`` maps
+    inlet / outlet / bottom / top to Patch arguments (kind, U, T, rho, p),
+    by default diffuse walls all round."""
+    mesh = meshgen.channel(nx, ny)
+    xis, w, xmax = _gh_set(n_dv, 273.0, R_DEMO)
+    gas = {"R": R_DEMO, "omega": OMEGA_VHS, "Tref": 273.0, "muRef": MU_DEMO, "Pr": PR_DEMO, "K": 0}
+    rho = RHO_DEMO * 0.075 / kn
+    sides = dict(sides or {})
+    patches = []
+    for name in ("inlet", "outlet", "bottom", "top"):
+        spec = dict(sides.get(name, {"kind": "maxwellWall"}))
+        kind = spec.pop("kind")
+        patches.append(Patch(name, kind, **spec))
+    patches.append(Patch("frontAndBack", "empty"))
+    nc = mesh.n_cells
+    c = Case(f"channel{nx}x{ny}_dv{n_dv}", mesh, 2, gas, xis, w, xmax, patches, np.full(nc, rho),
+             np.tile(np.asarray(U0, dtype=np.float64), (nc, 1)), np.full(nc, T0))
+    return c.flatten(geometry) if flatten else c
+
+
 def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None) -> Case:
     """The reference demo cavity read from its case files (polyMesh, Xis,
     weights, DVMProperties, 0/rho, 0/U, 0/T)."""
@@ -198,10 +241,13 @@ def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None) -> Case
         uv = U["patches"][p["name"]].get("value")
         tv = T["patches"][p["name"]].get("value")
         rv = rho["patches"][p["name"]].get("value")
-        kind = {"calculatedMaxwell": "maxwellWall", "farField": "farField"}[rtype]
+        if rtype not in RHO_PATCH_KINDS:
+            raise ValueError(f"unsupported rho patch type {rtype}")
+        kind = RHO_PATCH_KINDS[rtype]
+        pval = rho["patches"][p["name"]].get(kind, 0.0) if kind in ("pressureIn", "pressureOut") else 0.0
         patches.append(Patch(p["name"], kind, tuple(uv[0]) if uv is not None and len(uv) else (0, 0, 0),
                              float(tv[0]) if tv is not None and len(tv) else 273.0,
-                             float(rv[0]) if rv is not None and len(rv) else 0.0))
+                             float(rv[0]) if rv is not None and len(rv) else 0.0, float(pval)))
     c = Case("demo_cavity60", mesh, mesh.n_solution_dims, gas, xis, w, val(fp["xiMax"]), patches,
              rho["internal"], U["internal"], T["internal"])
     return c.flatten(geometry) if flatten else c

@@ -54,7 +54,7 @@ class Gas(C.Structure):
 
 
 class BC(C.Structure):
-    _fields_ = [("patch_type", _i32p), ("rho", _dp), ("U", _dp), ("T", _dp)]
+    _fields_ = [("patch_type", _i32p), ("rho", _dp), ("U", _dp), ("T", _dp), ("p", _dp)]
 
 
 class Adapt(C.Structure):
@@ -225,7 +225,8 @@ class Solver:
         rb = keep(fc["rho_b"], np.float64)
         ub = keep(fc["U_b"], np.float64)
         tb = keep(fc["T_b"], np.float64)
-        self.bc = BC(ptr(pt, C.c_int32), ptr(rb), ptr(ub), ptr(tb))
+        pb = keep(fc.get("p_b", np.zeros(len(fc["T_b"]))), np.float64)
+        self.bc = BC(ptr(pt, C.c_int32), ptr(rb), ptr(ub), ptr(tb), ptr(pb))
         opt = Options()
         self.lib.dugks_default_options(C.byref(opt))
         opt.precision = precision

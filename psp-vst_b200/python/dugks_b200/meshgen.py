@@ -165,6 +165,26 @@ def cavity(n: int, thickness: float = 0.1) -> PolyMesh:
                              n_solution_dims=2)
 
 
+def channel(nx: int, ny: int, lx: float = 2.0, ly: float = 1.0, thickness: float = 0.1) -> PolyMesh:
+    """2-D channel [0, lx] x [0, ly]: patches inlet (x = 0), outlet (x = lx),
+    bottom (y = 0), top (y = ly), frontAndBack (empty)."""
+    pts, cells = _box_hexes(nx, ny, 1, lx, ly, thickness)
+    tol = 1e-9
+
+    def classify(c):
+        out = np.full(len(c), -1, dtype=np.int64)
+        out[np.abs(c[:, 0]) < tol] = 0
+        out[np.abs(c[:, 0] - lx) < tol] = 1
+        out[np.abs(c[:, 1]) < tol] = 2
+        out[np.abs(c[:, 1] - ly) < tol] = 3
+        out[(np.abs(c[:, 2]) < tol) | (np.abs(c[:, 2] - thickness) < tol)] = 4
+        return out
+
+    return hexes_to_polymesh(pts, cells, classify,
+                             [("inlet", "patch"), ("outlet", "patch"), ("bottom", "wall"), ("top", "wall"),
+                              ("frontAndBack", "empty")], n_solution_dims=2)
+
+
 def cube(n: int) -> PolyMesh:
     pts, cells = _box_hexes(n, n, n, 1.0, 1.0, 1.0)
     tol = 1e-9

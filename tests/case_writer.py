@@ -75,12 +75,21 @@ def write_case(case, directory, control: dict | None = None, rho_patch_type: dic
         body += "}\n"
         _write(os.path.join(directory, "0", name), cls, name, body)
 
+    rho_types = {"maxwellWall": "calculatedMaxwell", "farField": "farField", "zeroGradient": "zeroGradient",
+                 "mixed": "fixedValue", "symmetryPlane": "symmetryPlane", "DVMsymmetry": "symmetryMod",
+                 "pressureIn": "pressureIn", "pressureOut": "pressureOut"}
+
     def rho_entry(s, p):
         if s.kind == "empty":
             return "        type            empty;\n"
-        if s.kind == "farField":
-            return f"        type            {rtypes.get(p['name'], 'farField')};\n        value           uniform {_num(s.rho)};\n"
-        return f"        type            {rtypes.get(p['name'], 'calculatedMaxwell')};\n        value           uniform {_num(case.rho0[0])};\n"
+        t = rtypes.get(p['name'], rho_types[s.kind])
+        if s.kind in ("farField", "mixed"):
+            return f"        type            {t};\n        value           uniform {_num(s.rho)};\n"
+        if s.kind in ("pressureIn", "pressureOut"):
+            return f"        type            {t};\n        {s.kind}      {_num(s.p)};\n"
+        if s.kind in ("zeroGradient", "symmetryPlane", "DVMsymmetry"):
+            return f"        type            {t};\n"
+        return f"        type            {t};\n        value           uniform {_num(case.rho0[0])};\n"
 
     def u_entry(s, p):
         if s.kind == "empty":

@@ -39,6 +39,7 @@ def load():
     lib.oracle_create.restype = C.c_void_p
     lib.oracle_destroy.argtypes = [C.c_void_p]
     lib.oracle_set_macros.argtypes = [C.c_void_p, _dp, _dp, _dp]
+    lib.oracle_set_patch_extra.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.oracle_evolve.argtypes = [C.c_void_p, C.c_double]
     lib.oracle_co_num.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     for name in ("oracle_get_macros", "oracle_get_face_macros"):
@@ -95,6 +96,8 @@ class Oracle:
                                         _p(nei, C.c_int64), _p(Cc), _p(V), _p(Cf), _p(Sf), len(pt), _p(pt, C.c_int),
                                         _p(ps, C.c_int), _p(rb), _p(ub), _p(tb), self.n_dv, _p(xa), _p(wa),
                                         case.xi_max, ls_weighting, threads)
+        self._p_b = np.ascontiguousarray(fl.get("p_b", np.zeros(fl["n_boundary"])), dtype=np.float64)
+        self.lib.oracle_set_patch_extra(self.s, len(case.xis), _p(self._p_b))
         self.set_macros(case.rho0, case.U0, case.T0)
 
     def set_macros(self, rho, U, T):

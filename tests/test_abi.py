@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
         assert n in dl.SIGNATURES, n
-    assert lib.dugks_abi_version() == 1
+    assert lib.dugks_abi_version() == 2
 
 
 def test_default_options():

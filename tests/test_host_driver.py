@@ -83,9 +83,9 @@ def test_check_reads_time_controls(driver, tmp_path):
 
 def test_unsupported_patch_type_is_an_error(driver, tmp_path):
     c = cs.cavity_case(4, 6)
-    d = case_writer.write_case(c, str(tmp_path / "bad"), rho_patch_type={"movingWall": "zeroGradient"})
+    d = case_writer.write_case(c, str(tmp_path / "bad"), rho_patch_type={"movingWall": "inletOutlet"})
     r = _run(driver, d, "--check", check=False)
-    assert r.returncode == 1 and "zeroGradient" in r.stderr
+    assert r.returncode == 1 and "inletOutlet" in r.stderr
 
 
 def test_missing_case_is_an_error(driver, tmp_path):
@@ -129,7 +129,8 @@ def test_restart_file_continues_exactly(driver, tmp_path):
     b = case_writer.write_case(c, str(tmp_path / "restarted"))
     sa = _summary(_run(driver, a, "--steps", 4, "--dt", repr(c.dt)))
     s1 = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--write-state"))
-    header, dfs, record = 8 + 4 + 4 + 8 + 8 + 8 + 8, 2 * 8 * c.n_cells * 64, 8 * (9 * c.n_cells + 2)
+    header, dfs = 8 + 4 + 4 + 8 + 8 + 8 + 8, 2 * 8 * c.n_cells * 64
+    record = 8 * (9 * c.n_cells + 2 + 2 * c.flat["n_boundary"])
     assert os.path.getsize(os.path.join(b, s1["time_name"], "dugksState")) == header + dfs + record
     sb = _summary(_run(driver, b, "--steps", 2, "--dt", repr(c.dt), "--restart", s1["time_name"]))
     assert sa["time_name"] == sb["time_name"]
@@ -169,6 +170,42 @@ def test_adjustable_time_step_from_control_dict(driver, tmp_path):
         t += dt
         n += 1
     assert s["steps"] == n and s["dt"] == dt and s["time"] == t
+    m = ref.macros()
+    sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
+    rho = foamio.read_vol_field(os.path.join(d, s["time_name"], "rho"), c.n_cells, sizes)
+    np.testing.assert_allclose(rho["internal"], m["rho"], rtol=1e-14, atol=0)
+
+
+def _channel_sides():
+    p = 1.0 * cs.R_DEMO * 273.0
+    return {"inlet": {"kind": "pressureIn", "p": 1.2 * p, "T": 273.0},
+            "outlet": {"kind": "pressureOut", "p": p, "T": 273.0},
+            "bottom": {"kind": "zeroGradient"}, "top": {"kind": "symmetryPlane"}}
+
+
+def test_check_reads_every_rho_patch_type(driver, tmp_path):
+    kinds = {"inlet": "mixed", "outlet": "zeroGradient", "bottom": "DVMsymmetry", "top": "farField"}
+    c = cs.channel_case(6, 3, 6, sides={k: {"kind": v, "rho": 1e-6} for k, v in kinds.items()})
+    d = case_writer.write_case(c, str(tmp_path / "a"))
+    s = _summary(_run(driver, d, "--check"))
+    got = {p["name"]: p["kind"] for p in s["patches"]}
+    assert got == dict(kinds, frontAndBack="empty")
+    c = cs.channel_case(6, 3, 6, sides=_channel_sides())
+    d = case_writer.write_case(c, str(tmp_path / "b"))
+    got = {p["name"]: p["kind"] for p in _summary(_run(driver, d, "--check"))["patches"]}
+    assert got == {"inlet": "pressureIn", "outlet": "pressureOut", "bottom": "zeroGradient", "top": "symmetryPlane",
+                   "frontAndBack": "empty"}
+
+
+@pytest.mark.gpu
+def test_driver_pressure_driven_channel_matches_python_solver(driver, tmp_path):
+    c = cs.channel_case(12, 6, 8, sides=_channel_sides(), flatten=False)
+    c.rho0 = np.full(c.n_cells, 1.0)
+    c.flatten()
+    d = case_writer.write_case(c, str(tmp_path / "channel"))
+    s = _summary(_run(driver, d, "--steps", 6, "--dt", repr(c.dt)))
+    ref = dl.Solver(c)
+    ref.step(6, c.dt)
     m = ref.macros()
     sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
     rho = foamio.read_vol_field(os.path.join(d, s["time_name"], "rho"), c.n_cells, sizes)
