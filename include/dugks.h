@@ -158,7 +158,12 @@ typedef struct dugks_options {
     int32_t device;                 /* CUDA device ordinal */
     int32_t tile_cells;             /* cells per tile; 0 = automatic */
     int32_t dv_chunks;              /* DV chunks per tile; 0 = automatic */
-    int32_t reserved[11];
+    int32_t macro_flux;             /* fvDVMparas macroFlux: 0 "no" (cell macros from the
+                                       DF moments), 1 "yes" (cell rho, rho U, rho E advance by
+                                       the face macro fluxes, fvDVM.C:1613-1679; the
+                                       unstructured-velocity-mesh variant of that branch is
+                                       not built) */
+    int32_t reserved[10];
 } dugks_options;
 
 typedef struct dugks_handle dugks_handle;

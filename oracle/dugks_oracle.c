@@ -38,6 +38,7 @@ struct oracle_state {
     double *rho_b, *U_b, *T_b;      /* rho patch values (farField keeps them), U/T patch values */
     double *p_b;                    /* pressureIn / pressureOut values */
     int n1d;                        /* DV nodes per dimension (symmetry targets) */
+    int macro_flux;                 /* fvDVMparas macroFlux yes */
     double *inByRho, *outGoing;     /* calculatedMaxwell patch members */
     int nv;
     double *xi, *wv, xi_max;
@@ -389,6 +390,8 @@ static inline double eq_by_rho(const oracle_state* s, const double* xi, const do
 static inline double tau_of(const oracle_state* s, double T, double rho) {
     return s->muRef * exp(s->omega * log(T / s->Tref)) / rho / T / s->R;
 }
+
+void oracle_set_macro_flux(oracle_state* s, int on) { s->macro_flux = on != 0; }
 
 void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b) {
     s->n1d = n_dv_1d;
@@ -781,17 +784,75 @@ void oracle_evolve(oracle_state* s, double dt) {
         }
     }
 
-    /* 11. updateMacroVol, macroFlux no (fvDVM.C:1521-1554, 1683-1742) */
+    /* 11a. updateMacroVol, macroFlux yes (fvDVM.C:1523-1526, :1613-1679): the
+     *      old rho, rho U, rho E advance by the face fluxes of this step's face
+     *      macros, internal faces in order, then the boundary faces.  The face
+     *      stress stays zero (its sum is commented out, fvDVM.C:1270, :1305).
+     *      The boundary momentum flux takes Sf of the INTERNAL face at the
+     *      patch-local index (fvDVM.C:1668-1669, Sf is the internal field).
+     *      "X & Sf*dt/V" is X & ((Sf dt)/V) by C++ precedence. */
+    double *mrho = NULL, *mrU = NULL, *mrE = NULL;
+    if (s->macro_flux) {
+        mrho = dup(NULL, nC);
+        mrU = dup(NULL, 3 * (size_t)nC);
+        mrE = dup(NULL, nC);
+        for (int c = 0; c < nC; ++c) {
+            const double* U = s->U + 3 * c;
+            mrho[c] = s->rho[c];
+            for (int k = 0; k < 3; ++k) mrU[3 * c + k] = s->rho[c] * U[k];
+            mrE[c] = s->rho[c] * (0.5 * magsqr3(U) + (K + 3) / 2.0 * R * s->T[c]);
+        }
+        for (int f = 0; f < nIF + nBF; ++f) {
+            const int internal = f < nIF;
+            const int64_t o = s->own[f];
+            const double *Uf = s->UF + 3 * f, *qf = s->qF + 3 * f, *S = s->Sf + 3 * f;
+            const double rf = s->rhoF[f];
+            const double rUf[3] = {rf * Uf[0], rf * Uf[1], rf * Uf[2]};
+            const double rEf = rf * (magsqr3(Uf) + (K + 3) / 2.0 * R * s->TF[f]);
+            const double ev[3] = {rEf * Uf[0] + qf[0], rEf * Uf[1] + qf[1], rEf * Uf[2] + qf[2]};
+            /* momentum: (rho_f U_f U_f + 0) & Sm */
+            const double* Sm = internal ? S : s->Sf + 3 * s->bf_local[f - nIF];
+            for (int side = 0; side < (internal ? 2 : 1); ++side) {
+                const int64_t c = side == 0 ? o : s->nei[f];
+                const double V = s->V[c], sgn = side == 0 ? -1.0 : 1.0;
+                const double Sd[3] = {S[0] * dt / V, S[1] * dt / V, S[2] * dt / V};
+                const double Smd[3] = {Sm[0] * dt / V, Sm[1] * dt / V, Sm[2] * dt / V};
+                double mU[3];
+                for (int i = 0; i < 3; ++i)
+                    mU[i] = (rUf[i] * Uf[0] + 0.0) * Smd[0] + (rUf[i] * Uf[1] + 0.0) * Smd[1] +
+                            (rUf[i] * Uf[2] + 0.0) * Smd[2];
+                const double mr = dot3(rUf, S) * dt / V;
+                const double mE = dot3(ev, Sd);
+                if (sgn < 0) {
+                    mrho[c] -= mr;
+                    for (int i = 0; i < 3; ++i) mrU[3 * c + i] -= mU[i];
+                    mrE[c] -= mE;
+                } else {
+                    mrho[c] += mr;
+                    for (int i = 0; i < 3; ++i) mrU[3 * c + i] += mU[i];
+                    mrE[c] += mE;
+                }
+            }
+        }
+    }
+
+    /* 11. updateMacroVol (fvDVM.C:1521-1554 macroFlux no, 1683-1742) */
 #pragma omp parallel for schedule(static) num_threads(s->nthreads)
     for (int c = 0; c < nC; ++c) {
         double rho = 0, rU[3] = {0, 0, 0}, rE = 0;
-        for (int i = 0; i < nv; ++i) {
-            const double* xi = s->xi + 3 * i;
-            double g = s->gT[(size_t)i * nC + c], h = s->hT[(size_t)i * nC + c];
-            double w = 1.0 * s->wv[i];
-            rho += w * g;
-            for (int k = 0; k < 3; ++k) rU[k] += w * g * xi[k];
-            rE += 0.5 * 1.0 * s->wv[i] * (magsqr3(xi) * g + h);
+        if (s->macro_flux) {
+            rho = mrho[c];
+            for (int k = 0; k < 3; ++k) rU[k] = mrU[3 * c + k];
+            rE = mrE[c];
+        } else {
+            for (int i = 0; i < nv; ++i) {
+                const double* xi = s->xi + 3 * i;
+                double g = s->gT[(size_t)i * nC + c], h = s->hT[(size_t)i * nC + c];
+                double w = 1.0 * s->wv[i];
+                rho += w * g;
+                for (int k = 0; k < 3; ++k) rU[k] += w * g * xi[k];
+                rE += 0.5 * 1.0 * s->wv[i] * (magsqr3(xi) * g + h);
+            }
         }
         double U[3] = {rU[0] / rho, rU[1] / rho, rU[2] / rho};
         double T = (rE - 0.5 * rho * magsqr3(U)) / ((K + 3) / 2.0 * R * rho);
@@ -813,6 +874,10 @@ void oracle_evolve(oracle_state* s, double dt) {
             s->q[3 * c + k] = fac * q[k];
         }
     }
+
+    free(mrho);
+    free(mrU);
+    free(mrE);
 
     /* 12. updatePressureInOutBC (fvDVM.C:1745-1821): the pressureIn rho and
      *     the pressureOut rho and T patch values from the owner cell (the

@@ -65,6 +65,10 @@ void oracle_destroy(oracle_state* s);
  * oracle_set_macros when the mesh has such patches. */
 void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b);
 
+/* fvDVMparas macroFlux (fvDVM.C:1940): nonzero = "yes", the cell rho, rho U
+ * and rho E advance by the face macro fluxes (fvDVM.C:1613-1679). */
+void oracle_set_macro_flux(oracle_state* s, int on);
+
 /* fvDVM ctor tail: initialiseDV (Maxwellian g/h), setCalculatedMaxwellRhoBC,
  * updateTau, linear Usurf (fvDVM.C:2110-2116). */
 void oracle_set_macros(oracle_state* s, const double* rho, const double* U, const double* T);

@@ -410,6 +410,39 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     dm.bface_ptype = d_bpt;
     dm.bface_owner = d_bown;
     dm.bface_mirror = d_bmir;
+    // macroFlux yes: the faces of every cell in face order (internal, then
+    // boundary), as the reference's face loops visit them
+    dm.macro_flux = opt.macro_flux ? 1 : 0;
+    dm.mf_off = nullptr;
+    dm.mf_ent = nullptr;
+    dm.mf_Sf = nullptr;
+    dm.mf_V = nullptr;
+    if (dm.macro_flux) {
+        std::vector<int32_t> cnt(nC + 1, 0), off(nC + 1, 0), ent(2 * static_cast<size_t>(nIF) + nBF);
+        for (int f = 0; f < nF; ++f) {
+            ++cnt[t.iperm[h->owner[f]]];
+            if (f < nIF) ++cnt[t.iperm[h->neighbour[f]]];
+        }
+        for (int c = 0; c < nC; ++c) off[c + 1] = off[c] + cnt[c];
+        std::vector<int32_t> pos(off.begin(), off.end() - 1);
+        for (int f = 0; f < nF; ++f) {
+            ent[pos[t.iperm[h->owner[f]]]++] = 2 * f;
+            if (f < nIF) ent[pos[t.iperm[h->neighbour[f]]]++] = 2 * f + 1;
+        }
+        std::vector<double> Vr(nC);
+        for (int c = 0; c < nC; ++c) Vr[c] = h->V[t.perm[c]];
+        int32_t *d_mo, *d_me;
+        double *d_ms, *d_mv;
+        if ((st = upload(h, &d_mo, off)) || (st = upload(h, &d_me, ent)) || (st = upload(h, &d_ms, h->Sf)) ||
+            (st = upload(h, &d_mv, Vr))) {
+            *out = h;
+            return st;
+        }
+        dm.mf_off = d_mo;
+        dm.mf_ent = d_me;
+        dm.mf_Sf = d_ms;
+        dm.mf_V = d_mv;
+    }
     dm.n_sym_faces = dm.n_pressure_faces = 0;
     for (int b = 0; b < nBF; ++b) {
         const int pt = h->bface_ptype[b];
@@ -1031,6 +1064,7 @@ int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double d
     if (st) return st;
     if (!(dt_prev > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: dt_prev must be > 0");
     dugks::StepArgs a = make_args(h, dt_prev, 0.0);
+    a.dm.macro_flux = 0;   // the macros of given DFs are their moments (macroFlux yes: restore the step record)
     CUDA_TRY(h, dugks::launch_state_moments(a, h->precision, h->stream));
     if ((st = shard_allreduce(h, h->ds.partC, static_cast<size_t>(h->nC) * dugks::kNM))) return st;
     CUDA_TRY(h, dugks::launch_cell_combine_one(a, 0.0, h->stream));

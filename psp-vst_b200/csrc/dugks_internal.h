@@ -106,6 +106,13 @@ struct DevMesh {
     const int32_t* bface_owner;    // [nBF] renumbered owner cell
     const int32_t* bface_mirror;   // [nBF] symmetry faces: mirrored DV axis 0..2; -1 otherwise
     int n_sym_faces, n_pressure_faces;
+    // macroFlux yes: faces of each (renumbered) cell in face order, entry
+    // f * 2 + (1 if the cell is the neighbour); face area vectors and volumes
+    int macro_flux;
+    const int32_t* mf_off;         // [nC+1]
+    const int32_t* mf_ent;         // [2 nIF + nBF]
+    const double* mf_Sf;           // [nF*3]
+    const double* mf_V;            // [nC] renumbered
     const double* dc;              // [nIF] deltaCoeffs
     const double* bS;              // [nBF*3] boundary face area vectors
     int n_items;

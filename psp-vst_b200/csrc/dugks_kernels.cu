@@ -176,6 +176,56 @@ __device__ __forceinline__ void write_cellrec(const StepArgs& a, const Consts& k
     write_maxwell_tables(a.dm, a.ds.ctab, n, c, U, 1.0 / RT, rho * inv_norm(RT, k.D));
 }
 
+// macroFlux yes (fvDVM.C:1523-1526, :1613-1679): the cell's old rho, rho U,
+// rho E advanced by this step's face macro fluxes, faces in face order.  The
+// face stress is zero (its sum is commented out, fvDVM.C:1270, :1305); the
+// boundary momentum flux takes Sf of the internal face at the patch-local
+// index (fvDVM.C:1668-1669); "X & Sf*dt/V" is X & ((Sf dt)/V).
+__device__ __forceinline__ void macro_flux_update(const StepArgs& a, const Consts& k, int c, double& rho, double rU[3],
+                                                  double& rE) {
+    const DevMesh& m = a.dm;
+    const double* cm = a.ds.cm + static_cast<size_t>(c) * 9;
+    const double U0[3] = {cm[1], cm[2], cm[3]};
+    rho = cm[0];
+    for (int i = 0; i < 3; ++i) rU[i] = rho * U0[i];
+    rE = rho * (0.5 * (U0[0] * U0[0] + U0[1] * U0[1] + U0[2] * U0[2]) + (k.Kin + 3) / 2.0 * k.R * cm[4]);
+    const double V = __ldg(m.mf_V + c), dt = k.dt;
+    for (int e = __ldg(m.mf_off + c); e < __ldg(m.mf_off + c + 1); ++e) {
+        const int code = __ldg(m.mf_ent + e), f = code >> 1;
+        const bool add = code & 1;
+        const double* fm = a.ds.fm + static_cast<size_t>(f) * 9;
+        const double rf = fm[0], Uf[3] = {fm[1], fm[2], fm[3]}, qf[3] = {fm[5], fm[6], fm[7]};
+        const double* S = m.mf_Sf + 3 * static_cast<size_t>(f);
+        const double* Sm = f < m.nIF ? S : m.mf_Sf + 3 * static_cast<size_t>(__ldg(m.bface_patch_local + f - m.nIF));
+        const double rUf[3] = {__dmul_rn(rf, Uf[0]), __dmul_rn(rf, Uf[1]), __dmul_rn(rf, Uf[2])};
+        const double rEf = __dmul_rn(rf, __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(Uf[0], Uf[0]), __dmul_rn(Uf[1], Uf[1])),
+                                                             __dmul_rn(Uf[2], Uf[2])),
+                                                   __dmul_rn(__dmul_rn((k.Kin + 3) / 2.0, k.R), fm[4])));
+        double ev[3], Sd[3], Smd[3];
+        for (int i = 0; i < 3; ++i) {
+            ev[i] = __dadd_rn(__dmul_rn(rEf, Uf[i]), qf[i]);
+            Sd[i] = __ddiv_rn(__dmul_rn(__ldg(S + i), dt), V);
+            Smd[i] = __ddiv_rn(__dmul_rn(__ldg(Sm + i), dt), V);
+        }
+        const double mr = __ddiv_rn(__dmul_rn(xi_dot_s(rUf, S), dt), V);
+        const double mE = xi_dot_s(ev, Sd);
+        double mU[3];
+        for (int i = 0; i < 3; ++i) {
+            const double t[3] = {__dmul_rn(rUf[i], Uf[0]), __dmul_rn(rUf[i], Uf[1]), __dmul_rn(rUf[i], Uf[2])};
+            mU[i] = xi_dot_s(t, Smd);
+        }
+        if (add) {
+            rho += mr;
+            for (int i = 0; i < 3; ++i) rU[i] += mU[i];
+            rE += mE;
+        } else {
+            rho -= mr;
+            for (int i = 0; i < 3; ++i) rU[i] -= mU[i];
+            rE -= mE;
+        }
+    }
+}
+
 __global__ void k_cell_combine(const StepArgs a, Consts k, double dt_next) {
     k.dt = step_dt(a);
     if (a.dtnp) dt_next = *a.dtnp;
@@ -189,7 +239,25 @@ __global__ void k_cell_combine(const StepArgs a, Consts k, double dt_next) {
         for (int j = 0; j < 14; ++j) s[j] += p[j];
     }
     double rho, U[3], T, q[3], tau;
-    macros_from_moments(s, k, rho, U, T, q, tau);
+    if (!m.macro_flux) {
+        macros_from_moments(s, k, rho, U, T, q, tau);
+    } else {
+        // rho, U, T from the fluxes; q from the DF moments about that U:
+        // q = 1/2 [V3 - 2 M2.U + |U|^2 M1 - U W + 2 U (M1.U) - U |U|^2 M0]
+        double rU[3], rE;
+        macro_flux_update(a, k, c, rho, rU, rE);
+        for (int i = 0; i < 3; ++i) U[i] = rU[i] / rho;
+        const double u2 = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+        T = (rE - 0.5 * rho * u2) / ((k.Kin + 3.0) / 2.0 * k.R * rho);
+        tau = k.muRef * exp(k.omega * log(T / k.Tref)) / rho / T / k.R;
+        const double* M2 = s + MOM_M2;
+        const double M2U[3] = {M2[0] * U[0] + M2[1] * U[1] + M2[2] * U[2], M2[1] * U[0] + M2[3] * U[1] + M2[4] * U[2],
+                               M2[2] * U[0] + M2[4] * U[1] + M2[5] * U[2]};
+        const double M1U = s[MOM_M1] * U[0] + s[MOM_M1 + 1] * U[1] + s[MOM_M1 + 2] * U[2];
+        for (int i = 0; i < 3; ++i)
+            q[i] = 0.5 * (s[MOM_V3 + i] - 2.0 * M2U[i] + u2 * s[MOM_M1 + i] - U[i] * s[MOM_W] + 2.0 * U[i] * M1U -
+                          U[i] * u2 * s[MOM_M0]);
+    }
     const double fac = 2.0 * tau / (2.0 * tau + k.dt * k.Pr);  // fvDVM.C:1742
     for (int i = 0; i < 3; ++i) q[i] *= fac;
     if (!(rho > 0.0) || !(T > 0.0) || !isfinite(rho + T + U[0] + U[1] + U[2])) atomicOr(a.ds.err, 1);

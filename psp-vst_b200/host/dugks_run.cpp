@@ -153,10 +153,11 @@ int main(int argc, char** argv) {
             for (double v : f.V) vol += v;
             std::printf("{\"cells\": %d, \"internal_faces\": %d, \"boundary_faces\": %d, \"D\": %d, "
                         "\"n_dv\": %.0f, \"volume\": %.17g, \"mass\": %.17g, \"xi_max\": %.17g, "
-                        "\"adjust_time_step\": %s, \"max_co\": %.17g, \"max_delta_t\": %.17g, \"patches\": [",
+                        "\"adjust_time_step\": %s, \"max_co\": %.17g, \"max_delta_t\": %.17g, "
+                        "\"macro_flux\": %s, \"patches\": [",
                         f.n_cells, f.n_internal, f.n_boundary, f.D, std::pow(double(c.xis.size()), f.D), vol,
                         total(c.rho0, f.V), c.xi_max, c.adjust_time_step ? "true" : "false", c.max_co,
-                        c.max_delta_t);
+                        c.max_delta_t, c.macro_flux ? "true" : "false");
             for (size_t p = 0; p < c.mesh.patches.size(); ++p)
                 std::printf("%s{\"name\": \"%s\", \"kind\": \"%s\", \"faces\": %lld}", p ? ", " : "",
                             c.mesh.patches[p].name.c_str(), kind_name(c.kinds[p]),

@@ -425,6 +425,7 @@ Case read_case(const std::string& dir) {
     c.Pr = gp.at("Pr").number();
     c.K_inner = gp.find("KInner") ? static_cast<int>(gp.at("KInner").number()) : 0;   // fvDVM.C:1948
     c.xi_max = fp.at("xiMax").number();
+    if (const FoamValue* mf = fp.find("macroFlux")) c.macro_flux = mf->kind == FoamValue::Word && mf->word == "yes";
     const int64_t nc = c.mesh.n_cells;
     const VolField rho = read_vol_field(dir + "/0/rho", nc, c.mesh.patches);
     const VolField U = read_vol_field(dir + "/0/U", nc, c.mesh.patches);

@@ -94,6 +94,7 @@ struct Case {
     int D = 3;
     std::vector<double> xis, weights;   // one-dimensional DV set
     double xi_max = 0;
+    bool macro_flux = false;            // fvDVMparas macroFlux yes
     double R = 0, omega = 0, Tref = 0, mu_ref = 0, Pr = 0;
     int K_inner = 0;
     std::vector<PatchKind> kinds;       // per mesh patch

@@ -19,6 +19,7 @@ FvDVM::FvDVM(const Case& c, int precision, int device) : case_(c), flat_(flatten
     dugks_default_options(&opt);
     opt.precision = precision;
     opt.device = device;
+    opt.macro_flux = case_.macro_flux ? 1 : 0;
     const int st = dugks_create(&mesh, &dv, &gas, &bc, &opt, &h_);
     if (st != DUGKS_OK) {
         const std::string msg = h_ ? dugks_last_error(h_) : "dugks_create failed";

@@ -81,6 +81,7 @@ class Case:
     U0: np.ndarray
     T0: np.ndarray
     dt: float = 0.0
+    macro_flux: bool = False        # fvDVMparas macroFlux yes
     flat: dict = field(default_factory=dict)
     geometry: dict = field(default_factory=dict)
 
@@ -250,6 +251,7 @@ def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None) -> Case
                              float(rv[0]) if rv is not None and len(rv) else 0.0, float(pval)))
     c = Case("demo_cavity60", mesh, mesh.n_solution_dims, gas, xis, w, val(fp["xiMax"]), patches,
              rho["internal"], U["internal"], T["internal"])
+    c.macro_flux = str(fp.get("macroFlux", "no")) == "yes"
     return c.flatten(geometry) if flatten else c
 
 

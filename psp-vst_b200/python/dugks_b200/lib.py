@@ -104,7 +104,8 @@ def dv_rows(n_rows: int, rank: int, world: int) -> tuple[int, int]:
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("ls_weighting", C.c_int32), ("device", C.c_int32),
-                ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("reserved", C.c_int32 * 11)]
+                ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("macro_flux", C.c_int32),
+                ("reserved", C.c_int32 * 10)]
 
 
 # every symbol include/dugks.h declares, with its ctypes signature
@@ -195,7 +196,7 @@ class Solver:
     """fvDVM-shaped wrapper over one dugks_handle."""
 
     def __init__(self, case, precision: int = FP64, ls_weighting: int = LS_MAGSF, device: int = 0,
-                 tile_cells: int = 0, dv_chunks: int = 0, shard: Shard | None = None):
+                 tile_cells: int = 0, dv_chunks: int = 0, shard: Shard | None = None, macro_flux: bool | None = None):
         self.lib = load()
         self.case = case
         fc = case.flat
@@ -234,6 +235,9 @@ class Solver:
         opt.device = device
         opt.tile_cells = tile_cells
         opt.dv_chunks = dv_chunks
+        if macro_flux is None:
+            macro_flux = getattr(case, "macro_flux", False)
+        opt.macro_flux = 1 if macro_flux else 0
         h = C.c_void_p()
         if shard is None:
             st = self.lib.dugks_create(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas), C.byref(self.bc),

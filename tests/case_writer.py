@@ -52,7 +52,7 @@ def write_case(case, directory, control: dict | None = None, rho_patch_type: dic
         f"    xiMax   xiMax [0 1 -1 0 0 0 0] {_num(case.xi_max)};\n"
         f"    xiMin   xiMin [0 1 -1 0 0 0 0] {_num(-case.xi_max)};\n"
         f"    nDV     {len(case.xis)};\n"
-        "    macroFlux no;\n}\n\n"
+        f"    macroFlux {'yes' if getattr(case, 'macro_flux', False) else 'no'};\n}}\n\n"
         "gasProperties\n{\n"
         f"    R       R [0 2 -2 -1 0 0 0] {_num(g['R'])};\n"
         f"    omega   {_num(g['omega'])};\n"

@@ -40,6 +40,7 @@ def load():
     lib.oracle_destroy.argtypes = [C.c_void_p]
     lib.oracle_set_macros.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.oracle_set_patch_extra.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.oracle_set_macro_flux.argtypes = [C.c_void_p, C.c_int]
     lib.oracle_evolve.argtypes = [C.c_void_p, C.c_double]
     lib.oracle_co_num.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
     for name in ("oracle_get_macros", "oracle_get_face_macros"):
@@ -77,7 +78,7 @@ def geometry(pm) -> dict:
 class Oracle:
     """Same interface as dugks_b200.lib.Solver, on the CPU restatement."""
 
-    def __init__(self, case, ls_weighting: int = 0, threads: int = 0, xi=None, w=None):
+    def __init__(self, case, ls_weighting: int = 0, threads: int = 0, xi=None, w=None, macro_flux: bool | None = None):
         self.lib = load()
         self.case = case
         fl = case.flat
@@ -98,6 +99,9 @@ class Oracle:
                                         case.xi_max, ls_weighting, threads)
         self._p_b = np.ascontiguousarray(fl.get("p_b", np.zeros(fl["n_boundary"])), dtype=np.float64)
         self.lib.oracle_set_patch_extra(self.s, len(case.xis), _p(self._p_b))
+        if macro_flux is None:
+            macro_flux = getattr(case, "macro_flux", False)
+        self.lib.oracle_set_macro_flux(self.s, 1 if macro_flux else 0)
         self.set_macros(case.rho0, case.U0, case.T0)
 
     def set_macros(self, rho, U, T):

@@ -210,3 +210,13 @@ def test_driver_pressure_driven_channel_matches_python_solver(driver, tmp_path):
     sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
     rho = foamio.read_vol_field(os.path.join(d, s["time_name"], "rho"), c.n_cells, sizes)
     np.testing.assert_allclose(rho["internal"], m["rho"], rtol=1e-14, atol=0)
+
+
+def test_check_reads_macro_flux(driver, tmp_path):
+    c = cs.cavity_case(4, 6)
+    c.macro_flux = True
+    d = case_writer.write_case(c, str(tmp_path / "mf"))
+    assert _summary(_run(driver, d, "--check"))["macro_flux"] is True
+    c.macro_flux = False
+    d = case_writer.write_case(c, str(tmp_path / "nomf"))
+    assert _summary(_run(driver, d, "--check"))["macro_flux"] is False
