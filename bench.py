@@ -42,15 +42,21 @@ def parse():
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["ball", "cavity", "cube"], default="ball")
-    p.add_argument("--precision", choices=["fp64", "fp32c"], default="fp64")
+    p.add_argument("--workload", choices=["ball", "cavity", "cube", "batch"], default="ball",
+                   help="batch: 64 seeded cavities of uneven size through one CUDA graph (FP32c), "
+                        "against the same cases stepped one at a time")
+    p.add_argument("--precision", choices=["fp64", "fp32c"], default=None,
+                   help="default fp64; fp32c for --workload batch")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
     p.add_argument("--dv-shard", action="store_true",
                    help="N>1: shard the DV rows of one workload over the ranks (NCCL) instead of replicas")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.precision is None:
+        a.precision = "fp32c" if a.workload == "batch" else "fp64"
+    return a
 
 
 def build_case(name, ndv1d=0):
@@ -203,6 +209,84 @@ def replica_rate(world: int, cells: int, dvs: int, steps: int, seconds: float) -
     return world * cells * dvs * steps / seconds
 
 
+def batch_cases(seed: int = 20261203, n: int = 64):
+    """The batched workload: n lid-driven cavities, side N from {32, 48, 64,
+    96, 128, 192, 256}, Kn log-uniform in [0.01, 10], lid speed uniform in
+    [10, 100] m/s, wall T uniform in [250, 350] K, 28^2 GH DVs; seeded."""
+    import numpy as np
+    from dugks_b200 import case as cs
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([32, 48, 64, 96, 128, 192, 256], size=n)
+    kn = 10.0 ** rng.uniform(-2.0, 1.0, size=n)
+    lid = rng.uniform(10.0, 100.0, size=n)
+    tw = rng.uniform(250.0, 350.0, size=n)
+    return [cs.cavity_case(int(N), 28, kn=float(k), u_lid=float(u), T_wall=float(t))
+            for N, k, u, t in zip(sizes, kn, lid, tw)]
+
+
+def run_batch(args):
+    """--workload batch on one GPU: aggregate cell.DV updates/s of the
+    batched graph, beside the same cases stepped one at a time."""
+    import torch
+    from dugks_b200 import lib as dl
+    torch.cuda.set_device(0)
+    seed = 20261203
+    cases = batch_cases(seed)
+    prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
+    solvers = [dl.Solver(c, precision=prec) for c in cases]
+    pairs = sum(c.n_cells * c.n_dv for c in cases)
+    K = max(2, args.steps - args.steps % 2)
+    W = max(4, args.warmup + args.warmup % 2)
+    batch = dl.Batch(solvers, [c.dt for c in cases])
+    batch.step(W)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_uuid(0))
+    sampler.start()
+    time.sleep(0.4)
+    l0 = sum(s.kernel_launches() for s in solvers)
+    batch.step(K)
+    launches = sum(s.kernel_launches() for s in solvers) - l0
+    clocks = sampler.stop()
+    t_ms = batch.last_ms()
+    value = pairs * K / (t_ms / 1e3)
+    # one at a time: each case's own K steps, CUDA events on its stream
+    seq_ms = 0.0
+    for s, c in zip(solvers, cases):
+        seq_ms += float(s.step_timed(K, c.dt)[4])
+    seq = pairs * K / (seq_ms / 1e3)
+    # end to end: two steps per call, then every case's macros to the host
+    te0 = time.perf_counter()
+    for _ in range(K // 2):
+        batch.step(2)
+        for s in solvers:
+            s.macros()
+    te = time.perf_counter() - te0
+    rs = 8 if prec == dl.FP64 else 4
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == dl.FP64 else "f32 storage / f64 moments", "data": "synthetic",
+        "config": {"workload": "batch: 64 lid-driven cavities, N in {32..256}, Kn log-U[0.01,10], lid U[10,100] m/s, "
+                               "T_wall U[250,350] K, 28^2 GH DVs, each at its own CFL-0.5 dt, one CUDA graph "
+                               "(a branch per case)",
+                   "cases": len(cases), "cells": sum(c.n_cells for c in cases), "pairs": pairs, "seed": seed,
+                   "precision": "fp64" if prec == dl.FP64 else "fp32c", "parallelism": "one GPU",
+                   "l2": "inputs larger than L2 (state %.2f GB)" % (4 * rs * pairs / 1e9)},
+        "one_at_a_time": {"value": seq, "ms_per_step": seq_ms / K, "speedup_of_batch": value / seq},
+        "e2e": {"value": pairs * K / te, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": sum(72 * c.n_cells for c in cases) // 2},
+        "gpu_launches": launches,
+        "graph_kernels_per_two_steps": batch.graph_kernels(),
+        "step_roofline": {"bytes_per_update": 6 * rs, "achieved": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9,
+                          "frac": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9 / peak, "peak": peak,
+                          "peak_kind": peak_kind},
+        "clocks": clocks,
+    }
+    batch.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -222,6 +306,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batch":
+        if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            raise SystemExit("--workload batch runs on one GPU")
+        run_batch(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

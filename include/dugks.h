@@ -302,6 +302,25 @@ int64_t dugks_step_record_size(const dugks_handle* h);
 int dugks_get_step_record(dugks_handle* h, double* rec);
 int dugks_set_step_record(dugks_handle* h, const double* rec);
 
+/* Many independent cases stepped together (no counterpart in the
+ * reference, which runs one case per dugksFoam process).  One CUDA graph
+ * holds two steps of every handle, each handle a parallel branch on its own
+ * stream, so that the tiles of small cases share the GPU; dugks_batch_step
+ * replays it (an odd step count ends with one ordinary step per handle).
+ * The handles must be initialised (dugks_set_macros), on one device and
+ * unsharded; dt[i] is handle i's fixed time step.  Every handle's result is
+ * bitwise the one dugks_step gives it alone.  A handle stays usable on its
+ * own between batch steps; the batch holds no copy of its state. */
+typedef struct dugks_batch dugks_batch;
+int dugks_batch_create(dugks_handle* const* handles, int32_t n, const double* dt, dugks_batch** out);
+int dugks_batch_step(dugks_batch* b, int32_t n_steps);
+/* CUDA-event milliseconds of the last dugks_batch_step call (graph replays
+ * only), and the kernels one replay of the two-step graph launches */
+int dugks_batch_last_ms(const dugks_batch* b, double* ms);
+int64_t dugks_batch_graph_kernels(const dugks_batch* b);
+const char* dugks_batch_last_error(const dugks_batch* b);
+void dugks_batch_destroy(dugks_batch* b);
+
 /* Number of discrete velocities (nDV^D). */
 int32_t dugks_n_dv(const dugks_handle* h);
 

@@ -835,6 +835,176 @@ int dugks_shard_phase(dugks_handle* h, int32_t phase, double dt, double** part, 
     return phase == 2 ? check_device_errors(h) : DUGKS_OK;
 }
 
+}  // extern "C"
+
+struct dugks_batch {
+    std::vector<dugks_handle*> hs;
+    std::vector<double> dt;
+    std::vector<cudaEvent_t> joins;
+    int device = 0;
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> launches_per_pair;   // per handle
+    int64_t graph_kernels = 0;
+    double last_ms = 0;
+    std::string last_error;
+};
+
+namespace {
+
+int batch_fail(dugks_batch* b, int code, const std::string& msg) {
+    b->last_error = msg;
+    return code;
+}
+
+void batch_free(dugks_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->s0) cudaStreamSynchronize(b->s0);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->joins) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->s0) cudaStreamDestroy(b->s0);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dugks_batch_create(dugks_handle* const* handles, int32_t n, const double* dt, dugks_batch** out) {
+    if (!out) return DUGKS_ERR_ARG;
+    *out = nullptr;
+    if (!handles || !dt || n < 1) return DUGKS_ERR_ARG;
+    for (int i = 0; i < n; ++i) {
+        dugks_handle* h = handles[i];
+        if (!h || !h->initialised || sharded(h) || h->device != handles[0]->device || !(dt[i] > 0) ||
+            !std::isfinite(dt[i]))
+            return DUGKS_ERR_ARG;
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == h) return DUGKS_ERR_ARG;
+    }
+    dugks_batch* b = new (std::nothrow) dugks_batch();
+    if (!b) return DUGKS_ERR_OOM;
+    b->hs.assign(handles, handles + n);
+    b->dt.assign(dt, dt + n);
+    b->device = handles[0]->device;
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        b->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+        *out = b;
+        return DUGKS_ERR_CUDA;
+    };
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&b->s0, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess)
+        return cuda_fail(e, "stream or event creation");
+    b->joins.assign(n, nullptr);
+    for (int i = 0; i < n; ++i)
+        if ((e = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_fail(e, "cudaEventCreate");
+    // every handle's cell records carry the relax factors of its dt, as the
+    // graph's cell combines write them for the next step
+    for (int i = 0; i < n; ++i) {
+        dugks_handle* h = b->hs[i];
+        if (h->cellrec_dt != b->dt[i]) {
+            if ((e = dugks::launch_cell_prep(make_args(h, b->dt[i], 0.0), h->stream)) != cudaSuccess)
+                return cuda_fail(e, "cell prep");
+            h->cellrec_dt = b->dt[i];
+        }
+        if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    }
+    // capture: fork from s0 into every handle's stream, two steps each, join
+    if ((e = cudaStreamBeginCapture(b->s0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return cuda_fail(e, "cudaStreamBeginCapture");
+    int st = DUGKS_OK;
+    cudaEventRecord(b->fork, b->s0);
+    b->launches_per_pair.assign(n, 0);
+    for (int i = 0; i < n && st == DUGKS_OK; ++i) {
+        dugks_handle* h = b->hs[i];
+        cudaStreamWaitEvent(h->stream, b->fork, 0);
+        const int cur0 = h->ds.cur;
+        for (int k = 0; k < 2 && st == DUGKS_OK; ++k) {
+            const dugks::StepArgs a = make_args(h, b->dt[i], b->dt[i]);
+            if (cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream) != cudaSuccess) st = DUGKS_ERR_CUDA;
+            else st = enqueue_step(h, a, nullptr, &b->launches_per_pair[i], nullptr);
+            h->ds.cur = 1 - h->ds.cur;
+        }
+        h->ds.cur = cur0;
+        cudaEventRecord(b->joins[i], h->stream);
+        cudaStreamWaitEvent(b->s0, b->joins[i], 0);
+    }
+    e = cudaStreamEndCapture(b->s0, &b->graph);
+    if (st != DUGKS_OK) {
+        *out = b;
+        return batch_fail(b, st, "capturing a step failed");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    for (int c : b->launches_per_pair) b->graph_kernels += c;
+    *out = b;
+    return DUGKS_OK;
+}
+
+int dugks_batch_step(dugks_batch* b, int32_t n_steps) {
+    if (!b) return DUGKS_ERR_ARG;
+    if (n_steps < 0 || !b->exec) return batch_fail(b, DUGKS_ERR_ARG, "dugks_batch_step: bad arguments");
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return batch_fail(b, DUGKS_ERR_CUDA, cudaGetErrorString(e));
+    const int pairs = n_steps / 2;
+    // handles' own queued work comes first
+    for (dugks_handle* h : b->hs) {
+        if ((e = cudaEventRecord(h->ev0, h->stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(b->s0, h->ev0, 0)) != cudaSuccess)
+            return batch_fail(b, DUGKS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaEventRecord(b->ev0, b->s0);
+    for (int p = 0; p < pairs; ++p)
+        if ((e = cudaGraphLaunch(b->exec, b->s0)) != cudaSuccess)
+            return batch_fail(b, DUGKS_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+    cudaEventRecord(b->ev1, b->s0);
+    if ((e = cudaStreamSynchronize(b->s0)) != cudaSuccess)
+        return batch_fail(b, DUGKS_ERR_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    for (size_t i = 0; i < b->hs.size(); ++i) {
+        dugks_handle* h = b->hs[i];
+        h->steps_done += 2 * pairs;
+        h->launches += static_cast<int64_t>(b->launches_per_pair[i]) * pairs;
+        if (n_steps % 2) {
+            // the odd step on the handle's own stream, then the relax factors
+            // of its dt again for the next replay
+            int st = run_steps(h, 1, &b->dt[i], nullptr);
+            if (st == DUGKS_OK && (e = dugks::launch_cell_prep(make_args(h, b->dt[i], 0.0), h->stream)) != cudaSuccess)
+                st = set_error(h, DUGKS_ERR_CUDA, cudaGetErrorString(e));
+            if (st != DUGKS_OK) return batch_fail(b, st, "handle " + std::to_string(i) + ": " + h->last_error);
+            h->cellrec_dt = b->dt[i];
+        }
+        const int st = check_device_errors(h);
+        if (st != DUGKS_OK) return batch_fail(b, st, "handle " + std::to_string(i) + ": " + h->last_error);
+    }
+    return DUGKS_OK;
+}
+
+int dugks_batch_last_ms(const dugks_batch* b, double* ms) {
+    if (!b || !ms) return DUGKS_ERR_ARG;
+    *ms = b->last_ms;
+    return DUGKS_OK;
+}
+
+int64_t dugks_batch_graph_kernels(const dugks_batch* b) { return b ? b->graph_kernels : 0; }
+
+const char* dugks_batch_last_error(const dugks_batch* b) { return b ? b->last_error.c_str() : "null batch"; }
+
+void dugks_batch_destroy(dugks_batch* b) { batch_free(b); }
+
 int64_t dugks_kernel_launches(const dugks_handle* h) { return h ? h->launches : 0; }
 
 int dugks_co_num(dugks_handle* h, double dt, double* co_max, double* co_mean) {

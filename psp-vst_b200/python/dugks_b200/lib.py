@@ -130,6 +130,12 @@ SIGNATURES = {
     "dugks_get_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
+    "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
+    "dugks_batch_step": (C.c_int, [C.c_void_p, C.c_int32]),
+    "dugks_batch_last_ms": (C.c_int, [C.c_void_p, _dp]),
+    "dugks_batch_graph_kernels": (C.c_int64, [C.c_void_p]),
+    "dugks_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "dugks_batch_destroy": (None, [C.c_void_p]),
     "dugks_nccl_unique_id": (C.c_int, [C.POINTER(C.c_ubyte)]),
     "dugks_create_sharded": (C.c_int, [C.POINTER(Mesh), C.POINTER(DVSet), C.POINTER(Gas), C.POINTER(BC),
                                        C.POINTER(Options), C.POINTER(Shard), C.POINTER(C.c_void_p)]),
@@ -367,6 +373,48 @@ class Solver:
         if getattr(self, "h", None) is not None and self.h.value:
             self.lib.dugks_destroy(self.h)
         self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent solvers stepped together through one CUDA graph
+    (dugks_batch_create / dugks_batch_step); solvers[i] steps with dt[i]."""
+
+    def __init__(self, solvers, dt):
+        self.lib = load()
+        self.solvers = list(solvers)
+        hs = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        self._dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.solvers),)))
+        b = C.c_void_p()
+        st = self.lib.dugks_batch_create(hs, len(self.solvers), ptr(self._dt), C.byref(b))
+        self.b = b
+        if st != 0:
+            msg = self.lib.dugks_batch_last_error(b).decode() if b.value else "dugks_batch_create failed"
+            self.close()
+            raise DugksError(st, msg)
+
+    def step(self, n: int):
+        st = self.lib.dugks_batch_step(self.b, n)
+        if st != 0:
+            raise DugksError(st, self.lib.dugks_batch_last_error(self.b).decode())
+
+    def last_ms(self) -> float:
+        v = C.c_double()
+        self.lib.dugks_batch_last_ms(self.b, C.byref(v))
+        return v.value
+
+    def graph_kernels(self) -> int:
+        return int(self.lib.dugks_batch_graph_kernels(self.b))
+
+    def close(self):
+        if getattr(self, "b", None) is not None and self.b.value:
+            self.lib.dugks_batch_destroy(self.b)
+        self.b = C.c_void_p()
 
     def __del__(self):
         try:
