@@ -749,21 +749,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                 }
             }
             const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
+            if (zero_grad || sym) {
+                // (a loop of its own: the rare types stay off the common path)
+#pragma unroll 1
+                for (int j = 0; j < NB; ++j) {
+                    if (FULL || j < bp.nb) {
+                        const double x = sm.x1[bp.ix0 + j];
+                        const double xs = xs_row(x, v.S[0], p2, p3);
+                        const double wx = sm.w1[bp.ix0 + j];
+                        Real gg, hh;
+                        if (zero_grad) {
+                            // every DV: the owner cell's gbar+ (fvDVM.C:887-891)
+                            gg = sm.gB[j * kSL + v.la];
+                            hh = sm.hB[j * kSL + v.la];
+                        } else if (xs > -kVSmall) {
+                            // outgoing and tangential: upwind from the owner
+                            // (fvDVM.C:1013-1023); incoming ones are the mirror
+                            // DVs' values, added by the symmetry pass after this one
+                            recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                        } else {
+                            continue;
+                        }
+                        row_add(rs, wx, x, double(gg), double(hh));
+                        fg[j * nI] = gg;
+                        fh[j * nI] = hh;
+                    }
+                }
+            } else
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 if (FULL || j < bp.nb) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const double wx = sm.w1[bp.ix0 + j];
-                    if (zero_grad) {
-                        // every DV: the owner cell's gbar+ (fvDVM.C:887-891)
-                        const Real gg = sm.gB[j * kSL + v.la], hh = sm.hB[j * kSL + v.la];
-                        row_add(rs, wx, x, double(gg), double(hh));
-                        fg[j * nI] = gg;
-                        fh[j * nI] = hh;
-                    } else if (xs > 0 || (sym && xs > -kVSmall)) {
-                        // outgoing (symmetry: and tangential): upwind from the owner
-                        // (fvDVM.C:916-923, :950-961, :1013-1023)
+                    if (xs > 0) {
+                        // outgoing: upwind from the owner (fvDVM.C:916-923, :950-961)
                         Real gg, hh;
                         recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         const double aw = row_add(rs, wx, x, double(gg), double(hh));
@@ -775,9 +795,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
                         row_add(rs, wx, x, double(Real(ge)), double(Real(ge * bHf)));
                     }
-                    // incoming wall DFs enter through rho_w in the face combine;
-                    // incoming symmetry DFs are the mirror DVs' values, added by
-                    // the symmetry pass after this one
+                    // incoming wall DFs enter through rho_w in the face combine
                 }
             }
         }
@@ -972,17 +990,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * nC + own);
                 }
                 const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
+                if (again) {
+                    // DVMsymmetry: every DV relaxed once more after the outgoing
+                    // ones (a loop of its own: the rare type stays off the common path)
+#pragma unroll 1
+                    for (int j = 0; j < NB; ++j) {
+                        if (FULL || j < bp.nb) {
+                            const double x = sm.x1[bp.ix0 + j];
+                            const double xs = xs_row(x, S[0], p2, p3);
+                            double gf = double(sg[j * kSI]), hf = double(sg[(NB + j) * kSI]);
+                            if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
+                            shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
+                            sm.Fg[j * kSI + it] = Real(xs * gf);
+                            sm.Fh[j * kSI + it] = Real(xs * hf);
+                        }
+                    }
+                } else
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
                     if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
                         double gf, hf;
-                        if (xs > 0 || stored_in) {
+                        if (xs > 0) {
+                            shk_relax<D, double>(fs, x, sx[j * kSI], double(sg[j * kSI]), double(sg[(NB + j) * kSI]),
+                                                 K3D, c0h, gf, hf);
+                        } else if (stored_in) {
                             gf = double(sg[j * kSI]);
                             hf = double(sg[(NB + j) * kSI]);
-                            if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
-                            if (again) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                         } else {
                             const double cx = x - bU[0];
                             const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
