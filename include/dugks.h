@@ -124,6 +124,17 @@ typedef struct dugks_dv_set {
     double xi_max;                  /* xiMax, used by the Courant number only */
 } dugks_dv_set;
 
+/* A DV set that is no tensor product: the reference's unstructured velocity
+ * mesh (the VMESH build, fvDVM.C:129-277), whose DVs are the cell centres of
+ * constant/vMesh and whose weights are their cell volumes (xiMax = the
+ * largest |xi|).  In 2-D the z components are ignored. */
+typedef struct dugks_dv_list {
+    int32_t n_dv;
+    const double* xi;               /* [n_dv*3] */
+    const double* weights;          /* [n_dv] */
+    double xi_max;
+} dugks_dv_list;
+
 /* DVMProperties gasProperties (fvDVM.C:1943-1948) */
 typedef struct dugks_gas {
     double R;
@@ -213,6 +224,15 @@ typedef struct dugks_dv_shard {
 } dugks_dv_shard;
 
 int dugks_nccl_unique_id(unsigned char id[128]);
+
+/* dugks_create (shard NULL) or dugks_create_sharded with a DV list.  The
+ * passes then evaluate each DV's Maxwellian with its own exponential (the
+ * tensor-product factoring does not apply).  Not built for DV lists:
+ * symmetry patches (the reference's VMESH build leaves their mirror ids
+ * unset) and macroFlux yes (its VMESH branch, fvDVM.C:1562-1611). */
+int dugks_create_dv_list(const dugks_mesh* mesh, const dugks_dv_list* dv, const dugks_gas* gas,
+                         const dugks_bc* bc, const dugks_options* opt, const dugks_dv_shard* shard,
+                         dugks_handle** out);
 int dugks_create_sharded(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas,
                          const dugks_bc* bc, const dugks_options* opt, const dugks_dv_shard* shard,
                          dugks_handle** out);

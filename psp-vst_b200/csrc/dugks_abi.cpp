@@ -138,11 +138,13 @@ void dugks_default_options(dugks_options* opt) {
     opt->ls_weighting = DUGKS_LS_MAGSF;
 }
 
-static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
-                       const dugks_options* opt_in, const dugks_dv_shard* shard, dugks_handle** out) {
+// dv: a tensor-product set; dvl: a DV list (exactly one of them)
+static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_dv_list* dvl,
+                       const dugks_gas* gas, const dugks_bc* bc, const dugks_options* opt_in,
+                       const dugks_dv_shard* shard, dugks_handle** out) {
     if (!out) return DUGKS_ERR_ARG;
     *out = nullptr;
-    if (!mesh || !dv || !gas || !bc) return DUGKS_ERR_ARG;
+    if (!mesh || (!dv && !dvl) || !gas || !bc) return DUGKS_ERR_ARG;
     dugks_options opt;
     dugks_default_options(&opt);
     if (opt_in) opt = *opt_in;
@@ -161,8 +163,14 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         return fail(DUGKS_ERR_ARG, "dugks_create: incomplete mesh");
     if (mesh->n_solution_dims != 2 && mesh->n_solution_dims != 3)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: n_solution_dims must be 2 or 3");
-    if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
-    if (dv->n_per_dim > dugks::kMaxN1d)
+    if (dvl) {
+        if (dvl->n_dv < 1 || !dvl->xi || !dvl->weights) return fail(DUGKS_ERR_ARG, "dugks_create_dv_list: empty DV list");
+        if (opt.macro_flux)
+            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_dv_list: macroFlux yes is not built for DV lists");
+    } else if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) {
+        return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
+    }
+    if (!dvl && dv->n_per_dim > dugks::kMaxN1d)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: more than 64 DV nodes per dimension");
     if (opt.precision != DUGKS_FP64 && opt.precision != DUGKS_FP32C)
         return fail(DUGKS_ERR_ARG, "dugks_create: unknown precision");
@@ -175,7 +183,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     h->nBF = mesh->n_boundary_faces;
     h->nP = mesh->n_patches;
     h->gas = *gas;
-    h->xi_max = dv->xi_max;
+    h->xi_max = dvl ? dvl->xi_max : dv->xi_max;
     const int nC = h->nC, nIF = h->nIF, nBF = h->nBF, nF = nIF + nBF;
     h->owner.assign(mesh->owner, mesh->owner + nF);
     h->neighbour.assign(mesh->neighbour, mesh->neighbour + nIF);
@@ -225,12 +233,20 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
                 return fail(DUGKS_ERR_ARG, "dugks_create: pressure must be > 0");
         }
     }
+    if (any_symmetry && dvl)
+        return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_dv_list: symmetry patches need a tensor-product DV set");
     if (any_symmetry && shard && shard->world > 1)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_sharded: symmetry patches need the whole DV set on one handle");
-    // tensor-product DV set, x fastest (fvDVM.C:293-374)
-    const int n = dv->n_per_dim;
+    // tensor-product DV set, x fastest (fvDVM.C:293-374); a DV list as given
+    // (the unstructured velocity mesh, fvDVM.C:166-196), one DV per "row"
+    const int n = dvl ? 1 : dv->n_per_dim;
     h->n1d = n;
-    if (h->D == 3) {
+    if (dvl) {
+        for (int d = 0; d < dvl->n_dv; ++d) {
+            h->w.push_back(dvl->weights[d]);
+            h->xi.insert(h->xi.end(), {dvl->xi[3 * d], dvl->xi[3 * d + 1], h->D == 3 ? dvl->xi[3 * d + 2] : 0.0});
+        }
+    } else if (h->D == 3) {
         for (int iz = 0; iz < n; ++iz)
             for (int iy = 0; iy < n; ++iy)
                 for (int ix = 0; ix < n; ++ix) {
@@ -349,6 +365,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     dm.nv_loc = rows_loc * h->n1d;
     dm.prec = h->precision;
     dm.n1d = h->n1d;
+    dm.general_dv = dvl ? 1 : 0;
     dm.n_tiles = t.n_tiles;
     dm.n_items = t.n_items();
     dm.nb_max = t.nb_max;
@@ -370,8 +387,13 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         for (int k = 0; k < 3; ++k) bS[3 * b + k] = h->Sf[3 * (nIF + b) + k];
         bown[b] = t.iperm[h->owner[nIF + b]];
     }
-    h->X1.assign(dv->xis, dv->xis + h->n1d);
-    h->W1.assign(dv->weights, dv->weights + h->n1d);
+    if (dvl) {
+        h->X1.assign(1, 0.0);
+        h->W1.assign(1, 1.0);
+    } else {
+        h->X1.assign(dv->xis, dv->xis + h->n1d);
+        h->W1.assign(dv->weights, dv->weights + h->n1d);
+    }
     double *d_X1, *d_W1;
     if ((st = upload(h, &d_X1, h->X1)) || (st = upload(h, &d_W1, h->W1)) ||
         (st = upload(h, &d_xi, h->xi)) || (st = upload(h, &d_w, h->w)) || (st = upload(h, &d_tb, t.tile_begin)) ||
@@ -506,7 +528,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
 
 int dugks_create(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
                  const dugks_options* opt, dugks_handle** out) {
-    return create_impl(mesh, dv, gas, bc, opt, nullptr, out);
+    return create_impl(mesh, dv, nullptr, gas, bc, opt, nullptr, out);
 }
 
 int dugks_create_sharded(const dugks_mesh* mesh, const dugks_dv_set* dv, const dugks_gas* gas, const dugks_bc* bc,
@@ -515,7 +537,16 @@ int dugks_create_sharded(const dugks_mesh* mesh, const dugks_dv_set* dv, const d
         if (out) *out = nullptr;
         return DUGKS_ERR_ARG;
     }
-    return create_impl(mesh, dv, gas, bc, opt, shard, out);
+    return create_impl(mesh, dv, nullptr, gas, bc, opt, shard, out);
+}
+
+int dugks_create_dv_list(const dugks_mesh* mesh, const dugks_dv_list* dv, const dugks_gas* gas, const dugks_bc* bc,
+                         const dugks_options* opt, const dugks_dv_shard* shard, dugks_handle** out) {
+    if (!dv) {
+        if (out) *out = nullptr;
+        return DUGKS_ERR_ARG;
+    }
+    return create_impl(mesh, nullptr, dv, gas, bc, opt, shard, out);
 }
 
 int dugks_nccl_unique_id(unsigned char id[128]) {

@@ -80,6 +80,7 @@ struct DevMesh {
     const double* xi;      // [nv*3]
     const double* w;       // [nv]
     int n1d;               // nodes per dimension; DV d = (iz n + iy) n + ix
+    int general_dv;        // 1: a DV list that is no tensor product (n1d is 1, a "row" is one DV)
     const double* X1;      // [n1d] one-dimensional nodes
     const double* W1;      // [n1d] one-dimensional weights
     // tiles

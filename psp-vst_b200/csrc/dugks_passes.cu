@@ -1093,9 +1093,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     }
 }
 
+#include "dugks_passes_gen.cuh"
+
+template <typename K>
+cudaError_t set_smem(K* kernel, size_t bytes);
+
 // ---------------------------------------------------------------------
 // launch plumbing
 // ---------------------------------------------------------------------
+constexpr int kNbGen = 8;   // DVs per batch of the general-DV passes
+
+template <int D, typename Real>
+cudaError_t launch_gen(const StepArgs& a, bool pass_b, cudaStream_t s) {
+    const dim3 grid(a.dm.n_tiles, a.chunks);
+    if (!pass_b) k_pass_a_gen<D, Real, kNbGen><<<grid, kThreads, a.smemA, s>>>(a);
+    else k_pass_b_gen<D, Real, kNbGen><<<grid, kThreads, a.smemB, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int D, typename Real>
+cudaError_t configure_gen(const StepArgs& a) {
+    cudaError_t e = set_smem(k_pass_a_gen<D, Real, kNbGen>, a.smemA);
+    return e != cudaSuccess ? e : set_smem(k_pass_b_gen<D, Real, kNbGen>, a.smemB);
+}
 template <int D, typename Real, int NA, int NBB>
 cudaError_t launch_nb(const StepArgs& a, bool pass_b, cudaStream_t s) {
     const dim3 grid(a.dm.n_tiles, a.chunks);
@@ -1147,6 +1167,11 @@ int row_waste(int n1d, int nb) { return (n1d + nb - 1) / nb * nb - n1d; }
 }  // namespace
 
 cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s) {
+    if (a.dm.general_dv) {
+        if (precision == DUGKS_FP64)
+            return a.dm.D == 3 ? launch_gen<3, double>(a, pass_b, s) : launch_gen<2, double>(a, pass_b, s);
+        return a.dm.D == 3 ? launch_gen<3, float>(a, pass_b, s) : launch_gen<2, float>(a, pass_b, s);
+    }
     if (precision == DUGKS_FP64)
         return a.dm.D == 3 ? launch_pass_d<3, double>(a, pass_b, s) : launch_pass_d<2, double>(a, pass_b, s);
     return a.dm.D == 3 ? launch_pass_d<3, float>(a, pass_b, s) : launch_pass_d<2, float>(a, pass_b, s);
@@ -1154,6 +1179,17 @@ cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStrea
 
 void pass_config(int D, int precision, int n1d, StepArgs* a) {
     const bool f64 = precision == DUGKS_FP64;
+    if (a->dm.general_dv) {
+        a->wideA = a->wideB = a->fullA = a->fullB = 0;
+        if (f64) {
+            a->smemA = D == 3 ? SmemAG<3, double, kNbGen>::bytes() : SmemAG<2, double, kNbGen>::bytes();
+            a->smemB = SmemBG<double, kNbGen>::bytes();
+        } else {
+            a->smemA = D == 3 ? SmemAG<3, float, kNbGen>::bytes() : SmemAG<2, float, kNbGen>::bytes();
+            a->smemB = SmemBG<float, kNbGen>::bytes();
+        }
+        return;
+    }
     const int a0 = f64 ? Width<double>::A0 : Width<float>::A0, a1 = f64 ? Width<double>::A1 : Width<float>::A1;
     const int b0 = f64 ? Width<double>::B0 : Width<float>::B0, b1 = f64 ? Width<double>::B1 : Width<float>::B1;
     // the wide batch unless it pads the rows more than the narrow one;
@@ -1172,6 +1208,10 @@ void pass_config(int D, int precision, int n1d, StepArgs* a) {
 }
 
 cudaError_t configure_kernels(int precision, const StepArgs& a) {
+    if (a.dm.general_dv) {
+        if (precision == DUGKS_FP64) return a.dm.D == 3 ? configure_gen<3, double>(a) : configure_gen<2, double>(a);
+        return a.dm.D == 3 ? configure_gen<3, float>(a) : configure_gen<2, float>(a);
+    }
     if (precision == DUGKS_FP64) return a.dm.D == 3 ? configure_d<3, double>(a) : configure_d<2, double>(a);
     return a.dm.D == 3 ? configure_d<3, float>(a) : configure_d<2, float>(a);
 }

@@ -8,7 +8,7 @@
 //
 //   dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] [--device D]
 //                  [--write-interval N] [--no-write] [--write-state] [--restart TIME] [--check]
-//                  [--max-co C] [--max-delta-t DT] [--fixed-dt]
+//                  [--max-co C] [--max-delta-t DT] [--fixed-dt] [--vmesh]
 //
 // The time step is --dt, else controlDict deltaT, else the Courant number
 // 0.5 of the initial state (fvDVM::getCoNum).  With controlDict
@@ -18,7 +18,9 @@
 // reach endTime (Time::run: time < endTime - dt/2).  Fixed steps write every
 // --write-interval steps, else every writeInterval / deltaT steps; adjusted
 // steps write when the time passes a multiple of writeInterval (the time step
-// is not shortened to land on it).  --write-state adds an exact restart file
+// is not shortened to land on it).  --vmesh takes the DVs from the velocity
+// mesh constant/vMesh (cell centres, cell volumes), as the reference's VMESH
+// build does.  --write-state adds an exact restart file
 // (dugksState, see fvdvm.hpp) to every written time directory; --restart TIME
 // continues from CASE/TIME/dugksState.  --check reads the case and computes the
 // mesh geometry on the host only (no GPU) and prints a summary.  The last
@@ -47,6 +49,7 @@ struct Args {
     bool write_state = false;
     bool check = false;
     bool fixed_dt = false;
+    bool vmesh = false;
     double max_co = 0, max_delta_t = 0;
     std::string restart;
 };
@@ -54,7 +57,7 @@ struct Args {
 [[noreturn]] void usage(const char* msg) {
     std::fprintf(stderr, "dugks_run: %s\nusage: dugks_run CASE [--steps N] [--dt DT] [--precision fp64|fp32c] "
                          "[--device D] [--write-interval N] [--no-write] [--write-state] [--restart TIME] "
-                         "[--check] [--max-co C] [--max-delta-t DT] [--fixed-dt]\n", msg);
+                         "[--check] [--max-co C] [--max-delta-t DT] [--fixed-dt] [--vmesh]\n", msg);
     std::exit(2);
 }
 
@@ -77,6 +80,7 @@ Args parse(int argc, char** argv) {
         else if (s == "--max-co") a.max_co = std::atof(val());
         else if (s == "--max-delta-t") a.max_delta_t = std::atof(val());
         else if (s == "--fixed-dt") a.fixed_dt = true;
+        else if (s == "--vmesh") a.vmesh = true;
         else if (s == "--precision") {
             const std::string p = val();
             if (p == "fp64") a.precision = DUGKS_FP64;
@@ -146,7 +150,7 @@ double total(const std::vector<double>& v, const std::vector<double>& w) {
 int main(int argc, char** argv) {
     const Args a = parse(argc, argv);
     try {
-        const Case c = read_case(a.dir);
+        const Case c = read_case(a.dir, a.vmesh);
         if (a.check) {
             const FlatMesh f = flatten(c);
             double vol = 0;
@@ -155,7 +159,8 @@ int main(int argc, char** argv) {
                         "\"n_dv\": %.0f, \"volume\": %.17g, \"mass\": %.17g, \"xi_max\": %.17g, "
                         "\"adjust_time_step\": %s, \"max_co\": %.17g, \"max_delta_t\": %.17g, "
                         "\"macro_flux\": %s, \"patches\": [",
-                        f.n_cells, f.n_internal, f.n_boundary, f.D, std::pow(double(c.xis.size()), f.D), vol,
+                        f.n_cells, f.n_internal, f.n_boundary, f.D,
+                        c.dv_w.empty() ? std::pow(double(c.xis.size()), f.D) : double(c.dv_w.size()), vol,
                         total(c.rho0, f.V), c.xi_max, c.adjust_time_step ? "true" : "false", c.max_co,
                         c.max_delta_t, c.macro_flux ? "true" : "false");
             for (size_t p = 0; p < c.mesh.patches.size(); ++p)

@@ -4,6 +4,7 @@
 // uniform/nonuniform field values.
 #include "foam_case.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -361,8 +362,8 @@ std::vector<PatchInfo> read_boundary(const std::string& path) {
     return out;
 }
 
-PolyMesh read_polymesh(const std::string& case_dir) {
-    const std::string base = case_dir + "/constant/polyMesh/";
+PolyMesh read_polymesh(const std::string& case_dir, const std::string& mesh) {
+    const std::string base = case_dir + "/constant/" + mesh + "/";
     PolyMesh m;
     m.points = read_points(base + "points");
     read_faces(base + "faces", m.face_offsets, m.face_points);
@@ -407,7 +408,7 @@ VolField read_vol_field(const std::string& path, int64_t n_cells, const std::vec
     return f;
 }
 
-Case read_case(const std::string& dir) {
+Case read_case(const std::string& dir, bool vmesh) {
     Case c;
     c.dir = dir;
     c.mesh = read_polymesh(dir);
@@ -425,6 +426,27 @@ Case read_case(const std::string& dir) {
     c.Pr = gp.at("Pr").number();
     c.K_inner = gp.find("KInner") ? static_cast<int>(gp.at("KInner").number()) : 0;   // fvDVM.C:1948
     c.xi_max = fp.at("xiMax").number();
+    if (vmesh) {
+        // the velocity mesh's cell centres and volumes, xiMax = max |xi|
+        // (fvDVM.C:166-196; 2-D drops z)
+        const PolyMesh vm = read_polymesh(dir, "vMesh");
+        const int64_t nF = vm.n_faces(), nv = vm.n_cells;
+        std::vector<double> Cf(3 * nF), Sf(3 * nF), C(3 * nv), V(nv);
+        const int st = dugks_mesh_geometry(static_cast<int32_t>(vm.points.size() / 3), vm.points.data(),
+                                           static_cast<int32_t>(nF), vm.face_offsets.data(), vm.face_points.data(),
+                                           vm.owner.data(), static_cast<int32_t>(vm.n_internal()),
+                                           vm.neighbour.data(), static_cast<int32_t>(nv), Cf.data(), Sf.data(),
+                                           C.data(), V.data());
+        if (st != DUGKS_OK) throw FoamError("constant/vMesh: geometry failed");
+        c.xi_max = 0;
+        for (int64_t i = 0; i < nv; ++i) {
+            if (c.D == 2) C[3 * i + 2] = 0.0;
+            c.xi_max = std::max(c.xi_max, std::sqrt(C[3 * i] * C[3 * i] + C[3 * i + 1] * C[3 * i + 1] +
+                                                    C[3 * i + 2] * C[3 * i + 2]));
+        }
+        c.dv_xi = C;
+        c.dv_w = V;
+    }
     if (const FoamValue* mf = fp.find("macroFlux")) c.macro_flux = mf->kind == FoamValue::Word && mf->word == "yes";
     const int64_t nc = c.mesh.n_cells;
     const VolField rho = read_vol_field(dir + "/0/rho", nc, c.mesh.patches);

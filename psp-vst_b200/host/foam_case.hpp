@@ -62,7 +62,8 @@ struct PolyMesh {
     int64_t n_internal() const { return static_cast<int64_t>(neighbour.size()); }
 };
 // n_solution_dims = 3 minus the number of non-empty patches of type empty
-PolyMesh read_polymesh(const std::string& case_dir);
+// constant/<mesh> of a case (polyMesh; vMesh: the velocity mesh)
+PolyMesh read_polymesh(const std::string& case_dir, const std::string& mesh = "polyMesh");
 
 // a volScalarField or volVectorField: internal values and, per patch, the
 // type and the first face value (the patch values the boundary conditions use)
@@ -95,6 +96,9 @@ struct Case {
     std::vector<double> xis, weights;   // one-dimensional DV set
     double xi_max = 0;
     bool macro_flux = false;            // fvDVMparas macroFlux yes
+    // DV list from constant/vMesh (the VMESH build, fvDVM.C:129-277): xi = its
+    // cell centres [n*3], weights = its cell volumes; empty = tensor product
+    std::vector<double> dv_xi, dv_w;
     double R = 0, omega = 0, Tref = 0, mu_ref = 0, Pr = 0;
     int K_inner = 0;
     std::vector<PatchKind> kinds;       // per mesh patch
@@ -109,7 +113,8 @@ struct Case {
     bool adjust_time_step = false;
     double max_co = 1.0, max_delta_t = 1.0e15;
 };
-Case read_case(const std::string& dir);
+// vmesh: take the DVs from constant/vMesh instead of Xis/weights
+Case read_case(const std::string& dir, bool vmesh = false);
 
 // fv addressing and geometry for dugks_create: internal faces, then the faces
 // of the non-empty patches in patch order (empty patches have no fv faces)

@@ -20,7 +20,14 @@ FvDVM::FvDVM(const Case& c, int precision, int device) : case_(c), flat_(flatten
     opt.precision = precision;
     opt.device = device;
     opt.macro_flux = case_.macro_flux ? 1 : 0;
-    const int st = dugks_create(&mesh, &dv, &gas, &bc, &opt, &h_);
+    int st;
+    if (!case_.dv_w.empty()) {
+        const dugks_dv_list dl{static_cast<int32_t>(case_.dv_w.size()), case_.dv_xi.data(), case_.dv_w.data(),
+                               case_.xi_max};
+        st = dugks_create_dv_list(&mesh, &dl, &gas, &bc, &opt, nullptr, &h_);
+    } else {
+        st = dugks_create(&mesh, &dv, &gas, &bc, &opt, &h_);
+    }
     if (st != DUGKS_OK) {
         const std::string msg = h_ ? dugks_last_error(h_) : "dugks_create failed";
         if (h_) dugks_destroy(h_);

@@ -82,6 +82,11 @@ class Case:
     T0: np.ndarray
     dt: float = 0.0
     macro_flux: bool = False        # fvDVMparas macroFlux yes
+    # a DV list instead of the tensor product of xis (the unstructured
+    # velocity mesh: xi = vMesh cell centres [n, 3], w = their volumes [n])
+    dv_xi: np.ndarray | None = None
+    dv_w: np.ndarray | None = None
+    vmesh: object = None            # the velocity PolyMesh they came from
     flat: dict = field(default_factory=dict)
     geometry: dict = field(default_factory=dict)
 
@@ -91,6 +96,8 @@ class Case:
 
     @property
     def n_dv(self) -> int:
+        if self.dv_w is not None:
+            return len(self.dv_w)
         return len(self.xis) ** self.D
 
     def flatten(self, geometry: dict | None = None) -> "Case":
@@ -146,7 +153,28 @@ class Case:
         return self
 
     def dv_set(self) -> tuple[np.ndarray, np.ndarray]:
+        if self.dv_w is not None:
+            xi = np.array(self.dv_xi, dtype=np.float64).reshape(-1, 3)
+            if self.D == 2:
+                xi[:, 2] = 0.0
+            return xi, np.asarray(self.dv_w, dtype=np.float64)
         return quadrature.tensor_product(self.xis, self.weights, self.D)
+
+    def use_velocity_mesh(self, vmesh, geometry: dict | None = None) -> "Case":
+        """DVs from an unstructured velocity mesh (the reference's VMESH
+        build, fvDVM.C:166-196): xi = cell centres, weights = cell volumes,
+        xiMax = max |xi|."""
+        if geometry is None:
+            from . import lib
+            geometry = lib.mesh_geometry(vmesh)
+        xi = np.array(geometry["C"], dtype=np.float64)
+        if self.D == 2:
+            xi[:, 2] = 0.0
+        self.dv_xi = xi
+        self.dv_w = np.array(geometry["V"], dtype=np.float64)
+        self.vmesh = vmesh
+        self.xi_max = float(np.max(np.linalg.norm(xi, axis=1)))
+        return self
 
 
 def cfl_dt(case: Case, co: float) -> float:
@@ -213,9 +241,10 @@ def channel_case(nx: int = 24, ny: int = 12, n_dv: int = 16, sides: dict | None 
     return c.flatten(geometry) if flatten else c
 
 
-def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None) -> Case:
+def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None, vmesh: bool = False) -> Case:
     """The reference demo cavity read from its case files (polyMesh, Xis,
-    weights, DVMProperties, 0/rho, 0/U, 0/T)."""
+    weights, DVMProperties, 0/rho, 0/U, 0/T); vmesh: the DVs from
+    constant/vMesh instead of Xis and weights."""
     from . import foamio
     mesh = meshgen.read_polymesh(case_dir)
     xis = foamio.read_scalar_list(f"{case_dir}/constant/Xis")
@@ -252,6 +281,8 @@ def demo_cavity_case(case_dir: str, flatten: bool = True, geometry=None) -> Case
     c = Case("demo_cavity60", mesh, mesh.n_solution_dims, gas, xis, w, val(fp["xiMax"]), patches,
              rho["internal"], U["internal"], T["internal"])
     c.macro_flux = str(fp.get("macroFlux", "no")) == "yes"
+    if vmesh:
+        c.use_velocity_mesh(meshgen.read_polymesh(case_dir, 3, mesh="vMesh"))
     return c.flatten(geometry) if flatten else c
 
 

@@ -48,6 +48,10 @@ class DVSet(C.Structure):
     _fields_ = [("n_per_dim", C.c_int32), ("xis", _dp), ("weights", _dp), ("xi_max", C.c_double)]
 
 
+class DVList(C.Structure):
+    _fields_ = [("n_dv", C.c_int32), ("xi", _dp), ("weights", _dp), ("xi_max", C.c_double)]
+
+
 class Gas(C.Structure):
     _fields_ = [("R", C.c_double), ("omega", C.c_double), ("Tref", C.c_double), ("mu_ref", C.c_double),
                 ("Pr", C.c_double), ("K_inner", C.c_int32)]
@@ -140,6 +144,8 @@ SIGNATURES = {
     "dugks_create_sharded": (C.c_int, [C.POINTER(Mesh), C.POINTER(DVSet), C.POINTER(Gas), C.POINTER(BC),
                                        C.POINTER(Options), C.POINTER(Shard), C.POINTER(C.c_void_p)]),
     "dugks_dv_range": (C.c_int, [C.c_void_p, _i32p, _i32p]),
+    "dugks_create_dv_list": (C.c_int, [C.POINTER(Mesh), C.POINTER(DVList), C.POINTER(Gas), C.POINTER(BC),
+                                       C.POINTER(Options), C.POINTER(Shard), C.POINTER(C.c_void_p)]),
     "dugks_shard_phase": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.POINTER(_dp), _i64p]),
     "dugks_last_step_ms": (C.c_int, [C.c_void_p, _dp]),
     "dugks_step_timed": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
@@ -245,7 +251,17 @@ class Solver:
             macro_flux = getattr(case, "macro_flux", False)
         opt.macro_flux = 1 if macro_flux else 0
         h = C.c_void_p()
-        if shard is None:
+        if getattr(case, "dv_w", None) is not None:
+            dxi, dw = case.dv_set()
+            dxi = keep(dxi.reshape(-1), np.float64)
+            dw = keep(dw, np.float64)
+            self.dv_list = DVList(len(dw), ptr(dxi), ptr(dw), case.xi_max)
+            if shard is not None and shard.use_nccl:
+                _load_torch_nccl()
+            st = self.lib.dugks_create_dv_list(C.byref(self.mesh), C.byref(self.dv_list), C.byref(self.gas),
+                                               C.byref(self.bc), C.byref(opt),
+                                               C.byref(shard) if shard is not None else None, C.byref(h))
+        elif shard is None:
             st = self.lib.dugks_create(C.byref(self.mesh), C.byref(self.dv), C.byref(self.gas), C.byref(self.bc),
                                        C.byref(opt), C.byref(h))
         else:

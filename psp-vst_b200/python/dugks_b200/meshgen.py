@@ -185,6 +185,33 @@ def channel(nx: int, ny: int, lx: float = 2.0, ly: float = 1.0, thickness: float
                               ("frontAndBack", "empty")], n_solution_dims=2)
 
 
+def velocity_box(n: int, half_width: float, D: int, jitter: float = 0.0, seed: int = 7,
+                 thickness: float = 1.0) -> PolyMesh:
+    """An unstructured-looking velocity mesh: the box [-L, L]^D in n cells per
+    direction (2-D: one cell of ``thickness`` in z, whose volume is the DV
+    weight), interior points moved by up to ``jitter`` of a cell width so
+    that the cell centres are no tensor product."""
+    nz = n if D == 3 else 1
+    lz = 2.0 * half_width if D == 3 else thickness
+    pts, cells = _box_hexes(n, n, nz, 2.0 * half_width, 2.0 * half_width, lz)
+    pts = pts.copy()
+    pts[:, 0] -= half_width
+    pts[:, 1] -= half_width
+    if D == 3:
+        pts[:, 2] -= half_width
+    if jitter > 0:
+        rng = np.random.default_rng(seed)
+        h = 2.0 * half_width / n
+        inner = np.all(np.abs(pts[:, :D]) < half_width - 1e-9 * half_width, axis=1)
+        pts[inner, :D] += rng.uniform(-jitter * h, jitter * h, size=(int(inner.sum()), D))
+    tol = 1e-9 * half_width
+
+    def classify(c):
+        return np.zeros(len(c), dtype=np.int64)
+
+    return hexes_to_polymesh(pts, cells, classify, [("outside", "patch")], n_solution_dims=D)
+
+
 def cube(n: int) -> PolyMesh:
     pts, cells = _box_hexes(n, n, n, 1.0, 1.0, 1.0)
     tol = 1e-9
@@ -256,10 +283,11 @@ def cubed_sphere(m: int = 24, nr: int = 32, stretch: float = 1.12, r0: float = 1
     return hexes_to_polymesh(pts, cells, classify, [("wall", "wall"), ("farField", "patch")], n_solution_dims=3)
 
 
-def read_polymesh(case_dir: str, n_solution_dims: int | None = None) -> PolyMesh:
-    """Read ``constant/polyMesh`` of an OpenFOAM case."""
+def read_polymesh(case_dir: str, n_solution_dims: int | None = None, mesh: str = "polyMesh") -> PolyMesh:
+    """Read ``constant/<mesh>`` of an OpenFOAM case (polyMesh, or vMesh for
+    the velocity mesh)."""
     from . import foamio
-    base = f"{case_dir}/constant/polyMesh"
+    base = f"{case_dir}/constant/{mesh}"
     pts = foamio.read_points(f"{base}/points")
     offs, labels = foamio.read_faces(f"{base}/faces")
     owner = foamio.read_label_list(f"{base}/owner")

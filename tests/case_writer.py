@@ -26,8 +26,26 @@ def _list(vals) -> str:
     return f"{len(vals)}\n(\n" + "\n".join(vals) + "\n)\n"
 
 
+def _write_polymesh(pm, mesh):
+    _write(os.path.join(mesh, "points"), "vectorField", "points",
+           _list(["(%s %s %s)" % tuple(_num(v) for v in p) for p in pm.points]))
+    faces = []
+    for k in range(pm.n_faces):
+        lab = pm.face_points[pm.face_offsets[k]:pm.face_offsets[k + 1]]
+        faces.append(f"{len(lab)}(" + " ".join(str(int(v)) for v in lab) + ")")
+    _write(os.path.join(mesh, "faces"), "faceList", "faces", _list(faces))
+    _write(os.path.join(mesh, "owner"), "labelList", "owner", _list([str(int(v)) for v in pm.owner]))
+    _write(os.path.join(mesh, "neighbour"), "labelList", "neighbour", _list([str(int(v)) for v in pm.neighbour]))
+    bnd = []
+    for p in pm.patches:
+        bnd.append(f"{p['name']}\n{{\n    type {p['type']};\n    nFaces {p['nFaces']};\n    startFace {p['startFace']};\n}}")
+    _write(os.path.join(mesh, "boundary"), "polyBoundaryMesh", "boundary", _list(bnd))
+
+
 def write_case(case, directory, control: dict | None = None, rho_patch_type: dict | None = None):
     pm = case.mesh
+    if getattr(case, "vmesh", None) is not None:
+        _write_polymesh(case.vmesh, os.path.join(directory, "constant", "vMesh"))
     mesh = os.path.join(directory, "constant", "polyMesh")
     _write(os.path.join(mesh, "points"), "vectorField", "points",
            _list(["(%s %s %s)" % tuple(_num(v) for v in p) for p in pm.points]))

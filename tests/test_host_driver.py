@@ -220,3 +220,31 @@ def test_check_reads_macro_flux(driver, tmp_path):
     c.macro_flux = False
     d = case_writer.write_case(c, str(tmp_path / "nomf"))
     assert _summary(_run(driver, d, "--check"))["macro_flux"] is False
+
+
+def _vmesh_case():
+    from dugks_b200 import meshgen
+    c = cs.cavity_case(6, 6, flatten=False)
+    c.use_velocity_mesh(meshgen.velocity_box(8, 1600.0, 2, jitter=0.2))
+    return c.flatten()
+
+
+def test_check_reads_the_velocity_mesh(driver, tmp_path):
+    c = _vmesh_case()
+    d = case_writer.write_case(c, str(tmp_path / "vm"))
+    s = _summary(_run(driver, d, "--check", "--vmesh"))
+    assert s["n_dv"] == 64 and s["xi_max"] == pytest.approx(c.xi_max, rel=1e-14)
+    assert _summary(_run(driver, d, "--check"))["n_dv"] == 36      # 6^2 from Xis without --vmesh
+
+
+@pytest.mark.gpu
+def test_driver_velocity_mesh_matches_python_solver(driver, tmp_path):
+    c = _vmesh_case()
+    d = case_writer.write_case(c, str(tmp_path / "vm"))
+    s = _summary(_run(driver, d, "--vmesh", "--steps", 4, "--dt", repr(c.dt)))
+    assert s["n_dv"] == 64
+    ref = dl.Solver(c)
+    ref.step(4, c.dt)
+    sizes = {p["name"]: p["nFaces"] for p in c.mesh.patches}
+    rho = foamio.read_vol_field(os.path.join(d, s["time_name"], "rho"), c.n_cells, sizes)
+    np.testing.assert_allclose(rho["internal"], ref.macros()["rho"], rtol=1e-13, atol=0)
