@@ -8,11 +8,13 @@
 // Pass A: one CTA of 512 threads per (tile, DV chunk).  A tile is up to 128
 // L0 cells, their L1 ring (up to 256 local cells in all) and its items = the
 // faces touching L0 (up to 512, one per thread), sorted by kind.  Per batch:
-//   stage 0  cp.async of the NEXT batch's g~, h~ and one-dimensional
-//            Maxwellian factors of the local cells into shared memory,
-//            overlapping this batch's stages
+//   stage 0  cp.async of the NEXT batch's g~, h~ (and, for DV sets of more
+//            than 2 NB nodes per dimension, x Maxwellian factors) of the
+//            local cells into shared memory, overlapping this batch's stages
 //   stage 1  gbar+/hbar+ of the local cells (updateGHbarPvol,
-//            fvDVM.C:648-683)
+//            fvDVM.C:648-683); the y and z Maxwellian factors of the row are
+//            computed here from the cell record: two exponentials per cell
+//            cost less than gathering them for the ring cells
 //   stage 2  least-squares gradients of the L0 cells (leastSquaresGrad;
 //            the zero-gradient boundary terms vanish, fvDVM.C:456-485,
 //            :775-809)
@@ -251,7 +253,6 @@ struct SmemA {
     // dimension, the whole table [n1d][kSL] is loaded once per CTA (e_x does
     // not depend on the row); otherwise [2][NB][kSL] staged per batch
     double* stgx;
-    double* stgyz;  // [2][2][kSL] staged e_y, e_z
     Real* stg;      // [2][2][NB][kSL] staged g~, h~
     Real* gB;       // [NB][kSL] gbar+
     Real* hB;
@@ -261,7 +262,7 @@ struct SmemA {
     Real* sls;      // [kMaxRegStencil][D][kS0] and least-squares vector
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) + static_cast<size_t>(kMaxRegStencil) * kS0 * sizeof(int) +
-               (static_cast<size_t>(CR_N) * kSL + 2 * NB * kSL + 2 * 2 * kSL) * sizeof(double) +
+               (static_cast<size_t>(CR_N) * kSL + 2 * NB * kSL) * sizeof(double) +
                (2 * 2 * static_cast<size_t>(NB) * kSL + 2 * NB * kSL + 2 * NB * D * kS0 +
                 static_cast<size_t>(kMaxRegStencil) * D * kS0) *
                    sizeof(Real);
@@ -275,8 +276,7 @@ __device__ __forceinline__ SmemA<D, Real, NB> carve_a(unsigned char* base) {
     s.w1 = s.x1 + kMaxN1d;
     s.crec = s.w1 + kMaxN1d;
     s.stgx = s.crec + CR_N * kSL;
-    s.stgyz = s.stgx + 2 * NB * kSL;
-    Real* p = reinterpret_cast<Real*>(s.stgyz + 2 * 2 * kSL);
+    Real* p = reinterpret_cast<Real*>(s.stgx + 2 * NB * kSL);
     s.stg = p;
     p += 2 * 2 * NB * kSL;
     s.gB = p;
@@ -451,9 +451,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
                 if (!ex_res) cp_async(sx + j * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
             }
         }
-        double* syz = sm.stgyz + buf * 2 * kSL;
-        if (part == 0) cp_async(syz + l, ctab + static_cast<size_t>(m.n1d + bp.iy) * nC + c);
-        else if (D == 3) cp_async(syz + kSL + l, ctab + static_cast<size_t>(2 * m.n1d + bp.iz) * nC + c);
+
     }
     cp_commit();
 }
@@ -468,10 +466,14 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
     s.qx = sm.crec[CR_QX * kSL + l];
     s.RTh = sm.crec[CR_RTH * kSL + l];
     s.omr = sm.crec[CR_OMR * kSL + l];
-    const double* syz = sm.stgyz + buf * 2 * kSL;
-    shk_batch<D, double>(s, sm.crec[CR_UY * kSL + l], sm.crec[CR_UZ * kSL + l], sm.crec[CR_QY * kSL + l],
-                         sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y, q.Z, syz[l],
-                         D == 3 ? syz[kSL + l] : 1.0);
+    // the y and z Maxwellian factors of the batch's row, as the combine
+    // kernels tabulate them (write_maxwell_tables): exp(-x^2/2 invRT)
+    const double uy = sm.crec[CR_UY * kSL + l], uz = sm.crec[CR_UZ * kSL + l];
+    const double yy = q.Y - uy, zz = q.Z - uz;
+    const double ey = exp(-0.5 * yy * yy * s.invRT);
+    const double ez = D == 3 ? exp(-0.5 * zz * zz * s.invRT) : 1.0;
+    shk_batch<D, double>(s, uy, uz, sm.crec[CR_QY * kSL + l], sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y,
+                         q.Z, ey, ez);
     const Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
     const double* sx = sm.stgx + (ex_res ? bp.ix0 : buf * NB) * kSL;
     constexpr int H = NB / kPartsL;
