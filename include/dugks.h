@@ -227,9 +227,11 @@ int dugks_nccl_unique_id(unsigned char id[128]);
 
 /* dugks_create (shard NULL) or dugks_create_sharded with a DV list.  The
  * passes then evaluate each DV's Maxwellian with its own exponential (the
- * tensor-product factoring does not apply).  Not built for DV lists:
- * symmetry patches (the reference's VMESH build leaves their mirror ids
- * unset) and macroFlux yes (its VMESH branch, fvDVM.C:1562-1611). */
+ * tensor-product factoring does not apply).  macroFlux yes takes the VMESH
+ * branch (fvDVM.C:1562-1611): the cell rho, rho U, rho E advance by the
+ * fluxes of the relaxed face DFs.  Not built for DV lists: symmetry patches
+ * (the reference's VMESH build leaves their mirror ids unset), and
+ * macroFlux yes on more than one shard. */
 int dugks_create_dv_list(const dugks_mesh* mesh, const dugks_dv_list* dv, const dugks_gas* gas,
                          const dugks_bc* bc, const dugks_options* opt, const dugks_dv_shard* shard,
                          dugks_handle** out);

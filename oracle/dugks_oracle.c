@@ -391,7 +391,7 @@ static inline double tau_of(const oracle_state* s, double T, double rho) {
     return s->muRef * exp(s->omega * log(T / s->Tref)) / rho / T / s->R;
 }
 
-void oracle_set_macro_flux(oracle_state* s, int on) { s->macro_flux = on != 0; }
+void oracle_set_macro_flux(oracle_state* s, int mode) { s->macro_flux = mode == 2 ? 2 : (mode != 0); }
 
 void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b) {
     s->n1d = n_dv_1d;
@@ -792,7 +792,53 @@ void oracle_evolve(oracle_state* s, double dt) {
      *      patch-local index (fvDVM.C:1668-1669, Sf is the internal field).
      *      "X & Sf*dt/V" is X & ((Sf dt)/V) by C++ precedence. */
     double *mrho = NULL, *mrU = NULL, *mrE = NULL;
-    if (s->macro_flux) {
+    if (s->macro_flux == 2) {
+        /* 11b. the unstructured-velocity-mesh branch (fvDVM.C:1562-1611):
+         *      fluxes from the relaxed face DFs of every DV, DVs in order,
+         *      internal faces then boundary faces; dXiCellSize = 1 (:1934-1939) */
+        double* fr = dup(NULL, nC);
+        double* fU = dup(NULL, 3 * (size_t)nC);
+        double* fE = dup(NULL, nC);
+        for (int dvi = 0; dvi < nv; ++dvi) {
+            const double* xi = s->xi + 3 * dvi;
+            const double w = 1.0 * s->wv[dvi], xi2 = magsqr3(xi);
+            for (int f = 0; f < nIF + nBF; ++f) {
+                const int internal = f < nIF;
+                const double g = internal ? s->gS[(size_t)dvi * nIF + f] : s->gSb[(size_t)dvi * nBF + f - nIF];
+                const double h = internal ? s->hS[(size_t)dvi * nIF + f] : s->hSb[(size_t)dvi * nBF + f - nIF];
+                const double rf = w * g, ef = 0.5 * 1.0 * s->wv[dvi] * (g * xi2 + h);
+                const double xs = dot3(xi, s->Sf + 3 * f);
+                for (int side = 0; side < (internal ? 2 : 1); ++side) {
+                    const int64_t c = side == 0 ? s->own[f] : s->nei[f];
+                    const double V = s->V[c];
+                    const double dr = xs * rf * dt / V, dE = xs * ef * dt / V;
+                    double dU[3];
+                    for (int k = 0; k < 3; ++k) dU[k] = xs * (rf * xi[k]) * dt / V;
+                    if (side == 0) {
+                        fr[c] -= dr;
+                        for (int k = 0; k < 3; ++k) fU[3 * c + k] -= dU[k];
+                        fE[c] -= dE;
+                    } else {
+                        fr[c] += dr;
+                        for (int k = 0; k < 3; ++k) fU[3 * c + k] += dU[k];
+                        fE[c] += dE;
+                    }
+                }
+            }
+        }
+        mrho = dup(NULL, nC);
+        mrU = dup(NULL, 3 * (size_t)nC);
+        mrE = dup(NULL, nC);
+        for (int c = 0; c < nC; ++c) {
+            const double* U = s->U + 3 * c;
+            mrho[c] = s->rho[c] + fr[c];
+            for (int k = 0; k < 3; ++k) mrU[3 * c + k] = s->rho[c] * U[k] + fU[3 * c + k];
+            mrE[c] = s->rho[c] * (0.5 * magsqr3(U) + (K + 3) / 2.0 * R * s->T[c]) + fE[c];
+        }
+        free(fr);
+        free(fU);
+        free(fE);
+    } else if (s->macro_flux) {
         mrho = dup(NULL, nC);
         mrU = dup(NULL, 3 * (size_t)nC);
         mrE = dup(NULL, nC);

@@ -65,9 +65,11 @@ void oracle_destroy(oracle_state* s);
  * oracle_set_macros when the mesh has such patches. */
 void oracle_set_patch_extra(oracle_state* s, int n_dv_1d, const double* p_b);
 
-/* fvDVMparas macroFlux (fvDVM.C:1940): nonzero = "yes", the cell rho, rho U
- * and rho E advance by the face macro fluxes (fvDVM.C:1613-1679). */
-void oracle_set_macro_flux(oracle_state* s, int on);
+/* fvDVMparas macroFlux (fvDVM.C:1940): 0 "no"; 1 "yes", the cell rho, rho U
+ * and rho E advance by the face macro fluxes (fvDVM.C:1613-1679); 2 "yes" in
+ * the unstructured-velocity-mesh build, by the fluxes of the relaxed face
+ * DFs (fvDVM.C:1562-1611). */
+void oracle_set_macro_flux(oracle_state* s, int mode);
 
 /* fvDVM ctor tail: initialiseDV (Maxwellian g/h), setCalculatedMaxwellRhoBC,
  * updateTau, linear Usurf (fvDVM.C:2110-2116). */

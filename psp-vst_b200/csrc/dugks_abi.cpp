@@ -165,8 +165,8 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: n_solution_dims must be 2 or 3");
     if (dvl) {
         if (dvl->n_dv < 1 || !dvl->xi || !dvl->weights) return fail(DUGKS_ERR_ARG, "dugks_create_dv_list: empty DV list");
-        if (opt.macro_flux)
-            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_dv_list: macroFlux yes is not built for DV lists");
+        if (opt.macro_flux && shard && shard->world > 1)
+            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_dv_list: macroFlux yes is not built for DV shards");
     } else if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) {
         return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
     }
@@ -491,6 +491,7 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     ds.cur = 0;
     if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
+        (dvl && opt.macro_flux && (st = dev_alloc(h, &ds.partX, static_cast<size_t>(chunks) * nC * dugks::kFX))) ||
         (st = dev_alloc(h, &ds.cellrec, static_cast<size_t>(dugks::REC_N) * nC)) ||
         (st = dev_alloc(h, &ds.facerec, static_cast<size_t>(dugks::REC_N) * dm.n_items)) ||
         (st = dev_alloc(h, &ds.ctab, static_cast<size_t>(h->D) * h->n1d * nC)) ||

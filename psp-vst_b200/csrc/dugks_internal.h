@@ -18,6 +18,7 @@ constexpr int kMaxLocal = 256;     // L0 + L1 cells per tile at most
 constexpr int kMaxItems = kThreads - 1;  // items per tile at most (one per thread; one flux slot kept zero)
 constexpr int kMaxN1d = 64;        // DV nodes per dimension at most
 constexpr int kNM = 16;            // stride of a partial-moment record (doubles)
+constexpr int kFX = 8;             // stride of a flux-moment record: M0, M1[3], W/2
 constexpr double kVSmall = 1.0e-300;  // OpenFOAM VSMALL (upwind switch, fvDVM.C:829-847)
 
 // Moment record layout (raw velocity moments of one face or cell, summed
@@ -132,6 +133,7 @@ struct DevState {
     void* fvh;
     double* partF;     // [chunks][n_items][kNM]
     double* partC;     // [chunks][nC][kNM]
+    double* partX;     // [chunks][nC][kFX] DV-list macroFlux: moments of the flux term (else null)
     double* cellrec;   // [REC_N][nC]
     // face records in item order (each face's record is written to its one
     // or two items, so that a tile reads its faces' records contiguously)

@@ -245,7 +245,23 @@ __global__ void k_cell_combine(const StepArgs a, Consts k, double dt_next) {
         // rho, U, T from the fluxes; q from the DF moments about that U:
         // q = 1/2 [V3 - 2 M2.U + |U|^2 M1 - U W + 2 U (M1.U) - U |U|^2 M0]
         double rU[3], rE;
-        macro_flux_update(a, k, c, rho, rU, rE);
+        if (!m.general_dv) {
+            macro_flux_update(a, k, c, rho, rU, rE);
+        } else {
+            // the velocity-mesh branch (fvDVM.C:1562-1611): the old rho, rho U,
+            // rho E plus the moments of the update's flux term (pass B)
+            const double* cm = a.ds.cm + static_cast<size_t>(c) * 9;
+            double f[5] = {0, 0, 0, 0, 0};
+            for (int ch = 0; ch < a.chunks; ++ch) {
+                const double* p = a.ds.partX + (static_cast<size_t>(ch) * m.nC + c) * kFX;
+                for (int j = 0; j < 5; ++j) f[j] += p[j];
+            }
+            const double U0[3] = {cm[1], cm[2], cm[3]};
+            rho = cm[0] + f[0];
+            for (int i = 0; i < 3; ++i) rU[i] = cm[0] * U0[i] + f[1 + i];
+            rE = cm[0] * (0.5 * (U0[0] * U0[0] + U0[1] * U0[1] + U0[2] * U0[2]) + (k.Kin + 3) / 2.0 * k.R * cm[4]) +
+                 f[4];
+        }
         for (int i = 0; i < 3; ++i) U[i] = rU[i] / rho;
         const double u2 = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
         T = (rE - 0.5 * rho * u2) / ((k.Kin + 3.0) / 2.0 * k.R * rho);

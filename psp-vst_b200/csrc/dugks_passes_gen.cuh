@@ -347,6 +347,9 @@ struct SmemBG {
     }
 };
 
+static_assert(static_cast<size_t>(kParts0 - 1) * kS0 * 20 * sizeof(double) <= 4 * 8 * kSI * sizeof(float),
+              "the cell-moment reduction must fit in the staging arrays");
+
 template <typename Real, int NB>
 __device__ __forceinline__ SmemBG<Real, NB> carve_bg(unsigned char* base) {
     SmemBG<Real, NB> s;
@@ -409,6 +412,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
+    // macroFlux yes (the velocity-mesh branch, fvDVM.C:1562-1611): the cell's
+    // rho, rho U, rho E gain sum_DV w (1, xi, |xi|^2/2 & h/2) times the flux
+    // term dt/V sum_f (+-)(xi.S) g_f of the update
+    double accx[5] = {0, 0, 0, 0, 0};
+    const bool fx = m.macro_flux != 0;
 
     const int d_first = t.r0 - m.row_base, d_end = t.r1 - m.row_base;
     const int nbt = (d_end - d_first + NB - 1) / NB;
@@ -496,20 +504,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
                 gn[idx] = g_new;
                 hn[idx] = h_new;
                 add_dv<D>(acc, xw[4 * j + 3], xi, double(g_new), double(h_new));
+                if (fx) {
+                    const double w = xw[4 * j + 3], fg = double(sg) * dtV, fhh = double(sh) * dtV;
+                    const double a = w * fg;
+                    accx[0] += a;
+                    accx[1] += a * xi[0];
+                    accx[2] += a * xi[1];
+                    accx[3] += a * xi[2];
+                    accx[4] += 0.5 * w * (fg * (xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2]) + fhh);
+                }
             }
         }
     }
     // the cell moments of a cell are split over kParts0 threads: reduce them
     // through shared memory in a fixed order
     __syncthreads();
-    if (part > 0 && has_cell)
-        for (int j = 0; j < 15; ++j) sm.red[((part - 1) * kS0 + lc) * 15 + j] = acc[j];
+    if (part > 0 && has_cell) {
+        for (int j = 0; j < 15; ++j) sm.red[((part - 1) * kS0 + lc) * 20 + j] = acc[j];
+        for (int j = 0; j < 5; ++j) sm.red[((part - 1) * kS0 + lc) * 20 + 15 + j] = accx[j];
+    }
     __syncthreads();
     if (part == 0 && has_cell) {
-        for (int p = 1; p < kParts0; ++p)
-            for (int j = 0; j < 15; ++j) acc[j] += sm.red[((p - 1) * kS0 + lc) * 15 + j];
+        for (int p = 1; p < kParts0; ++p) {
+            for (int j = 0; j < 15; ++j) acc[j] += sm.red[((p - 1) * kS0 + lc) * 20 + j];
+            for (int j = 0; j < 5; ++j) accx[j] += sm.red[((p - 1) * kS0 + lc) * 20 + 15 + j];
+        }
         double* dst = a.ds.partC + (static_cast<size_t>(blockIdx.y) * m.nC + c) * kNM;
 #pragma unroll
         for (int j = 0; j < 15; ++j) dst[j] = acc[j];
+        if (fx) {
+            double* dx = a.ds.partX + (static_cast<size_t>(blockIdx.y) * m.nC + c) * kFX;
+            for (int j = 0; j < 5; ++j) dx[j] = accx[j];
+        }
     }
 }

@@ -101,7 +101,9 @@ class Oracle:
         self.lib.oracle_set_patch_extra(self.s, len(case.xis), _p(self._p_b))
         if macro_flux is None:
             macro_flux = getattr(case, "macro_flux", False)
-        self.lib.oracle_set_macro_flux(self.s, 1 if macro_flux else 0)
+        # the velocity-mesh build takes the DF-flux branch of macroFlux yes
+        mode = (2 if getattr(case, "dv_w", None) is not None else 1) if macro_flux else 0
+        self.lib.oracle_set_macro_flux(self.s, mode)
         self.set_macros(case.rho0, case.U0, case.T0)
 
     def set_macros(self, rho, U, T):

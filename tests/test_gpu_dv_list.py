@@ -89,7 +89,7 @@ def test_velocity_mesh_shards_and_refusals():
     errs = ob.macro_errors(shards[0].macros(), orc.macros(), c.gas["R"])
     assert max(errs.values()) <= 1e-10, errs
     with pytest.raises(dl.DugksError) as e:
-        dl.Solver(c, macro_flux=True)
+        dl.Solver(c, macro_flux=True, shard=dl.shard(0, 2))
     assert e.value.code == 7
     s = cs.channel_case(6, 3, 6, sides={"top": {"kind": "symmetryPlane"}}, flatten=False)
     s.use_velocity_mesh(meshgen.velocity_box(6, 1600.0, 2))
@@ -97,3 +97,28 @@ def test_velocity_mesh_shards_and_refusals():
     with pytest.raises(dl.DugksError) as e:
         dl.Solver(s)
     assert e.value.code == 7
+
+
+# macroFlux yes on a velocity mesh (fvDVM.C:1562-1611): cell rho, rho U,
+# rho E advance by the fluxes of the relaxed face DFs
+@pytest.mark.parametrize("which", ["cavity", "pressure"])
+def test_velocity_mesh_macro_flux(which):
+    if which == "cavity":
+        c = _vmesh_cavity()
+    else:
+        p1 = cs.R_DEMO * 273.0
+        c = cs.channel_case(10, 5, 8, sides={"inlet": {"kind": "pressureIn", "p": 1.2 * p1, "T": 273.0},
+                                             "outlet": {"kind": "pressureOut", "p": p1, "T": 273.0}},
+                            flatten=False)
+        c.rho0 = np.full(c.n_cells, 1.0)
+        c.use_velocity_mesh(meshgen.velocity_box(10, 1600.0, 2, jitter=0.2))
+        c.flatten()
+    gpu, orc = dl.Solver(c, macro_flux=True), ob.Oracle(c, macro_flux=True)
+    for _ in range(8):
+        gpu.evolution(c.dt)
+        orc.evolution(c.dt)
+    errs = ob.macro_errors(gpu.macros(), orc.macros(), c.gas["R"])
+    assert max(errs.values()) <= 1e-10, errs
+    plain = dl.Solver(c)
+    plain.step(8, c.dt)
+    assert not np.array_equal(plain.macros()["rho"], gpu.macros()["rho"])

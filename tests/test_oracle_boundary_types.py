@@ -80,3 +80,23 @@ def test_macro_flux_conserves_mass_in_a_closed_cavity():
         o.evolution(c.dt)
     m = o.macros()
     assert abs(float(np.sum(m["rho"] * V)) - m0) <= 1e-13 * m0
+
+
+def test_velocity_mesh_macro_flux_keeps_a_gas_at_rest():
+    # the DF-flux branch (fvDVM.C:1562-1611) on a fine velocity mesh
+    # symmetric about zero (spacing 150 m/s, +-2400 m/s: its midpoint sums
+    # integrate the Maxwellian to round-off): between walls at rest and at
+    # the gas temperature, the uniform gas at rest stays put.  (Coarse or
+    # jittered velocity meshes do not integrate it exactly, so their rest
+    # state is no fixed point.)
+    from dugks_b200 import meshgen
+    c = cs.channel_case(6, 4, 6, flatten=False)
+    c.use_velocity_mesh(meshgen.velocity_box(32, 2400.0, 2))
+    c.flatten()
+    o = ob.Oracle(c, threads=2, macro_flux=True)
+    m0 = o.macros()
+    for _ in range(5):
+        o.evolution(c.dt)
+    m = o.macros()
+    assert np.max(np.abs(m["rho"] - m0["rho"])) <= 1e-12 * np.max(m0["rho"])
+    assert np.max(np.abs(m["U"])) <= 1e-9
