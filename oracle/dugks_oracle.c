@@ -27,28 +27,7 @@
 
 #define VSMALL 1.0e-300
 
-struct oracle_state {
-    int D, K;
-    double R, omega, Tref, muRef, Pr;
-    int nC, nIF, nBF, nP, nthreads;
-    int64_t *own, *nei;
-    double *C, *V, *Cf, *Sf, *magSf, *w, *dc;
-    double *lsP, *lsN, *lsB;
-    int *ptype, *pstart, *bf_patch, *bf_local;
-    double *rho_b, *U_b, *T_b;      /* rho patch values (farField keeps them), U/T patch values */
-    double *p_b;                    /* pressureIn / pressureOut values */
-    int n1d;                        /* DV nodes per dimension (symmetry targets) */
-    int macro_flux;                 /* fvDVMparas macroFlux yes */
-    double *inByRho, *outGoing;     /* calculatedMaxwell patch members */
-    int nv;
-    double *xi, *wv, xi_max;
-    /* state (DV-major, as fvDVM.C:403-408) */
-    double *gT, *hT, *gBP, *hBP, *gS, *hS, *gSb, *hSb;
-    /* cell macros */
-    double *rho, *U, *T, *q, *tau;
-    /* face macros, internal then boundary */
-    double *rhoF, *UF, *TF, *qF, *tauF;
-};
+#include "dugks_oracle_state.h"
 
 static inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 static inline double magsqr3(const double* a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }

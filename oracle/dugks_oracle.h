@@ -95,6 +95,18 @@ void oracle_get_face_values(oracle_state* s, double* g_int, double* h_int, doubl
 void oracle_get_ls(oracle_state* s, double* p, double* n, double* b);
 void oracle_get_weights(oracle_state* s, double* w, double* delta_coeffs);
 
+/* Tangent-linear run (dugks_tangent.cpp): n_steps steps of dt from the
+ * current state, which is left unchanged, on dual numbers.  J = 1/N sum
+ * over steps and boundary faces b and DVs i of w_i (xi_i . S_b)
+ * [heat_w_b (|xi_i|^2 g + h)/2 + (force_w_b . xi_i) g] over the relaxed
+ * boundary-face DFs; dJ = its derivative along the direction (dT_b per
+ * boundary face, dU_b per boundary face, d_muRef).  NULL weights or
+ * directions are zero.  g_out / h_out (or NULL) get the final g~, h~.
+ * Returns -1 for patches other than maxwellWall and farField or macroFlux. */
+int oracle_tangent(const oracle_state* s, int n_steps, double dt, const double* heat_w, const double* force_w,
+                   const double* dT_b, const double* dU_b, double d_muRef, double* J, double* dJ, double* g_out,
+                   double* h_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,9 @@ def load():
     lib.oracle_get_face_values.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
     lib.oracle_get_ls.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.oracle_get_weights.argtypes = [C.c_void_p, _dp, _dp]
+    lib.oracle_tangent.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                   _dp]
+    lib.oracle_tangent.restype = C.c_int
     _lib = lib
     return lib
 
@@ -173,6 +176,30 @@ class Oracle:
         self.lib.oracle_get_ls(self.s, _p(p), _p(n), _p(b))
         return p, n, b
 
+    def face_values(self):
+        """Relaxed face DFs of the last step, DV-major: internal g, h and
+        boundary g, h."""
+        fl = self.case.flat
+        out = [np.zeros((self.n_dv, fl[k])) for k in ("n_internal", "n_internal", "n_boundary", "n_boundary")]
+        self.lib.oracle_get_face_values(self.s, *[_p(a) for a in out])
+        return out
+
+    def tangent(self, n_steps, dt, heat_w=None, force_w=None, dT_b=None, dU_b=None, d_mu=0.0):
+        """Objective J of n_steps from the current state and its derivative
+        along (dT_b, dU_b, d_mu), on the dual-number restatement; the state is
+        left unchanged.  Returns (J, dJ, g, h) with the final g~, h~."""
+        nb = self.case.flat["n_boundary"]
+        arr = lambda a, n: None if a is None else np.ascontiguousarray(np.reshape(a, n), dtype=np.float64)  # noqa: E731
+        hw, fw, dT, dU = arr(heat_w, nb), arr(force_w, 3 * nb), arr(dT_b, nb), arr(dU_b, 3 * nb)
+        J, dJ = C.c_double(), C.c_double()
+        g = np.zeros((self.n_dv, self.case.n_cells))
+        h = np.zeros((self.n_dv, self.case.n_cells))
+        rc = self.lib.oracle_tangent(self.s, int(n_steps), float(dt), _p(hw), _p(fw), _p(dT), _p(dU), float(d_mu),
+                                     C.byref(J), C.byref(dJ), _p(g), _p(h))
+        if rc != 0:
+            raise ValueError("oracle_tangent: maxwellWall and farField patches only, macroFlux no")
+        return J.value, dJ.value, g, h
+
     def close(self):
         if getattr(self, "s", None):
             self.lib.oracle_destroy(self.s)
@@ -183,6 +210,19 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def boundary_flux_objective(case, xi, w, g_b, h_b, heat_w, force_w) -> float:
+    """One step's term of the boundary-flux objective from relaxed boundary
+    face DFs g_b, h_b [dv][boundary face]: sum over faces b and DVs i of
+    w_i (xi_i . S_b) [heat_w_b (|xi_i|^2 g + h)/2 + (force_w_b . xi_i) g]."""
+    fl = case.flat
+    Sb = np.asarray(fl["Sf"])[fl["n_internal"]:]
+    xs = np.asarray(xi) @ Sb.T                                   # [dv, b]
+    wx = np.asarray(w)[:, None] * xs
+    x2 = np.sum(np.asarray(xi) ** 2, axis=1)[:, None]
+    cg = np.asarray(xi) @ np.reshape(force_w, (-1, 3)).T          # [dv, b]
+    return float(np.sum(wx * (np.asarray(heat_w)[None, :] * 0.5 * (x2 * g_b + h_b) + cg * g_b)))
 
 
 def rel_l2(a, b) -> float:
