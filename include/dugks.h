@@ -343,6 +343,51 @@ int64_t dugks_batch_graph_kernels(const dugks_batch* b);
 const char* dugks_batch_last_error(const dugks_batch* b);
 void dugks_batch_destroy(dugks_batch* b);
 
+/* Discrete adjoint of the FP64 step (no counterpart in the reference: it
+ * differentiates fvDVM::evolution, fvDVM.C:2128-2174, in reverse mode).
+ * The objective of a run of n_steps fixed-dt steps from the handle's
+ * current state is the time average, over steps window_start .. n_steps-1,
+ * of the energy and momentum flux through the boundary faces carried by the
+ * relaxed boundary DFs of each step (the fluxes of fvDVM::updateGHtildeVol,
+ * fvDVM.C:1500-1517):
+ *   J_n = sum_b sum_i w_i (xi_i . Sf_b) [a_b (|xi_i|^2 g + h) / 2 + (c_b . xi_i) g]
+ * a_b = energy_weight[b] (wall heat flux: 1 on the wall faces), c_b =
+ * momentum_weight[3b..] (lid shear: (1,0,0) on the lid faces); NULL means 0.
+ * The gradient is taken with respect to the T and U patch values of every
+ * boundary face (boundary face b is mesh face n_internal_faces + b) and
+ * muRef; Kn is proportional to muRef, so dJ/dKn = dJ/dmuRef muRef / Kn.
+ * The start state counts as independent of the parameters.
+ * States are checkpointed binomially (Griewank's revolve schedule) in
+ * max_snapshots device copies of the state, so a run of N steps costs at
+ * most r N forward steps with C(max_snapshots + r, r) >= N.
+ * Supported: FP64, unsharded handles, maxwellWall and farField patches,
+ * macroFlux no (DUGKS_ERR_UNSUPPORTED otherwise).  On return the handle
+ * holds the state it started from. */
+typedef struct dugks_objective {
+    const double* energy_weight;    /* [n_boundary_faces] or NULL */
+    const double* momentum_weight;  /* [n_boundary_faces * 3] or NULL */
+    int32_t n_steps;                /* >= 1 */
+    int32_t window_start;           /* 0 <= window_start < n_steps */
+    double dt;                      /* fixed time step, > 0 */
+    int32_t max_snapshots;          /* device state copies for the checkpoints, >= 1 */
+    int32_t reserved[3];
+} dugks_objective;
+
+typedef struct dugks_adjoint_stats {
+    int64_t forward_steps;   /* forward steps run, recomputations included */
+    int64_t reverse_steps;   /* = n_steps */
+    int32_t snapshots;       /* state copies allocated */
+    int32_t reserved;
+    double ms_total;         /* CUDA-event milliseconds of the whole run */
+    double ms_forward;       /* of which the forward steps */
+    double device_bytes;     /* device memory the run allocated */
+} dugks_adjoint_stats;
+
+/* J, dJ_dT_b [n_boundary_faces], dJ_dU_b [n_boundary_faces * 3] and
+ * dJ_dmu_ref are host outputs (any may be NULL); stats may be NULL. */
+int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, double* dJ_dT_b, double* dJ_dU_b,
+                      double* dJ_dmu_ref, dugks_adjoint_stats* stats);
+
 /* Number of discrete velocities (nDV^D). */
 int32_t dugks_n_dv(const dugks_handle* h);
 

@@ -1298,3 +1298,17 @@ void dugks_destroy(dugks_handle* h) {
 }
 
 }  // extern "C"
+
+namespace dugks {
+
+// Rebuilds the cell records and Maxwellian tables from the cell macros in
+// ds.cm, as dugks_set_step_record does after restoring them; the next step
+// sets the relax factors for its dt.
+int rebuild_cell_records(dugks_handle* h) {
+    CUDA_TRY(h, launch_cell_records(make_args(h, 0.0, 0.0), h->stream));
+    h->launches += 1;
+    h->cellrec_dt = 0;
+    return DUGKS_OK;
+}
+
+}  // namespace dugks

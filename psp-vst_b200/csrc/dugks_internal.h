@@ -220,4 +220,6 @@ namespace dugks {
 void compute_weights_and_ls(dugks_handle* h, int weighting);
 void build_tiling(dugks_handle* h, int tile_cells);
 int set_error(dugks_handle* h, int code, const std::string& msg);
+// ABI helper (dugks_abi.cpp): cell records and tables from ds.cm
+int rebuild_cell_records(dugks_handle* h);
 }  // namespace dugks

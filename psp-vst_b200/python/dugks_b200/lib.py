@@ -106,6 +106,19 @@ def dv_rows(n_rows: int, rank: int, world: int) -> tuple[int, int]:
     return n_rows * rank // world, n_rows * (rank + 1) // world
 
 
+class Objective(C.Structure):
+    """dugks_objective: time-averaged boundary energy and momentum flux."""
+    _fields_ = [("energy_weight", _dp), ("momentum_weight", _dp), ("n_steps", C.c_int32),
+                ("window_start", C.c_int32), ("dt", C.c_double), ("max_snapshots", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
+
+
+class AdjointStats(C.Structure):
+    _fields_ = [("forward_steps", C.c_int64), ("reverse_steps", C.c_int64), ("snapshots", C.c_int32),
+                ("reserved", C.c_int32), ("ms_total", C.c_double), ("ms_forward", C.c_double),
+                ("device_bytes", C.c_double)]
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("ls_weighting", C.c_int32), ("device", C.c_int32),
                 ("tile_cells", C.c_int32), ("dv_chunks", C.c_int32), ("macro_flux", C.c_int32),
@@ -133,6 +146,7 @@ SIGNATURES = {
     "dugks_step_record_size": (C.c_int64, [C.c_void_p]),
     "dugks_get_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
+    "dugks_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, _dp, _dp, _dp, C.POINTER(AdjointStats)]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
     "dugks_batch_step": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -384,6 +398,28 @@ class Solver:
         rec = np.zeros(self.lib.dugks_step_record_size(self.h))
         self._check(self.lib.dugks_get_step_record(self.h, ptr(rec)))
         return rec
+
+    def adjoint(self, n_steps: int, dt: float, energy_weight=None, momentum_weight=None, window_start: int = 0,
+                max_snapshots: int = 64) -> dict:
+        """dugks_adjoint_run: the objective J (boundary energy and momentum
+        flux averaged over steps window_start .. n_steps-1 of a fixed-dt run
+        from the current state) and its gradient with respect to the T and U
+        patch values of every boundary face and muRef.  The solver's state is
+        left where it started.  Returns J, dT_b [nb], dU_b [nb, 3], dmu and
+        the run's statistics."""
+        nb = self.case.flat["n_boundary"]
+        ew = None if energy_weight is None else np.ascontiguousarray(np.reshape(energy_weight, nb), dtype=np.float64)
+        mw = None if momentum_weight is None else np.ascontiguousarray(np.reshape(momentum_weight, 3 * nb),
+                                                                         dtype=np.float64)
+        obj = Objective(ptr(ew), ptr(mw), int(n_steps), int(window_start), float(dt), int(max_snapshots))
+        J, dmu = C.c_double(), C.c_double()
+        dT, dU = np.zeros(nb), np.zeros((nb, 3))
+        stats = AdjointStats()
+        self._check(self.lib.dugks_adjoint_run(self.h, C.byref(obj), C.byref(J), ptr(dT), ptr(dU), C.byref(dmu),
+                                               C.byref(stats)))
+        return {"J": J.value, "dT_b": dT, "dU_b": dU, "dmu": dmu.value,
+                "stats": {k: getattr(stats, k) for k in ("forward_steps", "reverse_steps", "snapshots", "ms_total",
+                                                         "ms_forward", "device_bytes")}}
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -78,3 +78,9 @@ def test_geometry_rejects_bad_face():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(FileNotFoundError):
         dl.load(str(tmp_path / "nope.so"))
+
+
+def test_adjoint_rejects_null_arguments_on_host():
+    lib = dl.load()
+    obj = dl.Objective(None, None, 4, 0, 1e-6, 4)
+    assert lib.dugks_adjoint_run(None, C.byref(obj), None, None, None, None, None) == 1

@@ -2,27 +2,19 @@
 reference the GPU adjoint is checked against: its value part reproduces
 the oracle's trajectory and objective, and its derivative matches central
 finite differences of the oracle itself."""
-import copy
-
 import numpy as np
 import pytest
 
+import adjoint_cases as ac
 import oracle_bind as ob
 from dugks_b200 import case as cs
 
 N_STEPS = 6
 
 
-def _objective_weights(c):
-    """Energy flux through every wall face, x-momentum flux through the
-    first patch (the lid of the cavity)."""
-    fl = c.flat
-    nb = fl["n_boundary"]
-    first = np.zeros(nb, bool)
-    first[fl["patch_start"][0]:fl["patch_start"][1]] = True
-    fw = np.zeros((nb, 3))
-    fw[first, 0] = 1.0
-    return np.ones(nb), fw, first
+_objective_weights = ac.objective_weights
+_perturbed = ac.perturbed
+_cases = ac.cases
 
 
 def _oracle_J(c, hw, fw, steps=N_STEPS):
@@ -34,28 +26,6 @@ def _oracle_J(c, hw, fw, steps=N_STEPS):
         _, _, gb, hb = o.face_values()
         J += ob.boundary_flux_objective(c, xi, w, gb, hb, hw, fw)
     return J / steps, o
-
-
-def _perturbed(c, eps, dT_b=None, dU_b=None, d_mu=0.0):
-    cc = copy.copy(c)
-    cc.flat = dict(c.flat)
-    cc.gas = dict(c.gas)
-    if dT_b is not None:
-        cc.flat["T_b"] = c.flat["T_b"] + eps * dT_b
-    if dU_b is not None:
-        cc.flat["U_b"] = c.flat["U_b"] + eps * np.reshape(dU_b, (-1, 3))
-    cc.gas["muRef"] = c.gas["muRef"] + eps * d_mu
-    return cc
-
-
-def _cases():
-    ff = {"inlet": {"kind": "farField", "T": 300.0}, "outlet": {"kind": "farField", "T": 273.0}}
-    ch = cs.channel_case(8, 4, 8, sides=ff, U0=(40.0, 0.0, 0.0), flatten=False)
-    rho = float(ch.rho0[0])
-    for p in ch.patches:
-        if p.kind == "farField":
-            p.rho = rho
-    return {"cavity": cs.cavity_case(8, 8, kn=0.1), "farfield": ch.flatten()}
 
 
 @pytest.mark.parametrize("which", ["cavity", "farfield"])
