@@ -42,7 +42,7 @@ def parse():
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["ball", "cavity", "cube", "batch"], default="ball",
+    p.add_argument("--workload", choices=["ball", "cavity", "cube", "batch", "adjoint"], default="ball",
                    help="batch: 64 seeded cavities of uneven size through one CUDA graph (FP32c), "
                         "against the same cases stepped one at a time")
     p.add_argument("--precision", choices=["fp64", "fp32c"], default=None,
@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
+    p.add_argument("--fd-dirs", type=int, default=0,
+                   help="--workload adjoint: central-difference checks on this many random directions")
+    p.add_argument("--adjoint-n", type=int, default=0, help="--workload adjoint: cavity side (default 128)")
     p.add_argument("--dv-shard", action="store_true",
                    help="N>1: shard the DV rows of one workload over the ranks (NCCL) instead of replicas")
     a = p.parse_args()
@@ -287,6 +290,118 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_case(n: int = 128, seed: int = 20261203):
+    """The adjoint workload: n x n lid-driven cavity, 32^2 GH DVs, Kn 0.1,
+    lid 50 m/s, every wall face at its own temperature 273 K + N(0, 5 K)
+    (seeded); returns the case and the objective's weights (wall heat flux
+    on every wall face, x-momentum flux on the lid) and lid mask."""
+    import numpy as np
+    from dugks_b200 import case as cs
+    c = cs.cavity_case(n, 32, kn=0.1)
+    fl = dict(c.flat)
+    nb = fl["n_boundary"]
+    rng = np.random.default_rng(seed)
+    fl["T_b"] = 273.0 + rng.normal(0.0, 5.0, nb)
+    c.flat = fl
+    lid = np.zeros(nb, bool)
+    lid[fl["patch_start"][0]:fl["patch_start"][1]] = True
+    fw = np.zeros((nb, 3))
+    fw[lid, 0] = 1.0
+    return c, np.ones(nb), fw, lid
+
+
+def run_adjoint(args):
+    """--workload adjoint on one GPU: forward + reverse steps of the FP64
+    adjoint (binomial checkpointing, <= 64 device snapshots), objective
+    averaged over the last quarter of the steps; optionally central
+    differences (h = 1e-6 relative) of the objective along random
+    directions in (512 wall temperatures, lid speed, Kn)."""
+    import copy
+
+    import numpy as np
+    import torch
+    from dugks_b200 import lib as dl
+    torch.cuda.set_device(0)
+    n_side = args.adjoint_n or 128
+    case, hw, fw, lid = adjoint_case(n_side)
+    N = max(4, args.steps)
+    window = N - N // 4
+    snaps = 64
+    solver = dl.Solver(case)
+    nc, nv = case.n_cells, solver.n_dv
+    W = max(3, args.warmup)
+    solver.adjoint(W, case.dt, hw, fw, window_start=W - 1, max_snapshots=2)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_uuid(0))
+    sampler.start()
+    time.sleep(0.4)
+    l0 = solver.kernel_launches()
+    r = solver.adjoint(N, case.dt, hw, fw, window_start=window, max_snapshots=snaps)
+    launches = solver.kernel_launches() - l0
+    clocks = sampler.stop()
+    st = r["stats"]
+    # the plain forward rate of the same solver, for the cost ratio
+    fwd = solver.step_timed(20, case.dt)
+    fwd_ms = float(fwd[4]) / 20
+    rev_ms = (st["ms_total"] - st["ms_forward"]) / N
+    ms_per_step = st["ms_total"] / N
+    nb = case.flat["n_boundary"]
+    wall_T = case.flat["T_b"]
+    mu = case.gas["muRef"]
+    grad = {"dJ_dT_wall_l2": float(np.linalg.norm(r["dT_b"])),
+            "dJ_dU_lid": float(np.sum(r["dU_b"][lid, 0])),
+            "dJ_dKn_relative": float(r["dmu"] * mu)}
+    fd = None
+    if args.fd_dirs > 0:
+        rng = np.random.default_rng(20261204)
+        h = 1e-6
+        errs = []
+        for _ in range(args.fd_dirs):
+            dT = rng.normal(size=nb) * wall_T
+            dU = rng.normal() * 50.0
+            dmu = rng.normal() * mu
+            dUb = np.zeros((nb, 3))
+            dUb[lid, 0] = dU
+            ad = float(r["dT_b"] @ dT + np.sum(r["dU_b"] * dUb) + r["dmu"] * dmu)
+            J = []
+            for sgn in (1.0, -1.0):
+                cc = copy.copy(case)
+                cc.flat = dict(case.flat)
+                cc.gas = dict(case.gas)
+                cc.flat["T_b"] = wall_T + sgn * h * dT
+                cc.flat["U_b"] = case.flat["U_b"] + sgn * h * dUb
+                cc.gas["muRef"] = mu + sgn * h * dmu
+                J.append(dl.Solver(cc).objective(N, case.dt, hw, fw, window_start=window)[0])
+            fdv = (J[0] - J[1]) / (2 * h)
+            errs.append(abs(fdv - ad) / abs(ad))
+        fd = {"directions": args.fd_dirs, "h_relative": h, "max_rel_err": max(errs), "rel_errs": errs}
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": METRIC, "value": nc * nv * N / (st["ms_total"] / 1e3),
+        "unit": "cell·DV forward+reverse steps/s", "n_gpus": 1, "steps": N, "warmup": W,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"adjoint: {n_side}x{n_side} lid-driven cavity, 32^2 GH DVs, Kn 0.1, lid 50 m/s, "
+                               f"{nb} wall faces at 273 K + N(0, 5 K), objective = wall heat flux + lid shear "
+                               f"averaged over the last {N - window} of {N} steps",
+                   "cells": nc, "dvs": nv, "snapshots": st["snapshots"], "precision": "fp64",
+                   "l2": "state %.2f GB, the record and adjoint arrays %.2f GB more"
+                         % (16 * nc * nv / 1e9, st["device_bytes"] / 1e9)},
+        "J": r["J"], "gradient": grad,
+        "adjoint": {"forward_steps_incl_recompute": st["forward_steps"], "ms_forward_total": st["ms_forward"],
+                    "reverse_ms_per_step": rev_ms, "forward_ms_per_step": fwd_ms,
+                    "adjoint_step_over_forward_step": ms_per_step / fwd_ms,
+                    "device_gb": st["device_bytes"] / 1e9},
+        "fd_check": fd,
+        "gpu_launches": launches,
+        "step_roofline": {"bytes_per_update": 48, "achieved": 48 * nc * nv / (ms_per_step / 1e3) / 1e9,
+                          "frac": 48 * nc * nv / (ms_per_step / 1e3) / 1e9 / peak, "peak": peak,
+                          "peak_kind": peak_kind},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -311,6 +426,11 @@ def main():
         if int(os.environ.get("WORLD_SIZE", "1")) > 1:
             raise SystemExit("--workload batch runs on one GPU")
         run_batch(args)
+        return
+    if args.workload == "adjoint":
+        if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            raise SystemExit("--workload adjoint runs on one GPU")
+        run_adjoint(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

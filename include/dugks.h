@@ -388,6 +388,12 @@ typedef struct dugks_adjoint_stats {
 int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, double* dJ_dT_b, double* dJ_dU_b,
                       double* dJ_dmu_ref, dugks_adjoint_stats* stats);
 
+/* The objective alone: a forward run of obj->n_steps steps (the handle
+ * advances by n_steps) that evaluates J as dugks_adjoint_run defines it;
+ * max_snapshots is not used.  For finite-difference checks and line
+ * searches. */
+int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J, dugks_adjoint_stats* stats);
+
 /* Number of discrete velocities (nDV^D). */
 int32_t dugks_n_dv(const dugks_handle* h);
 

@@ -155,24 +155,24 @@ struct HandleOps {
 
 }  // namespace
 
-extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, double* dJ_dT_b,
-                                 double* dJ_dU_b, double* dJ_dmu_ref, dugks_adjoint_stats* stats) {
-    if (!h) return DUGKS_ERR_ARG;
-    if (!obj) return set_error(h, DUGKS_ERR_ARG, "dugks_adjoint_run: null objective");
-    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_adjoint_run before dugks_set_macros");
+namespace {
+
+// checks, mesh tables and the record buffers shared by both entry points;
+// with_adjoint also allocates the adjoint arrays
+int prepare(dugks_handle* h, const dugks_objective* obj, const char* who, Arena& ar, adj::View& v, int& sms,
+            bool with_adjoint, double** lam) {
+    if (!obj) return set_error(h, DUGKS_ERR_ARG, std::string(who) + ": null objective");
+    if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, std::string(who) + " before dugks_set_macros");
     if (obj->n_steps < 1 || obj->window_start < 0 || obj->window_start >= obj->n_steps || !(obj->dt > 0) ||
         obj->max_snapshots < 1)
-        return set_error(h, DUGKS_ERR_ARG, "dugks_adjoint_run: need n_steps >= 1, 0 <= window_start < n_steps, "
-                                           "dt > 0, max_snapshots >= 1");
+        return set_error(h, DUGKS_ERR_ARG, std::string(who) + ": need n_steps >= 1, 0 <= window_start < n_steps, "
+                                                              "dt > 0, max_snapshots >= 1");
     if (h->precision != DUGKS_FP64 || h->shard_world > 1 || h->shard_nccl || h->dm.macro_flux)
-        return set_error(h, DUGKS_ERR_UNSUPPORTED,
-                         "dugks_adjoint_run: FP64, unsharded handles with macroFlux no only");
+        return set_error(h, DUGKS_ERR_UNSUPPORTED, std::string(who) + ": FP64, unsharded handles with macroFlux no only");
     for (int b = 0; b < h->nBF; ++b)
         if (h->bface_ptype[b] != DUGKS_PATCH_MAXWELL_WALL && h->bface_ptype[b] != DUGKS_PATCH_FAR_FIELD)
-            return set_error(h, DUGKS_ERR_UNSUPPORTED,
-                             "dugks_adjoint_run: maxwellWall and farField patches only");
+            return set_error(h, DUGKS_ERR_UNSUPPORTED, std::string(who) + ": maxwellWall and farField patches only");
     ADJ_TRY(h, cudaSetDevice(h->device));
-    int sms = 0;
     ADJ_TRY(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
 
     const int nC = h->nC, nIF = h->nIF, nBF = h->nBF, nF = nIF + nBF, nv = h->nv;
@@ -193,10 +193,15 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     std::vector<double> ha(nBF, 0.0), fw(3 * static_cast<size_t>(nBF), 0.0);
     if (obj->energy_weight) std::copy(obj->energy_weight, obj->energy_weight + nBF, ha.begin());
     if (obj->momentum_weight) std::copy(obj->momentum_weight, obj->momentum_weight + 3 * nBF, fw.begin());
+    for (int b = 0; b < nBF; ++b) {
+        bool ok = std::isfinite(ha[b]);
+        for (int k = 0; k < 3; ++k) ok = ok && std::isfinite(fw[3 * b + k]);
+        if (!ok) return set_error(h, DUGKS_ERR_ARG, std::string(who) + ": non-finite objective weight");
+    }
     std::vector<double> Sf(h->Sf.begin(), h->Sf.begin() + 3 * static_cast<size_t>(nF));
     std::vector<double> Cf(h->Cf.begin(), h->Cf.begin() + 3 * static_cast<size_t>(nF));
 
-    adj::View v{};
+    v = adj::View{};
     v.nC = nC;
     v.nIF = nIF;
     v.nBF = nBF;
@@ -216,7 +221,6 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     v.xi = h->dm.xi;
     v.w = h->dm.w;
 
-    Arena ar;
     int32_t *d_own, *d_nei, *d_cfo, *d_cfe, *d_tho, *d_the, *d_bt, *d_bl;
     double *d_S, *d_Cf, *d_C, *d_iV, *d_lsP, *d_lsN, *d_bU, *d_bT, *d_brho, *d_ha, *d_fw;
     int st;
@@ -247,22 +251,44 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     v.brho = d_brho;
     v.ha = d_ha;
     v.fw = d_fw;
-    double* lam[4];
     if ((st = ar.get(h, &v.gbp, nvc)) || (st = ar.get(h, &v.hbp, nvc)) || (st = ar.get(h, &v.Gg, 3 * nvc)) ||
         (st = ar.get(h, &v.Gh, 3 * nvc)) || (st = ar.get(h, &v.fg, nvf)) || (st = ar.get(h, &v.fh, nvf)) ||
-        (st = ar.get(h, &v.pf, static_cast<size_t>(v.nchF) * nF * adj::kP)) ||
-        (st = ar.get(h, &v.pc, static_cast<size_t>(v.nchC) * nC * adj::kP)) || (st = ar.get(h, &v.rhow, nBF)) ||
+        (st = ar.get(h, &v.pf, static_cast<size_t>(v.nchF) * nF * adj::kP)) || (st = ar.get(h, &v.rhow, nBF)) ||
         (st = ar.get(h, &v.inby, nBF)) || (st = ar.get(h, &v.fmac, static_cast<size_t>(nF) * adj::kMac)) ||
+        (st = ar.zeros(h, &v.Jb, nBF)))
+        return st;
+    if (!with_adjoint) return DUGKS_OK;
+    if ((st = ar.get(h, &v.pc, static_cast<size_t>(v.nchC) * nC * adj::kP)) ||
         (st = ar.get(h, &v.cmac, static_cast<size_t>(nC) * adj::kMac)) || (st = ar.get(h, &v.ag, nvf)) ||
         (st = ar.get(h, &v.ah, nvf)) || (st = ar.get(h, &v.aGg, 3 * nvc)) || (st = ar.get(h, &v.aGh, 3 * nvc)) ||
         (st = ar.get(h, &v.fco, static_cast<size_t>(nF) * adj::kCo)) ||
         (st = ar.get(h, &v.cco, static_cast<size_t>(nC) * adj::kCo)) || (st = ar.get(h, &v.aout, nBF)) ||
         (st = ar.get(h, &v.aUown, 3 * static_cast<size_t>(nBF))) || (st = ar.zeros(h, &v.gTb, nBF)) ||
         (st = ar.zeros(h, &v.gUb, 3 * static_cast<size_t>(nBF))) || (st = ar.zeros(h, &v.aI, nBF)) ||
-        (st = ar.zeros(h, &v.amuF, nF)) || (st = ar.zeros(h, &v.amuC, nC)) || (st = ar.zeros(h, &v.Jb, nBF)) ||
-        (st = ar.zeros(h, &lam[0], nvc)) || (st = ar.zeros(h, &lam[1], nvc)) || (st = ar.get(h, &lam[2], nvc)) ||
-        (st = ar.get(h, &lam[3], nvc)))
+        (st = ar.zeros(h, &v.amuF, nF)) || (st = ar.zeros(h, &v.amuC, nC)) || (st = ar.zeros(h, &lam[0], nvc)) ||
+        (st = ar.zeros(h, &lam[1], nvc)) || (st = ar.get(h, &lam[2], nvc)) || (st = ar.get(h, &lam[3], nvc)))
         return st;
+    return DUGKS_OK;
+}
+
+double host_sum(const std::vector<double>& a) {
+    double s = 0;
+    for (double x : a) s += x;
+    return s;
+}
+
+}  // namespace
+
+extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, double* dJ_dT_b,
+                                 double* dJ_dU_b, double* dJ_dmu_ref, dugks_adjoint_stats* stats) {
+    if (!h) return DUGKS_ERR_ARG;
+    Arena ar;
+    adj::View v;
+    double* lam[4] = {};
+    int sms = 0, st;
+    if ((st = prepare(h, obj, "dugks_adjoint_run", ar, v, sms, true, lam))) return st;
+    const int nC = h->nC, nBF = h->nBF, nF = v.nF;
+    const size_t nvc = static_cast<size_t>(h->nv) * nC;
 
     HandleOps ops;
     ops.h = h;
@@ -309,10 +335,7 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     cudaEventDestroy(t1);
     h->steps_done = steps_before;
 
-    double Jsum = 0, mu = 0;
-    for (int b = 0; b < nBF; ++b) Jsum += Jb[b];
-    for (int f = 0; f < nF; ++f) mu += mF[f];
-    for (int c = 0; c < nC; ++c) mu += mC[c];
+    const double Jsum = host_sum(Jb), mu = host_sum(mF) + host_sum(mC);
     if (J) *J = Jsum;
     if (dJ_dT_b) std::copy(gT.begin(), gT.end(), dJ_dT_b);
     if (dJ_dU_b) std::copy(gU.begin(), gU.end(), dJ_dU_b);
@@ -328,5 +351,55 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     }
     if (!std::isfinite(Jsum) || !std::isfinite(mu))
         return set_error(h, DUGKS_ERR_NAN, "dugks_adjoint_run: non-finite objective or gradient");
+    return DUGKS_OK;
+}
+
+extern "C" int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J,
+                                   dugks_adjoint_stats* stats) {
+    if (!h) return DUGKS_ERR_ARG;
+    Arena ar;
+    adj::View v;
+    int sms = 0, st;
+    if ((st = prepare(h, obj, "dugks_objective_run", ar, v, sms, false, nullptr))) return st;
+    GpuEx ex{h, sms};
+    const int nBF = h->nBF;
+    const double dt = obj->dt;
+    cudaEvent_t t0, t1;
+    ADJ_TRY(h, cudaEventCreate(&t0));
+    ADJ_TRY(h, cudaEventCreate(&t1));
+    ADJ_TRY(h, cudaEventRecord(t0, h->stream));
+    if ((st = ex.run(nBF, adj::FInBy{v}))) return st;
+    if (obj->window_start > 0) {
+        std::vector<double> dts(obj->window_start, dt);
+        if ((st = dugks_step(h, obj->window_start, dts.data()))) return st;
+    }
+    for (int n = obj->window_start; n < obj->n_steps; ++n) {
+        adj::View w = v;
+        const int c = h->ds.cur;
+        w.g = static_cast<const double*>(h->ds.g[c]);
+        w.h = static_cast<const double*>(h->ds.h[c]);
+        w.cm = h->ds.cm;
+        w.wn = 1.0 / (obj->n_steps - obj->window_start);
+        if ((st = adj::record_step(ex, w))) return st;
+        if ((st = ex.run(nBF, adj::FObjective{w}))) return st;
+        if ((st = dugks_step(h, 1, &dt))) return st;
+    }
+    ADJ_TRY(h, cudaEventRecord(t1, h->stream));
+    std::vector<double> Jb(nBF);
+    ADJ_TRY(h, cudaMemcpyAsync(Jb.data(), v.Jb, nBF * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    ADJ_TRY(h, cudaStreamSynchronize(h->stream));
+    float ms_total = 0;
+    cudaEventElapsedTime(&ms_total, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    const double Jsum = host_sum(Jb);
+    if (J) *J = Jsum;
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->forward_steps = obj->n_steps;
+        stats->ms_total = ms_total;
+        stats->device_bytes = ar.bytes;
+    }
+    if (!std::isfinite(Jsum)) return set_error(h, DUGKS_ERR_NAN, "dugks_objective_run: non-finite objective");
     return DUGKS_OK;
 }

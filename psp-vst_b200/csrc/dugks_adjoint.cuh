@@ -557,6 +557,26 @@ struct FUpdate {
     }
 };
 
+// the objective of one step: every boundary face's energy and momentum flux
+// of its relaxed DFs, weighted by wn, added to Jb
+struct FObjective {
+    View v;
+    ADJ_HD void operator()(int64_t bi) const {
+        const int b = static_cast<int>(bi), f = v.nIF + b;
+        const double* S = v.S + 3 * f;
+        const double ea = v.wn * v.ha[b];
+        double s = 0;
+        for (int i = 0; i < v.nv; ++i) {
+            const double* xi = v.xi + 3 * i;
+            double gr, hr, gEq, hEq, r;
+            relaxed_value(v, i, f, gr, hr, gEq, hEq, r);
+            const double wx = v.w[i] * dot3(xi, S);
+            s += wx * (ea * 0.5 * (magsqr3(xi) * gr + hr) + v.wn * dot3(v.fw + 3 * b, xi) * gr);
+        }
+        v.Jb[b] += s;
+    }
+};
+
 // ---------------------------------------------------------------- reverse
 
 // R1: adjoint of the relaxed face values (from the update and the

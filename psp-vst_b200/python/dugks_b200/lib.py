@@ -147,6 +147,7 @@ SIGNATURES = {
     "dugks_get_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, _dp, _dp, _dp, C.POINTER(AdjointStats)]),
+    "dugks_objective_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, C.POINTER(AdjointStats)]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
     "dugks_batch_step": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -420,6 +421,20 @@ class Solver:
         return {"J": J.value, "dT_b": dT, "dU_b": dU, "dmu": dmu.value,
                 "stats": {k: getattr(stats, k) for k in ("forward_steps", "reverse_steps", "snapshots", "ms_total",
                                                          "ms_forward", "device_bytes")}}
+
+    def objective(self, n_steps: int, dt: float, energy_weight=None, momentum_weight=None,
+                  window_start: int = 0) -> tuple[float, dict]:
+        """dugks_objective_run: J of a forward run of n_steps (the solver
+        advances) and the run's statistics."""
+        nb = self.case.flat["n_boundary"]
+        ew = None if energy_weight is None else np.ascontiguousarray(np.reshape(energy_weight, nb), dtype=np.float64)
+        mw = None if momentum_weight is None else np.ascontiguousarray(np.reshape(momentum_weight, 3 * nb),
+                                                                         dtype=np.float64)
+        obj = Objective(ptr(ew), ptr(mw), int(n_steps), int(window_start), float(dt), 1)
+        J = C.c_double()
+        stats = AdjointStats()
+        self._check(self.lib.dugks_objective_run(self.h, C.byref(obj), C.byref(J), C.byref(stats)))
+        return J.value, {"ms_total": stats.ms_total, "device_bytes": stats.device_bytes}
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -82,7 +82,23 @@ def test_adjoint_leaves_the_state_and_repeats_bitwise():
 
 
 def _gpu_J(c, hw, fw, n, window):
-    return dl.Solver(c).adjoint(n, c.dt, hw, fw, window_start=window, max_snapshots=n)["J"]
+    return dl.Solver(c).objective(n, c.dt, hw, fw, window_start=window)[0]
+
+
+def test_objective_run_is_the_adjoint_objective():
+    """dugks_objective_run (forward only) gives the adjoint run's J and
+    advances the solver as dugks_step does."""
+    c = ac.cases()["farfield"]
+    hw, fw, _ = ac.objective_weights(c)
+    s = dl.Solver(c)
+    r = s.adjoint(7, c.dt, hw, fw, window_start=3, max_snapshots=3)
+    J, _ = s.objective(7, c.dt, hw, fw, window_start=3)
+    assert abs(J - r["J"]) <= 1e-12 * abs(J)
+    ref = dl.Solver(c)
+    ref.step(7, c.dt)
+    g1, _ = s.state()
+    g2, _ = ref.state()
+    assert np.array_equal(g1, g2)
 
 
 def test_adjoint_matches_central_differences_with_window():
