@@ -302,6 +302,67 @@ ADJ_HD void add_moments(const double* xi, double wi, double g, double h, double*
     m[13] += a * xi[2] * xi[2];
 }
 
+// The Shakhov equilibrium of one entity (cell or face) over many DVs, with
+// the entity's constants computed once: the same formula as shakhov(),
+// with (2 pi R T)^(D/2) by multiplication and one exp per DV, and its
+// reverse from the same intermediates.
+struct ShkEntity {
+    double U[3], q[3], rho, T, R, invRT, pref, iden, RTh, omp, k3;
+    int D, K;
+    ADJ_HD ShkEntity(const View& v, const double* Uv, double Tv, double rhov, const double* qv, double Th) {
+        D = v.D;
+        K = v.K;
+        for (int k = 0; k < 3; ++k) {
+            U[k] = Uv[k];
+            q[k] = qv[k];
+        }
+        rho = rhov;
+        T = Tv;
+        R = v.R;
+        const double RT = v.R * Tv;
+        invRT = 1.0 / RT;
+        const double s = sqrt(2.0 * kPi * RT);
+        pref = rhov / (D == 3 ? s * s * s : D == 2 ? s * s : s);
+        iden = 1.0 / (5.0 * rhov * RT * RT);
+        RTh = v.R * Th;
+        omp = 1.0 - v.Pr;
+        k3 = K + 3.0 - D;
+    }
+    // per-DV intermediates
+    struct DV {
+        double c[3], cS, P, G0, A, Bh;
+    };
+    ADJ_HD DV at(const double* xi) const {
+        DV d;
+        for (int k = 0; k < 3; ++k) d.c[k] = xi[k] - U[k];
+        d.cS = magsqr3(d.c) * invRT;
+        d.P = dot3(d.c, q) * iden;
+        d.G0 = pref * exp(-0.5 * d.cS);
+        d.A = 1.0 + omp * d.P * (d.cS - D - 2.0);
+        d.Bh = k3 + omp * d.P * ((d.cS - D) * k3 - 2 * K);
+        return d;
+    }
+    ADJ_HD double g(const DV& d) const { return d.A * d.G0; }
+    ADJ_HD double h(const DV& d) const { return d.Bh * d.G0 * RTh; }
+    // adds the adjoints of rho, U, T, q and Th into s[0], s[1..3], s[4],
+    // s[5..7], s[8], given the adjoints ag, ah of g^S and h^S
+    ADJ_HD void rev(const DV& d, double ag, double ah, double* s) const {
+        const double aG0 = ag * d.A + ah * d.Bh * RTh;
+        const double aA = ag * d.G0, aB = ah * d.G0 * RTh;
+        const double aP = omp * (aA * (d.cS - D - 2.0) + aB * ((d.cS - D) * k3 - 2 * K));
+        const double acS = omp * d.P * (aA + aB * k3) - 0.5 * aG0 * d.G0;
+        const double invT = 1.0 / T;
+        s[0] += (aG0 * d.G0 - aP * d.P) / rho;
+        s[4] += (-0.5 * D * aG0 * d.G0 - acS * d.cS - 2.0 * aP * d.P) * invT;
+        const double f1 = 2.0 * acS * invRT, f2 = aP * iden;
+        for (int k = 0; k < 3; ++k) {
+            s[1 + k] -= f1 * d.c[k] + f2 * q[k];
+            s[5 + k] += f2 * d.c[k];
+        }
+        s[8] += ah * d.Bh * d.G0 * R;
+    }
+};
+
 // ---------------------------------------------------------------- forward
 
 // inComingByRho of the wall faces (fvDVM.C:578-624)
@@ -329,10 +390,10 @@ struct FHalf {
         const double* m = v.cm + 9 * static_cast<size_t>(c);
         const double tau = tau_of(v, m[4], m[0]);
         const double r = 1.5 * v.dt / (2.0 * tau + v.dt);
-        double gEq, hEq;
-        shakhov(v, v.xi + 3 * i, m + 1, m[4], m[0], m + 5, m[4], gEq, hEq);
-        v.gbp[idx] = (1.0 - r) * v.g[idx] + r * gEq;
-        v.hbp[idx] = (1.0 - r) * v.h[idx] + r * hEq;
+        const ShkEntity e(v, m + 1, m[4], m[0], m + 5, m[4]);
+        const ShkEntity::DV d = e.at(v.xi + 3 * i);
+        v.gbp[idx] = (1.0 - r) * v.g[idx] + r * e.g(d);
+        v.hbp[idx] = (1.0 - r) * v.h[idx] + r * e.h(d);
     }
 };
 
@@ -588,35 +649,47 @@ struct RRelax {
         const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const bool bnd = f >= v.nIF;
         const int b = f - v.nIF;
-        const int ow = v.own[f], ne = bnd ? -1 : v.nei[f];
+        const int ow = v.own[f], ne = bnd ? ow : v.nei[f];
         const double* m = v.fmac + kMac * static_cast<size_t>(f);
         const double dtVo = v.dt * v.invV[ow], dtVn = bnd ? 0.0 : v.dt * v.invV[ne];
         const double ea = bnd ? v.wn * v.ha[b] : 0.0;
-        const double* cw = bnd ? v.fw + 3 * b : nullptr;
+        double cw[3] = {0, 0, 0};
+        if (bnd)
+            for (int k = 0; k < 3; ++k) cw[k] = v.wn * v.fw[3 * b + k];
+        const double S[3] = {v.S[3 * f], v.S[3 * f + 1], v.S[3 * f + 2]};
+        // h^S of a boundary face is scaled by the internal-face T at its patch-local index
+        const double Th = !bnd ? m[MAC_T] : v.fmac[kMac * static_cast<size_t>(v.blocal[b]) + MAC_T];
+        const ShkEntity e(v, m + MAC_U, m[MAC_T], m[MAC_RHO], m + MAC_Q, Th);
+        const double r = 0.5 * v.dt / (2.0 * m[MAC_TAU] + 0.5 * v.dt);
         double s[12] = {0};
         for (int i = chunk_lo(v.nv, v.nchF, ch); i < chunk_lo(v.nv, v.nchF, ch + 1); ++i) {
             const double* xi = v.xi + 3 * i;
-            const double xs = dot3(xi, v.S + 3 * f);
+            const double xs = dot3(xi, S);
             const size_t id = at(i, v.nF, f);
-            double a_g = -xs * dtVo * v.lg[at(i, v.nC, ow)];
-            double a_h = -xs * dtVo * v.lh[at(i, v.nC, ow)];
-            if (!bnd) {
-                a_g += xs * dtVn * v.lg[at(i, v.nC, ne)];
-                a_h += xs * dtVn * v.lh[at(i, v.nC, ne)];
+            const double lgo = v.lg[at(i, v.nC, ow)], lho = v.lh[at(i, v.nC, ow)];
+            const double lgn = v.lg[at(i, v.nC, ne)], lhn = v.lh[at(i, v.nC, ne)];
+            const double pg = v.fg[id], ph = v.fh[id];
+            double a_g = xs * (dtVn * lgn - dtVo * lgo);
+            double a_h = xs * (dtVn * lhn - dtVo * lho);
+            const bool rel = !bnd || xs > 0;
+            ShkEntity::DV d{};
+            double gEq = 0, hEq = 0;
+            if (rel) {
+                d = e.at(xi);
+                gEq = e.g(d);
+                hEq = e.h(d);
             }
-            double gr, hr, gEq = 0, hEq = 0, r = 0;
-            const bool rel = relaxed_value(v, i, f, gr, hr, gEq, hEq, r);
             if (bnd) {
-                const double wx = v.w[i] * xs;
-                const double cg = v.wn * dot3(cw, xi);
-                s[10] += wx * (ea * 0.5 * (magsqr3(xi) * gr + hr) + cg * gr);
-                a_g += wx * (ea * 0.5 * magsqr3(xi) + cg);
+                const double gr = rel ? (1.0 - r) * pg + r * gEq : pg;
+                const double hr = rel ? (1.0 - r) * ph + r * hEq : ph;
+                const double wx = v.w[i] * xs, x2 = magsqr3(xi), cg = dot3(cw, xi);
+                s[10] += wx * (ea * 0.5 * (x2 * gr + hr) + cg * gr);
+                a_g += wx * (ea * 0.5 * x2 + cg);
                 a_h += wx * ea * 0.5;
             }
             if (rel) {
-                s[0] += (gEq - v.fg[id]) * a_g + (hEq - v.fh[id]) * a_h;
-                const double Th = !bnd ? m[MAC_T] : v.fmac[kMac * static_cast<size_t>(v.blocal[b]) + MAC_T];
-                shakhov_rev(v, xi, m + MAC_U, m[MAC_T], m[MAC_RHO], m + MAC_Q, Th, r * a_g, r * a_h, s + 1);
+                s[0] += (gEq - pg) * a_g + (hEq - ph) * a_h;
+                e.rev(d, r * a_g, r * a_h, s + 1);
                 v.ag[id] = (1.0 - r) * a_g;
                 v.ah[id] = (1.0 - r) * a_h;
             } else {
@@ -785,34 +858,39 @@ struct RHalf {
         const double* m = v.cm + 9 * static_cast<size_t>(c);
         const double tau = tau_of(v, m[4], m[0]);
         const double r = 1.5 * v.dt / (2.0 * tau + v.dt);
+        const ShkEntity e(v, m + 1, m[4], m[0], m + 5, m[4]);
         const size_t n = static_cast<size_t>(v.nv) * v.nC;
+        const int e0 = v.cf_off[c], e1 = v.cf_off[c + 1];
         double s[9] = {0};
         for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
             const size_t cb = at(i, v.nC, 0), id = cb + c;
             double abg = v.og[id], abh = v.oh[id];
-            for (int e = v.cf_off[c]; e < v.cf_off[c + 1]; ++e) {
-                const int f = v.cf_ent[e] >> 1;
+            const double gc[3] = {v.aGg[id], v.aGg[n + id], v.aGg[2 * n + id]};
+            const double hc[3] = {v.aGh[id], v.aGh[n + id], v.aGh[2 * n + id]};
+            for (int en = e0; en < e1; ++en) {
+                const int f = v.cf_ent[en] >> 1;
                 if (f >= v.nIF) break;
-                const int ow = v.own[f], ne = v.nei[f];
-                double sg = 0, sh = 0;
-                for (int k = 0; k < 3; ++k) {
-                    sg += v.lsP[3 * f + k] * v.aGg[k * n + cb + ow] - v.lsN[3 * f + k] * v.aGg[k * n + cb + ne];
-                    sh += v.lsP[3 * f + k] * v.aGh[k * n + cb + ow] - v.lsN[3 * f + k] * v.aGh[k * n + cb + ne];
-                }
-                if (v.cf_ent[e] & 1) {
-                    abg += sg;
-                    abh += sh;
+                const bool is_nei = v.cf_ent[en] & 1;
+                const int o = is_nei ? v.own[f] : v.nei[f];  // the other cell of the face
+                const size_t io = cb + o;
+                const double go[3] = {v.aGg[io], v.aGg[n + io], v.aGg[2 * n + io]};
+                const double ho[3] = {v.aGh[io], v.aGh[n + io], v.aGh[2 * n + io]};
+                const double* P = v.lsP + 3 * f;
+                const double* N = v.lsN + 3 * f;
+                // s_f = lsP . aG_own - lsN . aG_nei; the neighbour adds it, the owner subtracts it
+                if (is_nei) {
+                    abg += dot3(P, go) - dot3(N, gc);
+                    abh += dot3(P, ho) - dot3(N, hc);
                 } else {
-                    abg -= sg;
-                    abh -= sh;
+                    abg -= dot3(P, gc) - dot3(N, go);
+                    abh -= dot3(P, hc) - dot3(N, ho);
                 }
             }
-            double gEq, hEq;
-            const double* xi = v.xi + 3 * i;
-            shakhov(v, xi, m + 1, m[4], m[0], m + 5, m[4], gEq, hEq);
+            const ShkEntity::DV d = e.at(v.xi + 3 * i);
+            const double gEq = e.g(d), hEq = e.h(d);
             s[0] += (gEq - v.g[id]) * abg + (hEq - v.h[id]) * abh;
             double t[9] = {0};
-            shakhov_rev(v, xi, m + 1, m[4], m[0], m + 5, m[4], r * abg, r * abh, t);
+            e.rev(d, r * abg, r * abh, t);
             for (int k = 0; k < 8; ++k) s[1 + k] += t[k];
             s[5] += t[8];  // h^S of a cell is scaled by the cell's own T
             v.og[id] = -1.0 / 3 * v.lg[id] + (1.0 - r) * abg;
