@@ -51,6 +51,10 @@ def parse():
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
+    p.add_argument("--cube-n", type=int, default=64, help="--workload cube: cells per side")
+    p.add_argument("--kn", type=float, default=0.1, help="--workload cube: Knudsen number")
+    p.add_argument("--tune", action="store_true",
+                   help="--workload batch: pick tile size and DV-chunk scale with the batch autotuner first")
     p.add_argument("--fd-dirs", type=int, default=0,
                    help="--workload adjoint: central-difference checks on this many random directions")
     p.add_argument("--adjoint-n", type=int, default=0, help="--workload adjoint: cavity side (default 128)")
@@ -62,7 +66,7 @@ def parse():
     return a
 
 
-def build_case(name, ndv1d=0):
+def build_case(name, ndv1d=0, cube_n=64, kn=0.1):
     from dugks_b200 import case as cs
     if name == "ball":
         c = cs.ball_case(24, 32, 1.12, ndv1d or 16, kn=0.1, mach=0.5)
@@ -70,9 +74,9 @@ def build_case(name, ndv1d=0):
                            "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall",
                "cells": c.n_cells, "n_dv": c.n_dv}
     elif name == "cube":
-        c = cs.cube_case(64, ndv1d or 20, kn=0.1)
-        cfg = {"workload": "cube: 64^3 lid-driven cube, 20^3 GH DVs, Kn 0.1, lid 50 m/s", "cells": c.n_cells,
-               "n_dv": c.n_dv}
+        c = cs.cube_case(cube_n, ndv1d or 20, kn=kn)
+        cfg = {"workload": f"cube: {cube_n}^3 lid-driven cube, {ndv1d or 20}^3 GH DVs, Kn {kn}, lid 50 m/s",
+               "cells": c.n_cells, "n_dv": c.n_dv}
     else:
         c = cs.cavity_case(61, ndv1d or 28)
         cfg = {"workload": "cavity: 61x61 lid-driven cavity, 28^2 GH DVs, Kn 0.075, lid 50 m/s", "cells": c.n_cells,
@@ -236,7 +240,15 @@ def run_batch(args):
     seed = 20261203
     cases = batch_cases(seed)
     prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
-    solvers = [dl.Solver(c, precision=prec) for c in cases]
+    tuning = None
+    if args.tune:
+        t0 = time.perf_counter()
+        best, table = dl.tune_batch(cases, [c.dt for c in cases], precision=prec)
+        tuning = {"chosen": {"tile_cells": best["tile_cells"], "chunk_scale": best["chunk_scale"]},
+                  "candidates": table, "tuning_seconds": time.perf_counter() - t0}
+        solvers = [dl.Solver(c, precision=prec, **kw) for c, kw in zip(cases, best["solver_kwargs"])]
+    else:
+        solvers = [dl.Solver(c, precision=prec) for c in cases]
     pairs = sum(c.n_cells * c.n_dv for c in cases)
     K = max(2, args.steps - args.steps % 2)
     W = max(4, args.warmup + args.warmup % 2)
@@ -281,6 +293,7 @@ def run_batch(args):
                 "d2h_bytes_per_step": sum(72 * c.n_cells for c in cases) // 2},
         "gpu_launches": launches,
         "graph_kernels_per_two_steps": batch.graph_kernels(),
+        "autotune": tuning,
         "step_roofline": {"bytes_per_update": 6 * rs, "achieved": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9,
                           "frac": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9 / peak, "peak": peak,
                           "peak_kind": peak_kind},
@@ -444,7 +457,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     from dugks_b200 import lib as dl
-    case, cfg = build_case(args.workload, args.ndv1d)
+    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn)
     prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
     shard = None
     if world > 1 and args.dv_shard:

@@ -394,6 +394,11 @@ int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, do
  * searches. */
 int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J, dugks_adjoint_stats* stats);
 
+/* The launch layout dugks_create chose: cells per tile (after shrinking
+ * to fit), number of tiles and DV chunks per tile.  An autotuner reads it
+ * to scale dugks_options.tile_cells / dv_chunks from the automatic choice. */
+int dugks_layout(const dugks_handle* h, int32_t* tile_cells, int32_t* n_tiles, int32_t* dv_chunks);
+
 /* Number of discrete velocities (nDV^D). */
 int32_t dugks_n_dv(const dugks_handle* h);
 

@@ -1277,6 +1277,14 @@ int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double d
 
 int32_t dugks_n_dv(const dugks_handle* h) { return h ? h->nv : 0; }
 
+int dugks_layout(const dugks_handle* h, int32_t* tile_cells, int32_t* n_tiles, int32_t* dv_chunks) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (tile_cells) *tile_cells = h->tiling.tile_cells;
+    if (n_tiles) *n_tiles = h->tiling.n_tiles;
+    if (dv_chunks) *dv_chunks = h->chunks;
+    return DUGKS_OK;
+}
+
 int dugks_last_step_ms(dugks_handle* h, double* ms) {
     if (!h || !ms) return DUGKS_ERR_ARG;
     *ms = h->last_step_ms;

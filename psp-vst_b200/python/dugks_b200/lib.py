@@ -148,6 +148,7 @@ SIGNATURES = {
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, _dp, _dp, _dp, C.POINTER(AdjointStats)]),
     "dugks_objective_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, C.POINTER(AdjointStats)]),
+    "dugks_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
     "dugks_batch_step": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -336,6 +337,12 @@ class Solver:
         self._check(self.lib.dugks_step_timed(self.h, n, ptr(dts), ptr(out)))
         return out
 
+    def layout(self) -> dict:
+        """dugks_layout: cells per tile, tiles and DV chunks the handle uses."""
+        t, n, c = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.lib.dugks_layout(self.h, C.byref(t), C.byref(n), C.byref(c)))
+        return {"tile_cells": t.value, "n_tiles": n.value, "dv_chunks": c.value}
+
     def kernel_launches(self) -> int:
         return int(self.lib.dugks_kernel_launches(self.h))
 
@@ -488,3 +495,42 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def tune_batch(cases, dt, precision: int = FP32C, tiles=(0, 96, 64), chunk_scales=(0.25, 0.5, 1.0, 2.0),
+               steps: int = 4, warmup: int = 2, device: int = 0):
+    """Autotuner of the batched launch.  Every candidate is a cell count per
+    tile (0: the automatic 128, shrunk to fit) and a factor on each case's
+    automatic DV-chunk count; it is measured as what it will run as -- the
+    whole batch of cases in one graph, CUDA-event time of `steps` steps after
+    `warmup` -- and the fastest wins.  Returns (best, table): best holds the
+    tile and scale and the per-case Solver keyword arguments, table every
+    candidate's milliseconds per step."""
+    dts = np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(cases),))
+    table = []
+    best = None
+    for tile in tiles:
+        base = [Solver(c, precision=precision, device=device, tile_cells=tile) for c in cases]
+        auto = [s.layout()["dv_chunks"] for s in base]
+        for scale in chunk_scales:
+            if scale == 1.0:
+                solvers = base
+            else:
+                solvers = [Solver(c, precision=precision, device=device, tile_cells=tile,
+                                  dv_chunks=max(1, int(round(scale * a)))) for c, a in zip(cases, auto)]
+            kwargs = [{"tile_cells": tile, "dv_chunks": s.layout()["dv_chunks"]} for s in solvers]
+            b = Batch(solvers, dts)
+            b.step(warmup)
+            b.step(steps)
+            ms = b.last_ms() / steps
+            b.close()
+            table.append({"tile_cells": tile, "chunk_scale": scale, "ms_per_step": ms})
+            if best is None or ms < best["ms_per_step"]:
+                best = {"tile_cells": tile, "chunk_scale": scale, "ms_per_step": ms, "solver_kwargs": kwargs}
+            if solvers is not base:
+                for s in solvers:
+                    s.close()
+        for s in base:
+            s.close()
+    return best, table
+

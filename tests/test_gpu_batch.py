@@ -51,3 +51,28 @@ def test_batch_rejects_bad_input():
     sh = dl.Solver(c, shard=dl.shard(0, 2))
     with pytest.raises(dl.DugksError):
         dl.Batch([sh], [c.dt])
+
+
+def test_autotuner_picks_a_measured_candidate_and_keeps_the_result():
+    """tune_batch measures every (tile, chunk scale) candidate on the whole
+    batch and returns the fastest; solvers built with its choice give the
+    oracle-parity result of the default layout (FP64, to 1e-12)."""
+    cases = _cases()
+    dts = [c.dt for c in cases]
+    best, table = dl.tune_batch(cases, dts, precision=dl.FP64, tiles=(0, 16), chunk_scales=(0.5, 1.0),
+                                steps=2, warmup=2)
+    assert len(table) == 4
+    assert best["ms_per_step"] == min(t["ms_per_step"] for t in table)
+    tuned = [dl.Solver(c, precision=dl.FP64, **kw) for c, kw in zip(cases, best["solver_kwargs"])]
+    for s, kw in zip(tuned, best["solver_kwargs"]):
+        assert s.layout()["dv_chunks"] == kw["dv_chunks"]
+    default = [dl.Solver(c, precision=dl.FP64) for c in cases]
+    b = dl.Batch(tuned, dts)
+    b.step(4)
+    b.close()
+    for s, c in zip(default, cases):
+        s.step(4, c.dt)
+    for a, d in zip(tuned, default):
+        ma, md = a.macros(), d.macros()
+        for k in ("rho", "T"):
+            assert np.linalg.norm(ma[k] - md[k]) <= 1e-12 * np.linalg.norm(md[k]), k
