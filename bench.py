@@ -49,6 +49,7 @@ def parse():
                    help="default fp64; fp32c for --workload batch")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32c", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the short adjoint measurement of the default run")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
     p.add_argument("--cube-n", type=int, default=64, help="--workload cube: cells per side")
@@ -324,6 +325,10 @@ def adjoint_case(n: int = 128, seed: int = 20261203):
 
 
 def run_adjoint(args):
+    print(json.dumps(adjoint_line(args)), flush=True)
+
+
+def adjoint_line(args):
     """--workload adjoint on one GPU: forward + reverse steps of the FP64
     adjoint (binomial checkpointing, <= 64 device snapshots), objective
     averaged over the last quarter of the steps; optionally central
@@ -388,6 +393,7 @@ def run_adjoint(args):
             fdv = (J[0] - J[1]) / (2 * h)
             errs.append(abs(fdv - ad) / abs(ad))
         fd = {"directions": args.fd_dirs, "h_relative": h, "max_rel_err": max(errs), "rel_errs": errs}
+    solver.close()
     peak, peak_kind = measured_peaks()
     line = {
         "metric": METRIC, "value": nc * nv * N / (st["ms_total"] / 1e3),
@@ -412,7 +418,7 @@ def run_adjoint(args):
                           "peak_kind": peak_kind},
         "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_reference(args):
@@ -558,6 +564,14 @@ def main():
         del s32
     else:
         del solver
+    if rank == 0 and world == 1 and not args.no_adjoint and args.workload == "ball":
+        # the adjoint configuration (128x128 cavity, 32^2 DVs, FP64) over a
+        # short horizon: forward + reverse steps with <= 64 snapshots
+        import types
+        sub = adjoint_line(types.SimpleNamespace(adjoint_n=128, steps=100, warmup=3, fd_dirs=0))
+        line["adjoint"] = {k: sub[k] for k in ("value", "unit", "steps", "ms_per_step", "adjoint", "J", "gradient",
+                                                "gpu_launches")}
+        line["adjoint"]["workload"] = sub["config"]["workload"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_sample_ndv, 2, 1)
     if rank == 0:
