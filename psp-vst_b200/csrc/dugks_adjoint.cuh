@@ -129,6 +129,19 @@ struct View {
 
 ADJ_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 ADJ_HD double magsqr3(const double* a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }
+
+// xi . Sf as the reference evaluates it: each product rounded, the sums
+// unfused, left to right.  Its sign picks the upwind side of a face and
+// whether a boundary DV is outgoing; on curved faces some DVs are
+// tangential up to rounding, so a contraction into FMAs would flip
+// decisions the forward made.
+ADJ_HD double xs_of(const double* xi, const double* S) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(__dadd_rn(__dmul_rn(xi[0], S[0]), __dmul_rn(xi[1], S[1])), __dmul_rn(xi[2], S[2]));
+#else
+    return (xi[0] * S[0] + xi[1] * S[1]) + xi[2] * S[2];
+#endif
+}
 ADJ_HD size_t at(int i, int n, int e) { return static_cast<size_t>(i) * n + e; }
 ADJ_HD int chunk_lo(int nv, int nch, int ch) { return static_cast<int>(static_cast<int64_t>(nv) * ch / nch); }
 
@@ -374,7 +387,7 @@ struct FInBy {
             const double* S = v.S + 3 * (v.nIF + b);
             for (int i = 0; i < v.nv; ++i) {
                 const double* xi = v.xi + 3 * i;
-                const double xs = dot3(xi, S);
+                const double xs = xs_of(xi, S);
                 if (xs < 0) acc += -v.w[i] * xs * eq_by_rho(v, xi, v.bU + 3 * b, v.bT[b]);
             }
         }
@@ -436,7 +449,7 @@ struct FFace {
     ADJ_HD void operator()(int64_t idx) const {
         const int i = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const double* xi = v.xi + 3 * i;
-        const double xs = dot3(xi, v.S + 3 * f);
+        const double xs = xs_of(xi, v.S + 3 * f);
         const size_t n = static_cast<size_t>(v.nv) * v.nC;
         const size_t cb = at(i, v.nC, 0);
         if (f < v.nIF) {
@@ -480,7 +493,7 @@ struct FWallOut {
         if (v.btype[b] == 1) {
             const double* S = v.S + 3 * f;
             for (int i = chunk_lo(v.nv, v.nchF, ch); i < chunk_lo(v.nv, v.nchF, ch + 1); ++i) {
-                const double xs = dot3(v.xi + 3 * i, S);
+                const double xs = xs_of(v.xi + 3 * i, S);
                 if (xs > 0) out += v.w[i] * xs * v.fg[at(i, v.nF, f)];
             }
         }
@@ -507,7 +520,7 @@ struct FWallIn {
         if (v.btype[b] != 1) return;
         const int f = v.nIF + b;
         const double* xi = v.xi + 3 * i;
-        if (dot3(xi, v.S + 3 * f) <= 0) {
+        if (xs_of(xi, v.S + 3 * f) <= 0) {
             const double Tb = v.bT[b];
             const double gi = v.rhow[b] * eq_by_rho(v, xi, v.bU + 3 * b, Tb);
             v.fg[at(i, v.nF, f)] = gi;
@@ -573,7 +586,7 @@ ADJ_HD bool relaxed_value(const View& v, int i, int f, double& gr, double& hr, d
     const size_t id = at(i, v.nF, f);
     gr = v.fg[id];
     hr = v.fh[id];
-    if (f >= v.nIF && !(dot3(xi, v.S + 3 * f) > 0)) return false;
+    if (f >= v.nIF && !(xs_of(xi, v.S + 3 * f) > 0)) return false;
     const double* m = v.fmac + kMac * static_cast<size_t>(f);
     const double Th = f < v.nIF ? m[MAC_T] : v.fmac[kMac * static_cast<size_t>(v.blocal[f - v.nIF]) + MAC_T];
     r = 0.5 * v.dt / (2.0 * m[MAC_TAU] + 0.5 * v.dt);
@@ -603,7 +616,7 @@ struct FUpdate {
         const double V = 1.0 / v.invV[c];
         for (int e = v.cf_off[c]; e < v.cf_off[c + 1]; ++e) {
             const int f = v.cf_ent[e] >> 1;
-            const double xs = dot3(xi, v.S + 3 * f);
+            const double xs = xs_of(xi, v.S + 3 * f);
             const size_t id = at(i, v.nF, f);
             if (v.cf_ent[e] & 1) {
                 g += (xs * v.ag[id] * v.dt / V);
@@ -631,7 +644,7 @@ struct FObjective {
             const double* xi = v.xi + 3 * i;
             double gr, hr, gEq, hEq, r;
             relaxed_value(v, i, f, gr, hr, gEq, hEq, r);
-            const double wx = v.w[i] * dot3(xi, S);
+            const double wx = v.w[i] * xs_of(xi, S);
             s += wx * (ea * 0.5 * (magsqr3(xi) * gr + hr) + v.wn * dot3(v.fw + 3 * b, xi) * gr);
         }
         v.Jb[b] += s;
@@ -664,7 +677,7 @@ struct RRelax {
         double s[12] = {0};
         for (int i = chunk_lo(v.nv, v.nchF, ch); i < chunk_lo(v.nv, v.nchF, ch + 1); ++i) {
             const double* xi = v.xi + 3 * i;
-            const double xs = dot3(xi, S);
+            const double xs = xs_of(xi, S);
             const size_t id = at(i, v.nF, f);
             const double lgo = v.lg[at(i, v.nC, ow)], lho = v.lh[at(i, v.nC, ow)];
             const double lgn = v.lg[at(i, v.nC, ne)], lhn = v.lh[at(i, v.nC, ne)];
@@ -750,7 +763,7 @@ struct RFaceMom {
             a_h += v.ah[id];
             v.ag[id] = a_g;
             v.ah[id] = a_h;
-            if (!bnd || dot3(xi, v.S + 3 * f) > 0) continue;
+            if (!bnd || xs_of(xi, v.S + 3 * f) > 0) continue;
             // incoming: g = rho_in E(U_in, T_b), h = g R T_b (K+3-D)
             const double Tb = v.bT[b], k3 = static_cast<double>(v.K + 3 - v.D);
             const double* Uin = type == 1 ? v.bU + 3 * b : v.cm + 9 * static_cast<size_t>(v.own[f]) + 1;
@@ -802,7 +815,7 @@ struct RWallOut {
         const int i = static_cast<int>(idx / v.nBF), b = static_cast<int>(idx % v.nBF);
         if (v.btype[b] != 1) return;
         const int f = v.nIF + b;
-        const double xs = dot3(v.xi + 3 * i, v.S + 3 * f);
+        const double xs = xs_of(v.xi + 3 * i, v.S + 3 * f);
         if (xs > 0) v.ag[at(i, v.nF, f)] += v.aout[b] * v.w[i] * xs;
     }
 };
@@ -820,7 +833,7 @@ struct RGradAdj {
         for (int e = v.cf_off[c]; e < v.cf_off[c + 1]; ++e) {
             const int f = v.cf_ent[e] >> 1;
             const bool is_nei = v.cf_ent[e] & 1;
-            const double xs = dot3(xi, v.S + 3 * f);
+            const double xs = xs_of(xi, v.S + 3 * f);
             double share;
             if (f >= v.nIF) share = xs > 0 ? 1.0 : 0.0;
             else if (xs >= kVSmall) share = is_nei ? 0.0 : 1.0;
@@ -955,7 +968,7 @@ struct RInBy {
         double sT = 0, sU[3] = {0, 0, 0};
         for (int i = 0; i < v.nv; ++i) {
             const double* xi = v.xi + 3 * i;
-            const double xs = dot3(xi, S);
+            const double xs = xs_of(xi, S);
             if (!(xs < 0)) continue;
             const double E = eq_by_rho(v, xi, v.bU + 3 * b, v.bT[b]);
             double dET, dEU[3];
