@@ -304,6 +304,28 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def sphere_loads(solver, case, steps_done):
+    """Drag and wall heat flux of the ball after steps_done steps: the
+    x-momentum and energy flux of the next step's relaxed DFs through the
+    sphere's wall faces (area vectors out of the gas, into the sphere),
+    from dugks_objective_run (it advances the solver by one step each)."""
+    import numpy as np
+    fl = case.flat
+    nb = fl["n_boundary"]
+    wall = np.zeros(nb, bool)
+    for p, t in enumerate(fl["patch_type"]):
+        if t == 1:
+            wall[fl["patch_start"][p]:fl["patch_start"][p + 1]] = True
+    mx = np.zeros((nb, 3))
+    mx[wall, 0] = 1.0
+    drag, _ = solver.objective(1, case.dt, None, mx)
+    heat, _ = solver.objective(1, case.dt, wall.astype(float), None)
+    area = float(np.linalg.norm(fl["Sf"][fl["n_internal"]:][wall], axis=1).sum())
+    return {"after_steps": steps_done, "drag_N": drag, "wall_heat_W": heat, "wall_area_m2": area,
+            "mean_wall_heat_flux_W_m2": heat / area,
+            "note": "fluxes of step %d (drag) and %d (heat) into the sphere wall" % (steps_done + 1, steps_done + 2)}
+
+
 def adjoint_case(n: int = 128, seed: int = 20261203):
     """The adjoint workload: n x n lid-driven cavity, 32^2 GH DVs, Kn 0.1,
     lid 50 m/s, every wall face at its own temperature 273 K + N(0, 5 K)
@@ -550,6 +572,8 @@ def main():
         import numpy as np
         ref = solver.macros()
         steps_done = W + 2 * K
+        if args.workload == "ball":
+            line["sphere"] = sphere_loads(solver, case, steps_done)
         del solver
         s32 = dl.Solver(case, precision=dl.FP32C, device=local)
         s32.step(W, case.dt)
