@@ -8,6 +8,12 @@ Run in a container that has the reference at REF (default /root/reference):
   is Python 2; only the text of those two functions is executed here (they
   run unchanged under Python 3 given an integer type whose `/` floors, as
   Python 2's does).
+* para_golden.json -- the case parameters of the reference demos' own
+  setup scripts (demo/cavity/para.py, demo/ball/para.py): gas constant,
+  density from Kn, dimensionless viscosity and muRef, for their own Kn and
+  for the Kn values of the benchmark configurations.  The scripts are
+  Python 2; their statements up to the first print are executed with Kn
+  (and L) substituted.
 * demo_cavity.npz -- the reference cavity demo's inputs
   (demo/cavity/constant/polyMesh, constant/Xis, constant/weights,
   constant/DVMProperties, 0/rho, 0/U, 0/T), so that the GPU tests can run
@@ -54,6 +60,22 @@ def reference_quadrature(ref):
     return out
 
 
+def reference_para(ref):
+    out = {}
+    for demo in ("cavity", "ball"):
+        src = open(os.path.join(ref, "demo", demo, "para.py")).read()
+        body = src.split("print")[0]
+        runs = {}
+        for kn in (None, 0.01, 0.075, 0.1, 1.0):
+            code = body if kn is None else re.sub(r"^Kn = .*$", f"Kn = {kn!r}", body, flags=re.M)
+            ns = {}
+            exec("from numpy import *\n" + code, ns)
+            runs["own" if kn is None else repr(kn)] = {k: float(ns[k]) for k in ("Kn", "R", "rho", "muBar", "mu", "C", "T",
+                                                                              "L", "omega_HS", "omega_VHS")}
+        out[demo] = runs
+    return out
+
+
 def demo_cavity(ref):
     d = os.path.join(ref, "demo/cavity")
     pm = meshgen.read_polymesh(d)
@@ -88,5 +110,7 @@ if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     with open(os.path.join(HERE, "quadrature_setdv.json"), "w") as f:
         json.dump(reference_quadrature(ref), f, indent=0)
+    with open(os.path.join(HERE, "para_golden.json"), "w") as f:
+        json.dump(reference_para(ref), f, indent=1)
     demo_cavity(ref)
     print("written:", sorted(os.listdir(HERE)))
