@@ -503,6 +503,19 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         *out = h;
         return st;
     }
+    if (h->precision == DUGKS_FP32C && !dvl) {
+        double *d_gref, *d_href;
+        if ((st = dev_alloc(h, &d_gref, dm.nv_loc)) || (st = dev_alloc(h, &d_href, dm.nv_loc)) ||
+            (st = dev_alloc(h, &ds.refmom, static_cast<size_t>(chunks) * dugks::kNM))) {
+            *out = h;
+            return st;
+        }
+        dm.gref = d_gref;
+        dm.href = d_href;
+    } else {
+        dm.gref = dm.href = nullptr;
+        ds.refmom = nullptr;
+    }
     ce = cudaMemset(ds.err, 0, 4 * sizeof(int));
     if (ce != cudaSuccess) return fail(DUGKS_ERR_CUDA, cudaGetErrorString(ce));
     ce = cudaMemset(ds.partF, 0, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM * sizeof(double));
@@ -646,6 +659,62 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     CUDA_TRY(h, cudaMemcpyAsync(h->ds.fm, fm.data(), fm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->ds.co, co_host, sizeof co_host, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaMemsetAsync(h->ds.err, 0, 4 * sizeof(int), h->stream));
+    if (h->dm.gref) {
+        // FP32 storage reference: the Maxwellian of the volume-mean density
+        // and the mass-weighted mean velocity and temperature of these macros
+        double vs = 0, ms = 0, mu[3] = {0, 0, 0}, mt = 0;
+        for (int o = 0; o < nC; ++o) {
+            const double Vm = h->V[o], mm = Vm * rho[o];
+            vs += Vm;
+            ms += mm;
+            for (int k = 0; k < 3; ++k) mu[k] += mm * U[3 * o + k];
+            mt += mm * T[o];
+        }
+        const double rb = ms / vs, Tb = mt / ms, RT = R * Tb;
+        const double Ub[3] = {mu[0] / ms, mu[1] / ms, mu[2] / ms};
+        const int nl = h->dm.nv_loc;
+        h->gref.assign(nl, 0.0);
+        h->href.assign(nl, 0.0);
+        for (int d = 0; d < nl; ++d) {
+            const double* xi = &h->xi[3 * static_cast<size_t>(h->dm.dv_base + d)];
+            const double c2 = (xi[0] - Ub[0]) * (xi[0] - Ub[0]) + (xi[1] - Ub[1]) * (xi[1] - Ub[1]) +
+                              (xi[2] - Ub[2]) * (xi[2] - Ub[2]);
+            h->gref[d] = rb * inv_norm_host(RT, D) * std::exp(-0.5 * c2 / RT);
+            h->href[d] = K3D * RT * h->gref[d];
+        }
+        CUDA_TRY(h, cudaMemcpyAsync(const_cast<double*>(h->dm.gref), h->gref.data(), nl * sizeof(double),
+                                    cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(const_cast<double*>(h->dm.href), h->href.data(), nl * sizeof(double),
+                                    cudaMemcpyHostToDevice, h->stream));
+        // raw moments of the reference over each DV chunk (moment record layout)
+        std::vector<double> rm(static_cast<size_t>(h->chunks) * dugks::kNM, 0.0);
+        for (int ch = 0; ch < h->chunks; ++ch) {
+            double* m = &rm[static_cast<size_t>(ch) * dugks::kNM];
+            for (int r = h->chunk_begin[ch]; r < h->chunk_begin[ch + 1]; ++r)
+                for (int ix = 0; ix < h->n1d; ++ix) {
+                    const int d = (r - h->dm.row_base) * h->n1d + ix;
+                    const double* xi = &h->xi[3 * static_cast<size_t>(h->dm.dv_base + d)];
+                    const double wd = h->w[h->dm.dv_base + d];
+                    const double a = wd * h->gref[d], u = a * (xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2]) +
+                                                          wd * h->href[d];
+                    m[dugks::MOM_M0] += a;
+                    m[dugks::MOM_W] += u;
+                    for (int k = 0; k < 3; ++k) {
+                        m[dugks::MOM_M1 + k] += a * xi[k];
+                        m[dugks::MOM_V3 + k] += u * xi[k];
+                    }
+                    m[dugks::MOM_M2] += a * xi[0] * xi[0];
+                    m[dugks::MOM_M2 + 1] += a * xi[0] * xi[1];
+                    m[dugks::MOM_M2 + 2] += a * xi[0] * xi[2];
+                    m[dugks::MOM_M2 + 3] += a * xi[1] * xi[1];
+                    m[dugks::MOM_M2 + 4] += a * xi[1] * xi[2];
+                    m[dugks::MOM_M2 + 5] += a * xi[2] * xi[2];
+                }
+        }
+        CUDA_TRY(h, cudaMemcpyAsync(h->ds.refmom, rm.data(), rm.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                    h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
     h->ds.cur = 0;
     dugks::StepArgs a = make_args(h, 0.0, 0.0);
     CUDA_TRY(h, dugks::launch_init(a, h->precision, h->stream));
@@ -1205,7 +1274,8 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
                 else {
                     float fv;
                     std::memcpy(&fv, &col[d * rs], sizeof fv);
-                    v = fv;
+                    const std::vector<double>& ref = which == 0 ? h->gref : h->href;
+                    v = ref.empty() ? fv : fv + ref[d];
                 }
                 dst[static_cast<size_t>(i) * h->dm.nv_loc + d] = v;
             }
@@ -1223,6 +1293,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
     const std::vector<int32_t>& perm = h->tiling.perm;
     for (int which = 0; which < 2; ++which) {
         void* dev = which == 0 ? h->ds.g[h->ds.cur] : h->ds.h[h->ds.cur];
+        const std::vector<double>& ref = which == 0 ? h->gref : h->href;
         if (get) {
             double* dst = which == 0 ? g : hh;
             if (!dst) continue;
@@ -1235,7 +1306,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
                     else {
                         float fv;
                         std::memcpy(&fv, &buf[s * rs], sizeof fv);
-                        dst[o] = fv;
+                        dst[o] = ref.empty() ? fv : fv + ref[d];
                     }
                 }
         } else {
@@ -1247,7 +1318,7 @@ static int state_io(dugks_handle* h, double* g, double* hh, const double* gi, co
                     const size_t o = static_cast<size_t>(d) * h->nC + perm[c];
                     if (rs == sizeof(double)) std::memcpy(&buf[s * rs], &src[o], sizeof(double));
                     else {
-                        const float fv = static_cast<float>(src[o]);
+                        const float fv = static_cast<float>(ref.empty() ? src[o] : src[o] - ref[d]);
                         std::memcpy(&buf[s * rs], &fv, sizeof fv);
                     }
                 }

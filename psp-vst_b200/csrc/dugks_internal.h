@@ -119,6 +119,12 @@ struct DevMesh {
     const double* bS;              // [nBF*3] boundary face area vectors
     int n_items;
     double xi_max_co;              // sqrt(D) * xiMax
+    // FP32 storage of a tensor DV set: g~, gbar+, the face values and the
+    // fluxes are stored as deviations from a per-DV reference Maxwellian,
+    // g = stored + gref[d] (h likewise), so that FP32 rounding acts on the
+    // deviation only; null for FP64 and for DV lists (absolute storage)
+    const double* gref;            // [nv_loc] local DVs
+    const double* href;
 };
 
 // Mutable device state
@@ -148,6 +154,10 @@ struct DevState {
     BRec* brec;        // [nBF]
     double* bmom_in;   // [nBF][kNM] incoming wall moments per unit rho_w
     double* cm;        // cell macros [nC][9]: rho U(3) T q(3) tau (renumbered)
+    // FP32 storage of a tensor DV set: the raw moments of the reference
+    // Maxwellian over each DV chunk, [chunks][kNM] (null otherwise); a face
+    // or cell whose DVs all count in full adds them once instead of per DV
+    double* refmom;
     double* fm;        // face macros [nF][9]
     double* co;        // [2] Courant max (as ordered bits) and sum
     int* err;          // [4] device error flags
@@ -185,6 +195,7 @@ struct dugks_handle {
     std::vector<int32_t> bface_mirror;   // symmetry faces: mirrored DV axis; -1 otherwise
     std::vector<double> xi, w;      // tensor-product DV set
     std::vector<double> X1, W1;     // one-dimensional nodes and weights
+    std::vector<double> gref, href; // host copy of the FP32-storage reference (empty: none)
     // geometry (original numbering)
     std::vector<int64_t> owner, neighbour;
     std::vector<double> C, V, Cf, Sf, weights, dc, lsP, lsN, lsB;

@@ -334,8 +334,16 @@ __global__ void k_init_state(const StepArgs a) {
         const double RT = m.R * cm[4];
         const double cx = cm[1] - m.xi[3 * d], cy = cm[2] - m.xi[3 * d + 1], cz = cm[3] - m.xi[3 * d + 2];
         const double ge = cm[0] * inv_norm(RT, m.D) * exp(-0.5 * (cx * cx + cy * cy + cz * cz) / RT);
-        reinterpret_cast<Real*>(a.ds.g[a.ds.cur])[i] = Real(ge);
-        reinterpret_cast<Real*>(a.ds.h[a.ds.cur])[i] = Real(K3D * ge * RT);
+        const double he = K3D * ge * RT;
+        if (sizeof(Real) == 4 && m.gref) {
+            // FP32 storage of a tensor DV set: the deviation from the reference
+            const int dl = static_cast<int>(i / m.nC);
+            reinterpret_cast<Real*>(a.ds.g[a.ds.cur])[i] = Real(ge - m.gref[dl]);
+            reinterpret_cast<Real*>(a.ds.h[a.ds.cur])[i] = Real(he - m.href[dl]);
+        } else {
+            reinterpret_cast<Real*>(a.ds.g[a.ds.cur])[i] = Real(ge);
+            reinterpret_cast<Real*>(a.ds.h[a.ds.cur])[i] = Real(he);
+        }
     }
 }
 
@@ -419,7 +427,9 @@ __global__ void k_state_moments(const StepArgs a) {
         const double xi[3] = {__ldg(m.xi + 3 * d), __ldg(m.xi + 3 * d + 1), __ldg(m.xi + 3 * d + 2)};
         const double xi2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
         const size_t idx = static_cast<size_t>(dl) * m.nC + c;
-        accum<D>(acc, __ldg(m.w + d), xi, xi2, double(g[idx]), double(h[idx]));
+        const double gr = (sizeof(Real) == 4 && m.gref) ? __ldg(m.gref + dl) : 0.0;
+        const double hr = (sizeof(Real) == 4 && m.href) ? __ldg(m.href + dl) : 0.0;
+        accum<D>(acc, __ldg(m.w + d), xi, xi2, double(g[idx]) + gr, double(h[idx]) + hr);
     }
     double* p = a.ds.partC + static_cast<size_t>(c) * kNM;
     for (int j = 0; j < 15; ++j) p[j] = acc[j];
@@ -458,10 +468,20 @@ __global__ void k_symmetry_in(const StepArgs a) {
         if (t == d) continue;
         const double w = __ldg(m.w + d), xi2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
         const size_t sd = static_cast<size_t>(d) * nI + it, st = static_cast<size_t>(t) * nI + it;
-        if (xi_dot_s(xi, S) > -kVSmall) accum<D>(acc, -w, xi, xi2, double(fg[sd]), double(fh[sd]));
-        fg[sd] = fg[st];
-        fh[sd] = fh[st];
-        accum<D>(acc, w, xi, xi2, double(fg[sd]), double(fh[sd]));
+        // FP32 storage of a tensor DV set holds deviations from the per-DV
+        // reference: the mirror's value moves with its own reference
+        const bool dev = sizeof(Real) == 4 && m.gref;
+        const double grd = dev ? m.gref[d] : 0.0, hrd = dev ? m.href[d] : 0.0;
+        const double grt = dev ? m.gref[t] : 0.0, hrt = dev ? m.href[t] : 0.0;
+        if (xi_dot_s(xi, S) > -kVSmall) accum<D>(acc, -w, xi, xi2, double(fg[sd]) + grd, double(fh[sd]) + hrd);
+        if (dev) {
+            fg[sd] = Real(double(fg[st]) + grt - grd);
+            fh[sd] = Real(double(fh[st]) + hrt - hrd);
+        } else {
+            fg[sd] = fg[st];
+            fh[sd] = fh[st];
+        }
+        accum<D>(acc, w, xi, xi2, double(fg[sd]) + grd, double(fh[sd]) + hrd);
     }
     double* p = a.ds.partF + static_cast<size_t>(it) * kNM;
     for (int j = 0; j < 14; ++j) p[j] += acc[j];

@@ -55,6 +55,25 @@ struct Width<float> {
     static constexpr int A0 = 8, A1 = 8, B0 = 8, B1 = 8;
 };
 
+// FP32 storage holds deviations from the per-DV reference Maxwellian
+// (DevMesh::gref, href): g = stored + ref.  These add and remove the
+// reference; for FP64 storage they are the identity and read nothing.
+template <typename Real>
+__device__ __forceinline__ double dv_ref(const double* ref, int d) {
+    if constexpr (sizeof(Real) == 4) return __ldg(ref + d);
+    else return 0.0;
+}
+template <typename Real>
+__device__ __forceinline__ double plus_ref(double x, double r) {
+    if constexpr (sizeof(Real) == 4) return x + r;
+    else return x;
+}
+template <typename Real>
+__device__ __forceinline__ double minus_ref(double x, double r) {
+    if constexpr (sizeof(Real) == 4) return x - r;
+    else return x;
+}
+
 // ---------------------------------------------------------------------
 // asynchronous global -> shared copies (cp.async, L1-allocating)
 // ---------------------------------------------------------------------
@@ -458,7 +477,8 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
-                                       int l, int part, bool active, double K3D, double c0h, bool ex_res) {
+                                       int l, int part, bool active, double K3D, double c0h, bool ex_res,
+                                       const double* gref, const double* href) {
     if (!active) return;
     Shk<double> s;
     s.Ux = sm.crec[CR_UX * kSL + l];
@@ -482,10 +502,11 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
         const int j = part * H + jj;
         if (FULL || j < bp.nb) {
             double go, ho;
-            shk_relax<D, double>(s, sm.x1[bp.ix0 + j], sx[j * kSL + l], double(sg[j * kSL + l]),
-                                 double(sg[(NB + j) * kSL + l]), K3D, c0h, go, ho);
-            sm.gB[j * kSL + l] = Real(go);
-            sm.hB[j * kSL + l] = Real(ho);
+            const double gr = dv_ref<Real>(gref, bp.d0 + j), hr = dv_ref<Real>(href, bp.d0 + j);
+            shk_relax<D, double>(s, sm.x1[bp.ix0 + j], sx[j * kSL + l], plus_ref<Real>(double(sg[j * kSL + l]), gr),
+                                 plus_ref<Real>(double(sg[(NB + j) * kSL + l]), hr), K3D, c0h, go, ho);
+            sm.gB[j * kSL + l] = Real(minus_ref<Real>(go, gr));
+            sm.hB[j * kSL + l] = Real(minus_ref<Real>(ho, hr));
         }
     }
 }
@@ -650,7 +671,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
             stage0<D, Real, NB, FULL>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
         }
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
-        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res);
+        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href);
         __syncthreads();
         stage2<D, Real, NB, FULL>(m, sm, bp, t);
         __syncthreads();
@@ -684,6 +705,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         gg = Real(0.5) * (g2 + g1);
                         hh = Real(0.5) * (h2 + h1);
                     }
+                    // FP32 storage: the deviations only; the reference part is added once below
                     row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
                     fg[j * nI] = gg;
                     fh[j * nI] = hh;
@@ -715,7 +737,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         gg *= cs;
                         hh *= cs;
-                        row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
+                        // this side's share of the face value and of its reference part
+                        const double gr = double(cs) * dv_ref<Real>(m.gref, bp.d0 + j);
+                        const double hr = double(cs) * dv_ref<Real>(m.href, bp.d0 + j);
+                        row_add(rs, sm.w1[bp.ix0 + j], x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
                         if (up) {
@@ -772,7 +797,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         } else {
                             continue;
                         }
-                        row_add(rs, wx, x, double(gg), double(hh));
+                        const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
+                        row_add(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
                     }
@@ -784,18 +810,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     const double x = sm.x1[bp.ix0 + j];
                     const double xs = xs_row(x, v.S[0], p2, p3);
                     const double wx = sm.w1[bp.ix0 + j];
+                    const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                     if (xs > 0) {
                         // outgoing: upwind from the owner (fvDVM.C:916-923, :950-961)
                         Real gg, hh;
                         recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
-                        const double aw = row_add(rs, wx, x, double(gg), double(hh));
+                        const double aw =
+                            row_add(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         if (wall) rs.O = fma(aw, xs, rs.O);
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
                     } else if (eq_in) {
                         const double cx = x - bU[0];
                         const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
-                        row_add(rs, wx, x, double(Real(ge)), double(Real(ge * bHf)));
+                        // rounded as pass B rounds the same incoming DF
+                        row_add(rs, wx, x, plus_ref<Real>(double(Real(minus_ref<Real>(ge, gr))), gr),
+                                plus_ref<Real>(double(Real(minus_ref<Real>(ge * bHf, hr))), hr));
                     }
                     // incoming wall DFs enter through rho_w in the face combine
                 }
@@ -804,6 +834,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         row_fold<D>(acc, rs, q);
     }
     if (has_item) {
+        if constexpr (sizeof(Real) == 4) {
+            // a tile-internal face counts every DV of the chunk in full: its
+            // moments gain the reference's chunk moments once
+            if (v.kind == ITEM_TILE_INTERNAL) {
+                const double* rm = a.ds.refmom + static_cast<size_t>(blockIdx.y) * kNM;
+#pragma unroll
+                for (int j = 0; j < 14; ++j) acc[j] += __ldg(rm + j);
+            }
+        }
         double* p = a.ds.partF + (static_cast<size_t>(blockIdx.y) * m.n_items + v.gi) * kNM;
 #pragma unroll
         for (int j = 0; j < 15; ++j) p[j] = acc[j];
@@ -960,10 +999,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             rg += __ldg(fvg + o);
                             rh += __ldg(fvh + o);
                         }
+                        const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                         double gf, hf;
-                        shk_relax<D, double>(fs, x, sx[j * kSI], double(rg), double(rh), K3D, c0h, gf, hf);
-                        sm.Fg[j * kSI + it] = Real(xs * gf);
-                        sm.Fh[j * kSI + it] = Real(xs * hf);
+                        shk_relax<D, double>(fs, x, sx[j * kSI], plus_ref<Real>(double(rg), gr),
+                                             plus_ref<Real>(double(rh), hr), K3D, c0h, gf, hf);
+                        // the reference part of the fluxes cancels over a closed cell (sum of +-Sf = 0)
+                        sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
+                        sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                     }
                 }
             } else {
@@ -1000,11 +1042,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                         if (FULL || j < bp.nb) {
                             const double x = sm.x1[bp.ix0 + j];
                             const double xs = xs_row(x, S[0], p2, p3);
-                            double gf = double(sg[j * kSI]), hf = double(sg[(NB + j) * kSI]);
+                            const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
+                            double gf = plus_ref<Real>(double(sg[j * kSI]), gr);
+                            double hf = plus_ref<Real>(double(sg[(NB + j) * kSI]), hr);
                             if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                             shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
-                            sm.Fg[j * kSI + it] = Real(xs * gf);
-                            sm.Fh[j * kSI + it] = Real(xs * hf);
+                            sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
+                            sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                         }
                     }
                 } else
@@ -1013,21 +1057,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
+                        const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                         double gf, hf;
                         if (xs > 0) {
-                            shk_relax<D, double>(fs, x, sx[j * kSI], double(sg[j * kSI]), double(sg[(NB + j) * kSI]),
-                                                 K3D, c0h, gf, hf);
+                            shk_relax<D, double>(fs, x, sx[j * kSI], plus_ref<Real>(double(sg[j * kSI]), gr),
+                                                 plus_ref<Real>(double(sg[(NB + j) * kSI]), hr), K3D, c0h, gf, hf);
                         } else if (stored_in) {
-                            gf = double(sg[j * kSI]);
-                            hf = double(sg[(NB + j) * kSI]);
+                            gf = plus_ref<Real>(double(sg[j * kSI]), gr);
+                            hf = plus_ref<Real>(double(sg[(NB + j) * kSI]), hr);
                         } else {
                             const double cx = x - bU[0];
                             const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
-                            gf = double(Real(ge));
-                            hf = double(Real(ge * bHf));
+                            gf = plus_ref<Real>(double(Real(minus_ref<Real>(ge, gr))), gr);
+                            hf = plus_ref<Real>(double(Real(minus_ref<Real>(ge * bHf, hr))), hr);
                         }
-                        sm.Fg[j * kSI + it] = Real(xs * gf);
-                        sm.Fh[j * kSI + it] = Real(xs * hf);
+                        sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
+                        sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                     }
                 }
             }
@@ -1048,8 +1093,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 if (FULL || j < bp.nb) {
                     const Real gt = pg[jj], ht = ph[jj];
                     const double x = sm.x1[bp.ix0 + j];
+                    const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                     double gb, hb;
-                    shk_relax<D, double>(cs, x, pe[jj], double(gt), double(ht), K3D, c0h, gb, hb);
+                    shk_relax<D, double>(cs, x, pe[jj], plus_ref<Real>(double(gt), gr), plus_ref<Real>(double(ht), hr),
+                                         K3D, c0h, gb, hb);
                     const Real* Fg = sm.Fg + j * kSI;
                     const Real* Fh = sm.Fh + j * kSI;
                     Real sg = 0, sh = 0;
@@ -1066,13 +1113,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             sh += e > 0 ? Fh[i] : -Fh[i];
                         }
                     }
-                    // the update in FP64, one rounding to the storage type
-                    const Real g_new = Real(fma(-1.0 / 3, double(gt), fma(4.0 / 3, gb, double(sg) * dtV)));
-                    const Real h_new = Real(fma(-1.0 / 3, double(ht), fma(4.0 / 3, hb, double(sh) * dtV)));
+                    // the update in FP64, one rounding to the storage type; with a
+                    // reference, -g/3 + 4/3 gbar+ - ref = -(g - ref)/3 + 4/3 (gbar+ - ref)
+                    const Real g_new =
+                        Real(fma(-1.0 / 3, double(gt), fma(4.0 / 3, minus_ref<Real>(gb, gr), double(sg) * dtV)));
+                    const Real h_new =
+                        Real(fma(-1.0 / 3, double(ht), fma(4.0 / 3, minus_ref<Real>(hb, hr), double(sh) * dtV)));
                     const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
                     gn[idx] = g_new;
                     hn[idx] = h_new;
-                    row_add(rs, sm.w1[bp.ix0 + j], x, double(g_new), double(h_new));
+                    row_add(rs, sm.w1[bp.ix0 + j], x, double(g_new), double(h_new));  // reference part below
                 }
             }
             row_fold<D>(acc, rs, q);
@@ -1089,6 +1139,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     if (part == 0 && has_cell) {
         for (int p = 1; p < kParts0; ++p)
             for (int j = 0; j < 15; ++j) acc[j] += sm.red[((p - 1) * kS0 + lc) * 15 + j];
+        if constexpr (sizeof(Real) == 4) {
+            // FP32 storage: the reference's moments over this chunk's DVs
+            const double* rm = a.ds.refmom + static_cast<size_t>(blockIdx.y) * kNM;
+            for (int j = 0; j < 14; ++j) acc[j] += __ldg(rm + j);
+        }
         double* dst = a.ds.partC + (static_cast<size_t>(blockIdx.y) * m.nC + c) * kNM;
 #pragma unroll
         for (int j = 0; j < 15; ++j) dst[j] = acc[j];
