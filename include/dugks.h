@@ -86,7 +86,11 @@ typedef enum dugks_patch_type {
 typedef enum dugks_precision {
     DUGKS_FP64 = 0,   /* FP64 storage and arithmetic, the plain path */
     DUGKS_FP32C = 1   /* FP32 g/h storage and flux arithmetic; FP64 moment accumulation,
-                         conserved update, heat-flux term and quadrature weights */
+                         conserved update, heat-flux term and quadrature weights.  With a
+                         tensor DV set the FP32 arrays hold deviations from the Maxwellian of
+                         the mean state that dugks_set_macros was given (one value per DV),
+                         so rounding acts on the deviation only; dugks_get_state,
+                         dugks_get_df and dugks_set_state convert to and from full values */
 } dugks_precision;
 
 /* Least-squares weighting (the stock leastSquares scheme as written in
