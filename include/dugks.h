@@ -398,6 +398,16 @@ int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, do
  * searches. */
 int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J, dugks_adjoint_stats* stats);
 
+/* Fluxes through every boundary face of the step a dugks_step(dt) from the
+ * current state would take, from the relaxed boundary DFs that its update
+ * uses (fvDVM::updateGHtildeVol, fvDVM.C:1500-1517); along Sf, i.e. out of
+ * the gas: flux[5b..5b+4] = sum_i w_i (xi_i.Sf) {g, xi_x g, xi_y g, xi_z g,
+ * (|xi|^2 g + h)/2} -- mass, momentum and energy per second.  A wall's drag
+ * is the sum of its faces' momentum fluxes, its heat load the sum of their
+ * energy fluxes.  The state does not advance.  FP64, unsharded handles with
+ * maxwellWall and farField patches (the dugks_adjoint_run restrictions). */
+int dugks_boundary_fluxes(dugks_handle* h, double dt, double* flux);
+
 /* The launch layout dugks_create chose: cells per tile (after shrinking
  * to fit), number of tiles and DV chunks per tile.  An autotuner reads it
  * to scale dugks_options.tile_cells / dv_chunks from the automatic choice. */

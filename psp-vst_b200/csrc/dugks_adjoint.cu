@@ -354,6 +354,35 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     return DUGKS_OK;
 }
 
+extern "C" int dugks_boundary_fluxes(dugks_handle* h, double dt, double* flux) {
+    if (!h) return DUGKS_ERR_ARG;
+    if (!flux) return set_error(h, DUGKS_ERR_ARG, "dugks_boundary_fluxes: null output");
+    dugks_objective obj{};
+    obj.n_steps = 1;
+    obj.dt = dt;
+    obj.max_snapshots = 1;
+    Arena ar;
+    adj::View v;
+    int sms = 0, st;
+    if ((st = prepare(h, &obj, "dugks_boundary_fluxes", ar, v, sms, false, nullptr))) return st;
+    const int nBF = h->nBF;
+    if (nBF == 0) return DUGKS_OK;
+    double* d_out;
+    if ((st = ar.get(h, &d_out, 5 * static_cast<size_t>(nBF)))) return st;
+    GpuEx ex{h, sms};
+    const int c = h->ds.cur;
+    v.g = static_cast<const double*>(h->ds.g[c]);
+    v.h = static_cast<const double*>(h->ds.h[c]);
+    v.cm = h->ds.cm;
+    if ((st = ex.run(nBF, adj::FInBy{v}))) return st;
+    if ((st = adj::record_step(ex, v))) return st;
+    if ((st = ex.run(nBF, adj::FBoundaryFlux{v, d_out}))) return st;
+    ADJ_TRY(h, cudaMemcpyAsync(flux, d_out, 5 * static_cast<size_t>(nBF) * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    ADJ_TRY(h, cudaStreamSynchronize(h->stream));
+    return DUGKS_OK;
+}
+
 extern "C" int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J,
                                    dugks_adjoint_stats* stats) {
     if (!h) return DUGKS_ERR_ARG;

@@ -651,6 +651,32 @@ struct FObjective {
     }
 };
 
+// mass, momentum and energy flux of every boundary face's relaxed DFs
+// (the fluxes of fvDVM::updateGHtildeVol, fvDVM.C:1500-1517), along Sf:
+// out[5b..5b+4] = sum_i w_i (xi_i.Sf) {g, xi g, (|xi|^2 g + h)/2}
+struct FBoundaryFlux {
+    View v;
+    double* out;
+    ADJ_HD void operator()(int64_t bi) const {
+        const int b = static_cast<int>(bi), f = v.nIF + b;
+        const double* S = v.S + 3 * f;
+        double m = 0, p[3] = {0, 0, 0}, e = 0;
+        for (int i = 0; i < v.nv; ++i) {
+            const double* xi = v.xi + 3 * i;
+            double gr, hr, gEq, hEq, r;
+            relaxed_value(v, i, f, gr, hr, gEq, hEq, r);
+            const double a = v.w[i] * xs_of(xi, S) * gr;
+            m += a;
+            for (int k = 0; k < 3; ++k) p[k] += a * xi[k];
+            e += v.w[i] * xs_of(xi, S) * 0.5 * (magsqr3(xi) * gr + hr);
+        }
+        double* o = out + 5 * static_cast<size_t>(b);
+        o[0] = m;
+        for (int k = 0; k < 3; ++k) o[1 + k] = p[k];
+        o[4] = e;
+    }
+};
+
 // ---------------------------------------------------------------- reverse
 
 // R1: adjoint of the relaxed face values (from the update and the

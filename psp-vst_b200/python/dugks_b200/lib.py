@@ -148,6 +148,7 @@ SIGNATURES = {
     "dugks_set_step_record": (C.c_int, [C.c_void_p, _dp]),
     "dugks_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, _dp, _dp, _dp, C.POINTER(AdjointStats)]),
     "dugks_objective_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, C.POINTER(AdjointStats)]),
+    "dugks_boundary_fluxes": (C.c_int, [C.c_void_p, C.c_double, _dp]),
     "dugks_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
@@ -428,6 +429,14 @@ class Solver:
         return {"J": J.value, "dT_b": dT, "dU_b": dU, "dmu": dmu.value,
                 "stats": {k: getattr(stats, k) for k in ("forward_steps", "reverse_steps", "snapshots", "ms_total",
                                                          "ms_forward", "device_bytes")}}
+
+    def boundary_fluxes(self, dt: float) -> np.ndarray:
+        """dugks_boundary_fluxes: [n_boundary, 5] mass, momentum (3) and
+        energy flux through every boundary face in the next step (along Sf,
+        out of the gas); the state does not advance."""
+        out = np.zeros((self.case.flat["n_boundary"], 5))
+        self._check(self.lib.dugks_boundary_fluxes(self.h, float(dt), ptr(out)))
+        return out
 
     def objective(self, n_steps: int, dt: float, energy_weight=None, momentum_weight=None,
                   window_start: int = 0) -> tuple[float, dict]:

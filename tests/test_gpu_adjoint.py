@@ -150,6 +150,34 @@ def test_adjoint_matches_central_differences_with_window():
         assert abs(a - fd) <= 1e-5 * abs(a), (d.keys(), a, fd)
 
 
+@pytest.mark.parametrize("which", ["cavity", "farfield"])
+def test_boundary_fluxes_match_the_oracle_step(which):
+    """dugks_boundary_fluxes after 3 steps gives the 4th step's per-face
+    fluxes: their energy and momentum sums equal the oracle's boundary-flux
+    objective of its 4th step's relaxed DFs (1e-10), and the state does not
+    advance."""
+    c = ac.cases()[which]
+    hw, fw, first = ac.objective_weights(c)
+    s = dl.Solver(c)
+    s.step(3, c.dt)
+    g0, _ = s.state()
+    F = s.boundary_fluxes(c.dt)
+    g1, _ = s.state()
+    assert np.array_equal(g0, g1)
+    o = ob.Oracle(c)
+    o.step(4, c.dt)
+    xi, w = c.dv_set()
+    _, _, gb, hb = o.face_values()
+    nb = c.flat["n_boundary"]
+    e_ref = ob.boundary_flux_objective(c, xi, w, gb, hb, np.ones(nb), np.zeros((nb, 3)))
+    m_ref = ob.boundary_flux_objective(c, xi, w, gb, hb, np.zeros(nb), fw)
+    assert abs(F[:, 4].sum() - e_ref) <= 1e-10 * abs(e_ref)
+    assert abs(F[first, 1].sum() - m_ref) <= 1e-10 * abs(m_ref)
+    # the same step through dugks_objective_run
+    J, _ = s.objective(1, c.dt, np.ones(nb), None)
+    assert abs(J - F[:, 4].sum()) <= 1e-12 * abs(J)
+
+
 def test_adjoint_refuses_unsupported_cases():
     c = cs.cavity_case(6, 6)
     s = dl.Solver(c, precision=dl.FP32C)
