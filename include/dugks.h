@@ -398,6 +398,11 @@ int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, double* J, do
  * searches. */
 int dugks_objective_run(dugks_handle* h, const dugks_objective* obj, double* J, dugks_adjoint_stats* stats);
 
+/* The forward steps a dugks_adjoint_run of n_steps with n_snapshots state
+ * copies runs (recomputation included), from its checkpoint schedule alone;
+ * no device work.  -1 on bad arguments or an inconsistent schedule. */
+int64_t dugks_checkpoint_forward_steps(int32_t n_steps, int32_t n_snapshots);
+
 /* Fluxes through every boundary face of the step a dugks_step(dt) from the
  * current state would take, from the relaxed boundary DFs that its update
  * uses (fvDVM::updateGHtildeVol, fvDVM.C:1500-1517); along Sf, i.e. out of

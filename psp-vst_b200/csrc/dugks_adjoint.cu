@@ -354,6 +354,33 @@ extern "C" int dugks_adjoint_run(dugks_handle* h, const dugks_objective* obj, do
     return DUGKS_OK;
 }
 
+namespace {
+// revolve's operations that only count what a run would do
+struct CountOps {
+    int64_t forward = 0, reverses = 0, saves = 0, restores = 0;
+    int next = 0;  // the step whose reverse comes next: must run n-1, ..., 0 in order
+    bool order_ok = true;
+    int save(int) { ++saves; return 0; }
+    int restore(int) { ++restores; return 0; }
+    int advance(int k) { forward += k; return 0; }
+    int reverse(int n) {
+        if (n != next) order_ok = false;
+        --next;
+        ++reverses;
+        return 0;
+    }
+};
+}  // namespace
+
+extern "C" int64_t dugks_checkpoint_forward_steps(int32_t n_steps, int32_t n_snapshots) {
+    if (n_steps < 1 || n_snapshots < 1) return -1;
+    CountOps ops;
+    ops.next = n_steps - 1;
+    const int slots = n_snapshots < n_steps ? n_snapshots : n_steps;
+    if (adj::revolve_run(ops, n_steps, slots) != 0 || !ops.order_ok || ops.reverses != n_steps) return -1;
+    return ops.forward;
+}
+
 extern "C" int dugks_boundary_fluxes(dugks_handle* h, double dt, double* flux) {
     if (!h) return DUGKS_ERR_ARG;
     if (!flux) return set_error(h, DUGKS_ERR_ARG, "dugks_boundary_fluxes: null output");

@@ -32,6 +32,7 @@
 // [entity][k] for per-entity records, [chunk][entity][kP] for partials.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -1068,15 +1069,49 @@ inline int chunks_for(int n_entities, int nv, int64_t target_threads) {
 
 // ---------------------------------------------------------------- checkpoints
 
-// Binomial checkpointing (Griewank's revolve schedule): with s snapshot
-// slots and r recomputations per step, beta(s, r) = C(s + r, s) steps can be
-// reversed.  Ops provides save(slot), restore(slot), advance(k) (k forward
-// steps from the current state) and reverse(n) (record and reverse step n,
-// whose start state is current).
-inline double beta(int s, int r) {
+// Binomial checkpointing (Griewank's revolve schedule).  A segment of n
+// steps whose start state is held in one slot, with c slots in all (that one
+// included), can be reversed with r recomputations of each step as long as
+// n <= beta(c, r) = C(c + r, c); the fewest forward steps are
+//   T(n, c) = r n - beta(c + 1, r - 1),  r the least with beta(c, r) >= n.
+// The next checkpoint goes m steps in, where the rest (n - m steps, c - 1
+// slots) needs exactly r recomputations and the first m steps (c slots)
+// r - 1: then m + T(n - m, c - 1) + T(m, c) = T(n, c) by Pascal's rule.
+// Ops provides save(slot), restore(slot), advance(k) (k forward steps from
+// the current state) and reverse(n) (record and reverse step n, whose start
+// state is current).
+inline double beta(int c, int r) {
+    if (r < 0) return 0;
     double b = 1;
-    for (int j = 1; j <= s; ++j) b = b * (r + j) / j;
+    for (int j = 1; j <= c; ++j) b = b * (r + j) / j;
     return b;
+}
+
+inline int reps_for(double n, int c) {
+    int r = 0;
+    while (beta(c, r) < n) ++r;
+    return r;
+}
+
+// fewest forward steps to reverse n steps with c slots (the start's included)
+inline double optimal_forward(int n, int c) {
+    if (n <= 1) return 0;
+    const int r = reps_for(n, c);
+    return r * static_cast<double>(n) - beta(c + 1, r - 1);
+}
+
+// offset of the next checkpoint in a segment of n >= 2 steps with c >= 2 slots
+inline int checkpoint_split(int n, int c) {
+    const int r = reps_for(n, c);
+    const double lo = std::max({static_cast<double>(n) - beta(c - 1, r), beta(c, r - 2) + 1, 1.0});
+    const double hi = std::min({static_cast<double>(n) - beta(c - 1, r - 1) - 1, beta(c, r - 1), n - 1.0});
+    if (lo <= hi) return static_cast<int>(hi);
+    // just past a boundary beta(c, r - 1) the optimal split mixes other
+    // recomputation counts: search for it
+    const double best = optimal_forward(n, c);
+    for (int m = n - 1; m >= 1; --m)
+        if (m + optimal_forward(n - m, c - 1) + optimal_forward(m, c) == best) return m;
+    return 1;
 }
 
 template <class Ops>
@@ -1092,10 +1127,7 @@ int revolve(Ops& ops, int a, int b, int slot_a, int free_lo, int free_n) {
         }
         return 0;
     }
-    int r = 1;
-    while (beta(free_n, r) < n) ++r;
-    const double first = beta(free_n, r - 1);
-    const int m = a + (first < n - 1 ? static_cast<int>(first) : n - 1);
+    const int m = a + checkpoint_split(n, free_n + 1);
     if ((st = ops.advance(m - a))) return st;
     if ((st = ops.save(free_lo))) return st;
     if ((st = revolve(ops, m, b, free_lo, free_lo + 1, free_n - 1))) return st;

@@ -149,6 +149,7 @@ SIGNATURES = {
     "dugks_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, _dp, _dp, _dp, C.POINTER(AdjointStats)]),
     "dugks_objective_run": (C.c_int, [C.c_void_p, C.POINTER(Objective), _dp, C.POINTER(AdjointStats)]),
     "dugks_boundary_fluxes": (C.c_int, [C.c_void_p, C.c_double, _dp]),
+    "dugks_checkpoint_forward_steps": (C.c_int64, [C.c_int32, C.c_int32]),
     "dugks_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p]),
     "dugks_n_dv": (C.c_int32, [C.c_void_p]),
     "dugks_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _dp, C.POINTER(C.c_void_p)]),
