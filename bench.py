@@ -58,7 +58,10 @@ def parse():
                    help="--workload batch: pick tile size and DV-chunk scale with the batch autotuner first")
     p.add_argument("--fd-dirs", type=int, default=0,
                    help="--workload adjoint: central-difference checks on this many random directions")
-    p.add_argument("--adjoint-n", type=int, default=0, help="--workload adjoint: cavity side (default 128)")
+    p.add_argument("--adjoint-n", type=int, default=0,
+                   help="--workload adjoint: cavity side (default 128), or the ball's cells per cube-face edge")
+    p.add_argument("--adjoint-case", choices=["cavity", "ball"], default="cavity",
+                   help="--workload adjoint: the lid-driven cavity, or far-field flow past the sphere")
     p.add_argument("--dv-shard", action="store_true",
                    help="N>1: shard the DV rows of one workload over the ranks (NCCL) instead of replicas")
     a = p.parse_args()
@@ -348,6 +351,30 @@ def run_adjoint(args):
     print(json.dumps(adjoint_line(args)), flush=True)
 
 
+def adjoint_ball_case(m: int = 8, seed: int = 20261203):
+    """The adjoint on a curved mesh: flow past the sphere (cubed sphere 6 x
+    m x m x m, stretch 1.12, 8^3 GH DVs, Ma 0.5, Kn 0.1), every wall face at
+    its own temperature 273 K + N(0, 5 K) (seeded); objective = heat load
+    into the sphere + drag (x-momentum flux into it)."""
+    import numpy as np
+    from dugks_b200 import case as cs
+    c = cs.ball_case(m, m, 1.12, 8, kn=0.1, mach=0.5)
+    fl = dict(c.flat)
+    nb = fl["n_boundary"]
+    wall = np.zeros(nb, bool)
+    for p, t in enumerate(fl["patch_type"]):
+        if t == 1:
+            wall[fl["patch_start"][p]:fl["patch_start"][p + 1]] = True
+    rng = np.random.default_rng(seed)
+    T_b = np.array(fl["T_b"], dtype=float)
+    T_b[wall] = 273.0 + rng.normal(0.0, 5.0, int(wall.sum()))
+    fl["T_b"] = T_b
+    c.flat = fl
+    fw = np.zeros((nb, 3))
+    fw[wall, 0] = 1.0
+    return c, wall.astype(float), fw, wall
+
+
 def adjoint_line(args):
     """--workload adjoint on one GPU: forward + reverse steps of the FP64
     adjoint (binomial checkpointing, <= 64 device snapshots), objective
@@ -360,8 +387,10 @@ def adjoint_line(args):
     import torch
     from dugks_b200 import lib as dl
     torch.cuda.set_device(0)
-    n_side = args.adjoint_n or 128
-    case, hw, fw, lid = adjoint_case(n_side)
+    ball = getattr(args, "adjoint_case", "cavity") == "ball"
+    n_side = args.adjoint_n or (8 if ball else 128)
+    # lid: the faces whose x velocity is the "speed" parameter (the lid, or the sphere)
+    case, hw, fw, lid = adjoint_ball_case(n_side) if ball else adjoint_case(n_side)
     N = max(4, args.steps)
     window = N - N // 4
     snaps = 64
@@ -420,9 +449,12 @@ def adjoint_line(args):
         "unit": "cell·DV forward+reverse steps/s", "n_gpus": 1, "steps": N, "warmup": W,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"adjoint: {n_side}x{n_side} lid-driven cavity, 32^2 GH DVs, Kn 0.1, lid 50 m/s, "
-                               f"{nb} wall faces at 273 K + N(0, 5 K), objective = wall heat flux + lid shear "
-                               f"averaged over the last {N - window} of {N} steps",
+        "config": {"workload": (f"adjoint: flow past the sphere, cubed sphere 6x{n_side}x{n_side}x{n_side}, 8^3 GH DVs, "
+                                f"Ma 0.5, Kn 0.1, {int(lid.sum())} wall faces at 273 K + N(0, 5 K), objective = sphere "
+                                f"heat load + drag averaged over the last {N - window} of {N} steps") if ball else
+                               (f"adjoint: {n_side}x{n_side} lid-driven cavity, 32^2 GH DVs, Kn 0.1, lid 50 m/s, "
+                                f"{nb} wall faces at 273 K + N(0, 5 K), objective = wall heat flux + lid shear "
+                                f"averaged over the last {N - window} of {N} steps"),
                    "cells": nc, "dvs": nv, "snapshots": st["snapshots"], "precision": "fp64",
                    "l2": "state %.2f GB, the record and adjoint arrays %.2f GB more"
                          % (16 * nc * nv / 1e9, st["device_bytes"] / 1e9)},
