@@ -597,41 +597,6 @@ ADJ_HD bool relaxed_value(const View& v, int i, int f, double& gr, double& hr, d
     return true;
 }
 
-// plain forward (stages 7-9), used to advance without the tiled passes:
-// relaxed face values into ag/ah, the new state into og/oh
-struct FRelax {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int i = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
-        double gEq, hEq, r;
-        relaxed_value(v, i, f, v.ag[idx], v.ah[idx], gEq, hEq, r);
-    }
-};
-struct FUpdate {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int i = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const double* xi = v.xi + 3 * i;
-        double g = -1.0 / 3 * v.g[idx] + 4.0 / 3 * v.gbp[idx];
-        double h = -1.0 / 3 * v.h[idx] + 4.0 / 3 * v.hbp[idx];
-        const double V = 1.0 / v.invV[c];
-        for (int e = v.cf_off[c]; e < v.cf_off[c + 1]; ++e) {
-            const int f = v.cf_ent[e] >> 1;
-            const double xs = xs_of(xi, v.S + 3 * f);
-            const size_t id = at(i, v.nF, f);
-            if (v.cf_ent[e] & 1) {
-                g += (xs * v.ag[id] * v.dt / V);
-                h += (xs * v.ah[id] * v.dt / V);
-            } else {
-                g -= (xs * v.ag[id] * v.dt / V);
-                h -= (xs * v.ah[id] * v.dt / V);
-            }
-        }
-        v.og[idx] = g;
-        v.oh[idx] = h;
-    }
-};
-
 // the objective of one step: every boundary face's energy and momentum flux
 // of its relaxed DFs, weighted by wn, added to Jb
 struct FObjective {
@@ -1024,14 +989,6 @@ int record_step(Ex& ex, const View& v) {
     }
     if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nF, FFaceMom{v}))) return st;
     return ex.run(v.nF, FFaceMac{v});
-}
-
-// plain forward step from the record: new state into og/oh
-template <class Ex>
-int advance_from_record(Ex& ex, const View& v) {
-    int st;
-    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nF, FRelax{v}))) return st;
-    return ex.run(static_cast<int64_t>(v.nv) * v.nC, FUpdate{v});
 }
 
 // reverse of one step from its record: og/oh = adjoint of the state before
