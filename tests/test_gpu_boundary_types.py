@@ -93,6 +93,22 @@ def test_fp32c_boundary_types():
     assert max(errs.values()) <= 5e-6, errs
 
 
+def test_fp32c_mirror_across_the_reference_velocity():
+    """FP32 storage holds deviations from the reference Maxwellian of the
+    mean state; with the gas moving along x, a DVMsymmetry outlet mirrors x
+    and the mirror DV has another reference value, which k_symmetry_in must
+    carry over.  FP32c = oracle to 5e-6 after 8 steps."""
+    c = cs.channel_case(10, 5, 8, sides={"top": {"kind": "symmetryPlane"}, "outlet": {"kind": "DVMsymmetry"},
+                                         "bottom": {"kind": "maxwellWall", "U": (50.0, 0.0, 0.0)}},
+                        U0=(60.0, 0.0, 0.0))
+    gpu, orc = dl.Solver(c, precision=dl.FP32C), ob.Oracle(c)
+    for _ in range(8):
+        gpu.evolution(c.dt)
+        orc.evolution(c.dt)
+    errs = ob.macro_errors(gpu.macros(), orc.macros(), c.gas["R"], floor=1e-2)
+    assert max(errs.values()) <= 5e-6, errs
+
+
 def test_restart_with_pressure_patches_is_exact():
     sides = {"inlet": {"kind": "pressureIn", "p": 1.2 * P1, "T": 273.0},
              "outlet": {"kind": "pressureOut", "p": P1, "T": 273.0}}
