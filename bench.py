@@ -70,24 +70,37 @@ def parse():
     return a
 
 
-def build_case(name, ndv1d=0, cube_n=64, kn=0.1):
+def build_case(name, ndv1d=0, cube_n=64, kn=0.1, geometry=None):
+    """The workload's case and its config description.  geometry: a
+    function of the PolyMesh giving its cell and face geometry (default:
+    the library's dugks_mesh_geometry; the reference arm passes the
+    oracle's restatement, which gives the same numbers bit for bit)."""
     from dugks_b200 import case as cs
     if name == "ball":
-        c = cs.ball_case(24, 32, 1.12, ndv1d or 16, kn=0.1, mach=0.5)
+        c = cs.ball_case(24, 32, 1.12, ndv1d or 16, kn=0.1, mach=0.5, flatten=False)
         cfg = {"workload": "ball: cubed sphere 6x24x24x32 (110592 cells), stretch 1.12, r 1..10, 16^3 GH DVs, "
-                           "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall",
-               "cells": c.n_cells, "n_dv": c.n_dv}
+                           "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall"}
     elif name == "cube":
-        c = cs.cube_case(cube_n, ndv1d or 20, kn=kn)
-        cfg = {"workload": f"cube: {cube_n}^3 lid-driven cube, {ndv1d or 20}^3 GH DVs, Kn {kn}, lid 50 m/s",
-               "cells": c.n_cells, "n_dv": c.n_dv}
+        c = cs.cube_case(cube_n, ndv1d or 20, kn=kn, flatten=False)
+        cfg = {"workload": f"cube: {cube_n}^3 lid-driven cube, {ndv1d or 20}^3 GH DVs, Kn {kn}, lid 50 m/s"}
     else:
-        c = cs.cavity_case(61, ndv1d or 28)
-        cfg = {"workload": "cavity: 61x61 lid-driven cavity, 28^2 GH DVs, Kn 0.075, lid 50 m/s", "cells": c.n_cells,
-               "n_dv": c.n_dv}
+        c = cs.cavity_case(61, ndv1d or 28, flatten=False)
+        cfg = {"workload": "cavity: 61x61 lid-driven cavity, 28^2 GH DVs, Kn 0.075, lid 50 m/s"}
+    c.flatten(geometry(c.mesh) if geometry is not None else None)
+    cfg["cells"] = c.n_cells
+    cfg["n_dv"] = c.n_dv
     cfg["dt"] = c.dt
     cfg["cfl"] = 0.5
     return c, cfg
+
+
+def run_config(cfg, precision, world, shard, nv_loc, nc):
+    """The config object both arms print for the same workload."""
+    rs = 8 if precision == "fp64" else 4
+    return dict(cfg, precision=precision,
+                parallelism=f"dv-shard x{world} (NCCL all-reduce of raw moments)" if shard
+                else f"replicas x{world}",
+                l2="inputs larger than L2 (state %.2f GB per GPU)" % (4 * rs * nc * nv_loc / 1e9))
 
 
 def profiled_traffic(kernel: str, precision: str):
@@ -177,30 +190,63 @@ def gpu_uuid(dev: int):
         return None
 
 
-def cpu_baseline(case_name: str, n1d: int, steps: int, warmup: int):
-    """The CPU restatement of the step (the reference itself cannot be built
-    here: it needs OpenFOAM, MPI and legacy TBB) on all host cores, on a
-    bounded sample of the workload: the same mesh with an n1d^D DV set."""
+def oracle_rate(case, threads: int, steps: int, warmup: int, xi=None, w=None):
+    """cell.DV updates/s and ms per step of the CPU oracle on `case` (or on
+    its mesh with the DV set xi, w), `threads` OpenMP threads."""
     import oracle_bind as ob
-    from dugks_b200 import case as cs
-    from dugks_b200 import quadrature
-    c, _ = build_case(case_name)
-    C = math.sqrt(2.0 * c.gas["R"] * c.gas["Tref"])
-    xis, w = quadrature.gauss_hermite_half_range(C, n1d)
-    xi, ww = quadrature.tensor_product(xis, w, c.D)
-    cores = os.cpu_count() or 1
-    o = ob.Oracle(c, threads=cores, xi=xi, w=ww)
+    o = ob.Oracle(case, threads=threads, xi=xi, w=w)
     for _ in range(warmup):
-        o.evolution(c.dt)
+        o.evolution(case.dt)
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.evolution(c.dt)
+        o.evolution(case.dt)
     t = time.perf_counter() - t0
-    n = c.n_cells * len(ww) * steps
+    n = case.n_cells * o.n_dv * steps
     o.close()
-    return {"value": n / t, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"same mesh ({c.n_cells} cells) with a {n1d}^{c.D} = {len(ww)}-DV Gauss-Hermite set, "
-                      f"{steps} steps after {warmup} warm-up, OpenMP over DVs/faces/cells ({cores} threads)"}
+    return n / t, 1e3 * t / steps
+
+
+def dv_sample(case, n1d: int):
+    """A smaller Gauss-Hermite set of the same form for a bounded CPU sample."""
+    from dugks_b200 import quadrature
+    C = math.sqrt(2.0 * case.gas["R"] * case.gas["Tref"])
+    xis, w = quadrature.gauss_hermite_half_range(C, n1d)
+    return quadrature.tensor_product(xis, w, case.D)
+
+
+def oracle_bytes(case, n_dv: int) -> int:
+    """Host memory of the oracle's per-(DV, cell) and per-(DV, face) arrays."""
+    fl = case.flat
+    return 8 * n_dv * (4 * case.n_cells + 2 * (fl["n_internal"] + fl["n_boundary"]))
+
+
+def host_available_bytes() -> int:
+    try:
+        return os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        return 0
+
+
+def cpu_baseline(case_name: str, n1d: int, steps: int, warmup: int, one_thread: bool = True):
+    """The CPU restatement of the step (the reference itself cannot be built
+    here: it needs OpenFOAM, MPI and legacy TBB) on all host cores, on a
+    bounded sample of the workload: the same mesh with an n1d^D DV set; and
+    on one thread, as the reference runs each rank (fvDVM.C:41)."""
+    import oracle_bind as ob
+    c, _ = build_case(case_name, geometry=ob.geometry)
+    xi, w = dv_sample(c, n1d)
+    cores = os.cpu_count() or 1
+    rate, ms = oracle_rate(c, cores, steps, warmup, xi, w)
+    out = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"same mesh ({c.n_cells} cells) with a {n1d}^{c.D} = {len(w)}-DV Gauss-Hermite set, "
+                     f"{steps} steps after {warmup} warm-up, OpenMP over DVs/faces/cells ({cores} threads)",
+           "ms_per_sample_step": ms}
+    if one_thread:
+        r1, ms1 = oracle_rate(c, 1, 1, 0, xi, w)
+        out["single_thread"] = {"value": r1, "unit": UNIT, "cores": 1, "ms_per_sample_step": ms1,
+                                "sample": f"the same {len(w)}-DV sample, 1 step, 1 thread (the reference's "
+                                          f"NUM_THREADS 1 per rank, fvDVM.C:41)"}
+    return out
 
 
 def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
@@ -474,17 +520,60 @@ def adjoint_line(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU oracle (the reference dugksFoam cannot be
+    built here: OpenFOAM, MPI and legacy TBB are absent) on the same
+    workload and config as the CUDA arm, W warm-up and K timed steps on all
+    host cores.  It loads no library of this repository: the mesh geometry
+    comes from the oracle's own restatement.  When the host cannot hold the
+    oracle's arrays, or the full DV set would not finish within a few
+    minutes, each step is a bounded sample instead (the same mesh with an
+    8^D Gauss-Hermite set), and `cpu_baseline.sample` says so."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, cfg = build_case(args.workload, args.ndv1d)
-    steps = max(1, min(args.steps, 5))
-    warm = 1
-    cb = cpu_baseline(args.workload, args.cpu_sample_ndv, steps, warm)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": warm, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    import oracle_bind as ob
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn, geometry=ob.geometry)
+    nc, nv = case.n_cells, case.n_dv
+    K, W = args.steps, max(3, args.warmup)
+    config = run_config(cfg, args.precision, world, args.dv_shard and world > 1, nv, nc)
+    cores = os.cpu_count() or 1
+    budget_s = 300.0   # warm-up + timed steps of the full workload
+    full = oracle_bytes(case, nv) < 0.6 * host_available_bytes()
+    rate = ms = None
+    if full:
+        o = ob.Oracle(case, threads=cores)
+        t0 = time.perf_counter()
+        o.evolution(case.dt)
+        t1 = time.perf_counter() - t0
+        if t1 * (W + K - 1) <= budget_s:
+            for _ in range(W - 1):
+                o.evolution(case.dt)
+            t0 = time.perf_counter()
+            for _ in range(K):
+                o.evolution(case.dt)
+            t = time.perf_counter() - t0
+            rate, ms = nc * nv * K / t, 1e3 * t / K
+            sample = (f"the full workload ({nc} cells x {nv} DVs), {K} steps after {W} warm-up, OpenMP over "
+                      f"DVs/faces/cells ({cores} threads)")
+        o.close()
+        del o
+    if rate is None:
+        why = "host memory" if not full else "time"
+        xi, w = dv_sample(case, 8)
+        rate, ms = oracle_rate(case, cores, K, W, xi, w)
+        sample = (f"bounded by {why}: same mesh ({nc} cells) with an 8^{case.D} = {len(w)}-DV Gauss-Hermite set "
+                  f"per step, {K} steps after {W} warm-up, OpenMP over DVs/faces/cells ({cores} threads)")
+    cb = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    xi, w = dv_sample(case, 8)
+    r1, ms1 = oracle_rate(case, 1, 1, 0, xi, w)
+    cb["single_thread"] = {"value": r1, "unit": UNIT, "cores": 1, "ms_per_sample_step": ms1,
+                           "sample": f"same mesh with an 8^{case.D} = {len(w)}-DV set, 1 step, 1 thread (the "
+                                     f"reference's NUM_THREADS 1 per rank, fvDVM.C:41)"}
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "cpu_baseline": cb,
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -579,10 +668,7 @@ def main():
         "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "strong" if shard is not None else "weak",
         "vs_baseline": None,
         "dtype": "f64" if prec == dl.FP64 else "f32 storage / f64 moments", "data": "synthetic",
-        "config": dict(cfg, precision=args.precision,
-                       parallelism=f"dv-shard x{world} (NCCL all-reduce of raw moments)" if shard is not None
-                       else f"replicas x{world}",
-                       l2="inputs larger than L2 (state %.2f GB per GPU)" % (4 * rs * nc * nv_loc / 1e9)),
+        "config": run_config(cfg, args.precision, world, shard is not None, nv_loc, nc),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 72 * nc + 16},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",

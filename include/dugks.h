@@ -46,7 +46,7 @@ typedef enum dugks_status {
     DUGKS_ERR_CUDA = 2,      /* a CUDA runtime call failed */
     DUGKS_ERR_OOM = 3,       /* device or host allocation failed */
     DUGKS_ERR_TIMEOUT = 4,   /* a bounded device wait ran out */
-    DUGKS_ERR_NAN = 5,       /* non-finite macroscopic state detected */
+    DUGKS_ERR_NAN = 5,       /* non-finite or non-positive rho/T given or computed */
     DUGKS_ERR_STATE = 6,     /* call out of order (e.g. step before set_macros) */
     DUGKS_ERR_UNSUPPORTED = 7
 } dugks_status;
@@ -260,7 +260,9 @@ int dugks_shard_phase(dugks_handle* h, int32_t phase, double dt, double** part, 
 
 /* fvDVM::fvDVM, second half: g~ = Maxwellian(rho,U,T), h~ = (K+3-D)RT g~,
  * wall inComingByRho, tau, q = 0, linear face velocity.
- * fvDVM.C:414-426, :578-624, :2115-2116.  U is [n_cells*3]. */
+ * fvDVM.C:414-426, :578-624, :2115-2116.  U is [n_cells*3].  A non-finite
+ * or non-positive rho or T, or a non-finite U, returns DUGKS_ERR_NAN and
+ * leaves the handle as it was (the reference runs on into NaNs). */
 int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const double* T);
 
 /* n_steps calls of fvDVM::evolution() (fvDVM.C:2128-2174) with time steps
@@ -310,7 +312,9 @@ int dugks_get_df(dugks_handle* h, const int32_t* cells, int32_t n, double* g_out
  * the Maxwellian on restart, fvDVM.C:414-426).  dugks_set_state (after
  * dugks_set_macros) recomputes the cell macros from the given DFs as
  * fvDVM::updateMacroVol does (fvDVM.C:1528-1554, :1682-1742); dt_prev is
- * the time step that produced them (it enters the heat-flux correction). */
+ * the time step that produced them (it enters the heat-flux correction).
+ * DFs whose moments give a non-finite or non-positive rho or T return
+ * DUGKS_ERR_NAN. */
 int dugks_get_state(dugks_handle* h, double* g, double* hh);
 int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double dt_prev);
 
@@ -454,11 +458,14 @@ void dugks_destroy(dugks_handle* h);
  * (others are rejected); gas is a host pointer; stream is a cudaStream_t
  * (NULL: the default stream); the call only enqueues work on it.  msg
  * (msg_len bytes, may be NULL) receives the error text.
+ * Each pointer's allocation must have room for what is read or written
+ * there (DUGKS_ERR_ARG otherwise, before any launch).
  * Limits: n_cells <= 131072 per call (DUGKS_ERR_ARG beyond).  The first call
- * on a device looks up the scratch address and caches it: make it before
- * any stream capture on that device.  Nothing has to start at zero.  Calls
- * that overlap in time on one device share the scratch and race: serialise
- * them. */
+ * on a device looks up the scratch address and caches it per CUDA context
+ * (a reset device is looked up again): make the first call in a context
+ * before any stream capture on that device.  Nothing has to start at zero.
+ * Calls that overlap in time on one device share the scratch and race:
+ * serialise them. */
 int dugks_cell_macros_noalloc(int32_t n_dims, int32_t n_dv, const double* xi, const double* w, int32_t n_cells,
                               const double* g, const double* hh, const dugks_gas* gas, double dt, double* rho,
                               double* U, double* T, double* q, void* stream, char* msg, int32_t msg_len);

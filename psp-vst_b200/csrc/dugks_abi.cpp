@@ -195,9 +195,23 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     h->C.assign(mesh->cell_centres, mesh->cell_centres + 3 * static_cast<size_t>(nC));
     h->V.assign(mesh->cell_volumes, mesh->cell_volumes + nC);
     for (int c = 0; c < nC; ++c)
-        if (!(h->V[c] > 0)) return fail(DUGKS_ERR_ARG, "dugks_create: non-positive cell volume");
+        if (!(h->V[c] > 0) || !std::isfinite(h->V[c])) return fail(DUGKS_ERR_ARG, "dugks_create: non-positive cell volume");
     h->Cf.assign(mesh->face_centres, mesh->face_centres + 3 * static_cast<size_t>(nF));
     h->Sf.assign(mesh->face_areas, mesh->face_areas + 3 * static_cast<size_t>(nF));
+    for (size_t i = 0; i < 3 * static_cast<size_t>(nC); ++i)
+        if (!std::isfinite(h->C[i])) return fail(DUGKS_ERR_ARG, "dugks_create: non-finite cell centre");
+    for (size_t i = 0; i < 3 * static_cast<size_t>(nF); ++i)
+        if (!std::isfinite(h->Cf[i]) || !std::isfinite(h->Sf[i]))
+            return fail(DUGKS_ERR_ARG, "dugks_create: non-finite face centre or area");
+    {
+        // every cell is the owner or neighbour of some face (a cell without
+        // faces has no flux list and no gradient stencil)
+        std::vector<unsigned char> seen(nC, 0);
+        for (int f = 0; f < nF; ++f) seen[h->owner[f]] = 1;
+        for (int f = 0; f < nIF; ++f) seen[h->neighbour[f]] = 1;
+        for (int c = 0; c < nC; ++c)
+            if (!seen[c]) return fail(DUGKS_ERR_ARG, "dugks_create: cell " + std::to_string(c) + " has no faces");
+    }
     h->patch_start.assign(mesh->patch_start, mesh->patch_start + h->nP + 1);
     if (h->nP == 0) h->patch_start.assign(1, 0);
     if (h->patch_start[0] != 0 || h->patch_start[h->nP] != nBF)
@@ -591,7 +605,13 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     std::vector<double> cr(static_cast<size_t>(dugks::REC_N) * nC, 0.0);
     for (int c = 0; c < nC; ++c) {
         const int o = t.perm[c];
-        if (!(rho[o] > 0) || !(T[o] > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_macros: rho and T must be > 0");
+        // a non-finite or non-positive macroscopic state is refused as the
+        // step refuses one it computes (DUGKS_ERR_NAN), before any launch
+        if (!(rho[o] > 0) || !(T[o] > 0) || !std::isfinite(rho[o]) || !std::isfinite(T[o]) ||
+            !std::isfinite(U[3 * o]) || !std::isfinite(U[3 * o + 1]) || !std::isfinite(U[3 * o + 2]))
+            return set_error(h, DUGKS_ERR_NAN,
+                             "dugks_set_macros: non-finite or non-positive rho/T (or non-finite U) in cell " +
+                                 std::to_string(o));
         const double tau = h->gas.mu_ref * std::exp(h->gas.omega * std::log(T[o] / h->gas.Tref)) / rho[o] / T[o] / R;
         double* m = &cm[9 * static_cast<size_t>(c)];
         m[0] = rho[o];
@@ -1338,6 +1358,8 @@ int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double d
     if (!(dt_prev > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: dt_prev must be > 0");
     dugks::StepArgs a = make_args(h, dt_prev, 0.0);
     a.dm.macro_flux = 0;   // the macros of given DFs are their moments (macroFlux yes: restore the step record)
+    // a new state replaces a poisoned one: its own check starts clear
+    CUDA_TRY(h, cudaMemsetAsync(h->ds.err, 0, 4 * sizeof(int), h->stream));
     CUDA_TRY(h, dugks::launch_state_moments(a, h->precision, h->stream));
     if ((st = shard_allreduce(h, h->ds.partC, static_cast<size_t>(h->nC) * dugks::kNM))) return st;
     CUDA_TRY(h, dugks::launch_cell_combine_one(a, 0.0, h->stream));

@@ -20,8 +20,14 @@
 //     moments per cell and DV chunk; 16 MiB in all); larger calls are
 //     rejected with DUGKS_ERR_ARG before anything is launched;
 //   * the first call on a device looks up the scratch address
-//     (cudaGetSymbolAddress) and caches it; make that first call before any
-//     stream capture on that device;
+//     (cudaGetSymbolAddress) and caches it, keyed by the device's current
+//     CUDA context: after cudaDeviceReset (or a released and re-created
+//     primary context) the module may load at another address, and the
+//     next call looks it up again; make the first call in each context
+//     before any stream capture on that device;
+//   * every buffer must have room for what the kernels touch: the call
+//     checks each pointer's allocation range and rejects short buffers with
+//     DUGKS_ERR_ARG before anything is launched;
 //   * nothing has to start at zero: every call writes each scratch element
 //     it reads before reading it;
 //   * calls that overlap in time on one device (different streams, or
@@ -30,6 +36,8 @@
 #include <mutex>
 #include <cstdarg>
 #include <cstdio>
+
+#include <cuda.h>   // driver types for the entry points below; libcuda is not linked
 
 #include "dugks_device.cuh"
 
@@ -47,7 +55,56 @@ constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
 
 std::mutex g_noalloc_mutex;
+// scratch address per device, and the id of the context it was looked up in
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kNoAllocMaxDevices] = {};
+
+// driver entry points reached through the runtime (no link-time dependency
+// on libcuda): the current context's unique id and allocation ranges
+struct DriverFns {
+    CUresult (*ctx_current)(CUcontext*) = nullptr;
+    CUresult (*ctx_id)(CUcontext, unsigned long long*) = nullptr;
+    CUresult (*addr_range)(CUdeviceptr*, size_t*, CUdeviceptr) = nullptr;
+};
+
+const DriverFns& driver_fns() {
+    static const DriverFns f = [] {
+        DriverFns d;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault) == cudaSuccess && p)
+            d.ctx_current = reinterpret_cast<CUresult (*)(CUcontext*)>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault) == cudaSuccess && p)
+            d.ctx_id = reinterpret_cast<CUresult (*)(CUcontext, unsigned long long*)>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault) == cudaSuccess && p)
+            d.addr_range = reinterpret_cast<CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr)>(p);
+        cudaGetLastError();
+        return d;
+    }();
+    return f;
+}
+
+// unique id of the current context (0: unknown)
+unsigned long long current_ctx_id() {
+    const DriverFns& d = driver_fns();
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!d.ctx_current || !d.ctx_id || d.ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (d.ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// true when the allocation holding p extends at least `bytes` past p
+bool has_room(const void* p, size_t bytes) {
+    const DriverFns& d = driver_fns();
+    if (!d.addr_range) return true;   // no range query on this driver: the type check alone
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    const CUdeviceptr dp = reinterpret_cast<CUdeviceptr>(p);
+    if (d.addr_range(&base, &size, dp) != CUDA_SUCCESS) return false;
+    return dp >= base && dp - base <= size && bytes <= size - (dp - base);
+}
 
 // raw moments of the DVs [d0, d1) of chunk blockIdx.y, one thread per cell;
 // rows of g, h are contiguous in cells, so a warp reads coalesced
@@ -155,17 +212,30 @@ extern "C" int dugks_cell_macros_noalloc(int32_t n_dims, int32_t n_dv, const dou
             return report(msg, msg_len, DUGKS_ERR_ARG,
                           "dugks_cell_macros_noalloc: argument %d is not device memory of the current device %d", i,
                           dev);
+    // ... and long enough for what the kernels read and write
+    const size_t nvc = static_cast<size_t>(n_dv) * n_cells, n1 = static_cast<size_t>(n_cells);
+    const size_t need[8] = {3 * static_cast<size_t>(n_dv), static_cast<size_t>(n_dv), nvc, nvc, n1, 3 * n1, n1, 3 * n1};
+    for (int i = 0; i < 8; ++i)
+        if (ptrs[i] && !has_room(ptrs[i], need[i] * sizeof(double)))
+            return report(msg, msg_len, DUGKS_ERR_ARG,
+                          "dugks_cell_macros_noalloc: argument %d is too small (needs %zu doubles)", i, need[i]);
 
     double* scratch = nullptr;
     {
+        // looked up once per device and context (a reset context may hold
+        // the module at another address)
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
+        const unsigned long long ctx = current_ctx_id();
+        if (!g_noalloc_ptr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p)
+            if (e != cudaSuccess || !p) {
+                g_noalloc_ptr[dev] = nullptr;
                 return report(msg, msg_len, DUGKS_ERR_CUDA, "dugks_cell_macros_noalloc: cudaGetSymbolAddress: %s",
                               cudaGetErrorString(e));
+            }
             g_noalloc_ptr[dev] = static_cast<double*>(p);
+            g_noalloc_ctx[dev] = ctx;
         }
         scratch = g_noalloc_ptr[dev];
     }

@@ -1,7 +1,9 @@
 """Generate the golden fixtures of tests/golden from the reference checkout.
 
-Run in a container that has the reference at REF (default /root/reference):
-    python tests/golden/gen_golden.py [REF]
+Run where the reference checkout is readable, giving its root as REF (the
+argument, or the environment variable DUGKS_REFERENCE; there is no
+default):
+    python tests/golden/gen_golden.py REF
 
 * quadrature_setdv.json -- nodes and weights produced by the reference's own
   generator functions dvGH / dvNC (src/scripts/setDV.py:83-138).  The script
@@ -107,7 +109,9 @@ def demo_cavity(ref):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DUGKS_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        sys.exit("usage: gen_golden.py REF  (the reference checkout's root; or set DUGKS_REFERENCE)")
     with open(os.path.join(HERE, "quadrature_setdv.json"), "w") as f:
         json.dump(reference_quadrature(ref), f, indent=0)
     with open(os.path.join(HERE, "para_golden.json"), "w") as f:

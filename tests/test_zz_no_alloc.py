@@ -139,3 +139,115 @@ def test_noalloc_rejects_oversize_and_host_buffers():
     st = lib.dugks_cell_macros_noalloc(2, 4, xi.data_ptr(), w.data_ptr(), 8, host.ctypes.data, g.data_ptr(),
                                        C.byref(gas), 1e-6, None, None, None, None, None, msg, len(msg))
     assert st == 1 and b"not device memory" in msg.value
+
+
+def _rt():
+    """The CUDA runtime the library itself links (already loaded by dl.load)."""
+    dl.load()
+    return C.CDLL("libcudart.so.12")
+
+
+def test_noalloc_rejects_short_device_buffers():
+    # a buffer from plain cudaMalloc holding far fewer doubles than n_dv x
+    # n_cells: the allocation range check refuses it before any launch
+    _torch()
+    lib = dl.load()
+    rt = _rt()
+    n_dv, n = 64, 1024
+    ptrs = []
+
+    def dmalloc(nbytes):
+        p = C.c_void_p()
+        assert rt.cudaMalloc(C.byref(p), C.c_size_t(nbytes)) == 0
+        ptrs.append(p)
+        return p
+
+    try:
+        xi, w = dmalloc(3 * n_dv * 8), dmalloc(n_dv * 8)
+        g_ok, g_short = dmalloc(n_dv * n * 8), dmalloc(4096)
+        rho = dmalloc(n * 8)
+        gas = dl.Gas(cs.R_DEMO, 0.81, 273.0, 2.117e-5, 2.0 / 3.0, 0)
+        msg = C.create_string_buffer(256)
+        st = lib.dugks_cell_macros_noalloc(3, n_dv, xi, w, n, g_short, g_ok, C.byref(gas), 1e-6, rho, None, None,
+                                           None, None, msg, len(msg))
+        assert st == 1 and b"argument 2 is too small" in msg.value, msg.value
+        for p, nbytes in zip(ptrs, (3 * n_dv * 8, n_dv * 8, n_dv * n * 8, 4096, n * 8)):
+            assert rt.cudaMemset(p, 0, C.c_size_t(nbytes)) == 0
+        st = lib.dugks_cell_macros_noalloc(3, n_dv, xi, w, n, g_ok, g_ok, C.byref(gas), 1e-6, rho, None, None,
+                                           None, None, msg, len(msg))
+        assert st == 0, msg.value
+        st = lib.dugks_cell_macros_noalloc(3, n_dv, xi, w, n, g_ok, g_ok, C.byref(gas), 1e-6, g_short, None, None,
+                                           None, None, msg, len(msg))
+        assert st == 1 and b"argument 4 is too small" in msg.value, msg.value
+        st = lib.dugks_cell_macros_noalloc(3, n_dv, xi, w, n, g_ok, g_ok, C.byref(gas), 1e-6, rho, rho, None,
+                                           None, None, msg, len(msg))
+        assert st == 1 and b"argument 5 is too small" in msg.value, msg.value
+        assert rt.cudaDeviceSynchronize() == 0
+    finally:
+        for p in ptrs:
+            rt.cudaFree(p)
+
+
+_RESET_SCRIPT = r'''
+import ctypes as C, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from dugks_b200 import case as cs
+from dugks_b200 import lib as dl
+from dugks_b200 import quadrature
+lib = dl.load()
+rt = C.CDLL("libcudart.so.12")
+c = cs.cavity_case(10, 8)
+xi, w = quadrature.tensor_product(c.xis, c.weights, 2)
+rng = np.random.default_rng(3)
+RT = c.gas["R"] * 273.0
+c2 = ((xi[:, None, :2] - 20.0 * rng.random((1, c.n_cells, 2))) ** 2).sum(-1)
+g = np.ascontiguousarray(1e-6 / (2 * np.pi * RT) * np.exp(-0.5 * c2 / RT) * (1 + 0.01 * rng.random(c2.shape)))
+hh = np.ascontiguousarray(g * RT)
+gas = dl.Gas(c.gas["R"], c.gas["omega"], c.gas["Tref"], c.gas["muRef"], c.gas["Pr"], 0)
+
+def run():
+    bufs = []
+    def put(a):
+        p = C.c_void_p()
+        assert rt.cudaMalloc(C.byref(p), C.c_size_t(a.nbytes)) == 0
+        assert rt.cudaMemcpy(p, a.ctypes.data_as(C.c_void_p), C.c_size_t(a.nbytes), 1) == 0
+        bufs.append(p)
+        return p
+    n = c.n_cells
+    outs = [np.zeros(n), np.zeros(3 * n), np.zeros(n), np.zeros(3 * n)]
+    d_in = [put(np.ascontiguousarray(a)) for a in (xi, w, g, hh)]
+    d_out = [put(o) for o in outs]
+    msg = C.create_string_buffer(256)
+    st = lib.dugks_cell_macros_noalloc(2, len(w), d_in[0], d_in[1], n, d_in[2], d_in[3], C.byref(gas), c.dt,
+                                       d_out[0], d_out[1], d_out[2], d_out[3], None, msg, len(msg))
+    assert st == 0, msg.value
+    assert rt.cudaDeviceSynchronize() == 0
+    for o, p in zip(outs, d_out):
+        assert rt.cudaMemcpy(o.ctypes.data_as(C.c_void_p), p, C.c_size_t(o.nbytes), 2) == 0
+    for p in bufs:
+        rt.cudaFree(p)
+    return outs
+
+first = run()
+assert rt.cudaDeviceReset() == 0
+second = run()
+assert all(np.array_equal(a, b) for a, b in zip(first, second))
+assert np.all(first[0] > 0) and np.all(first[2] > 0)
+print("reset ok")
+'''
+
+
+def test_noalloc_after_device_reset(tmp_path):
+    # the scratch address is cached per context: after cudaDeviceReset the
+    # next call looks it up again and gives the same macros (a fresh process
+    # without torch, which does not survive a device reset)
+    _torch()
+    import os
+    import subprocess
+    import sys
+    script = tmp_path / "reset.py"
+    script.write_text(_RESET_SCRIPT)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "psp-vst_b200", "python")
+    r = subprocess.run([sys.executable, str(script), pkg], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "reset ok" in r.stdout, r.stdout + r.stderr
