@@ -50,6 +50,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the short adjoint measurement of the default run")
+    p.add_argument("--no-cube", action="store_true",
+                   help="skip the mixed-precision sub-line of the default run (64^3 cube, 20^3 DVs, FP64 and FP32c)")
+    p.add_argument("--cube-steps", type=int, default=40,
+                   help="steps after which the cube sub-line compares FP32c with FP64")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
     p.add_argument("--cube-n", type=int, default=64, help="--workload cube: cells per side")
@@ -328,6 +332,23 @@ def run_batch(args):
     te = time.perf_counter() - te0
     rs = 8 if prec == dl.FP64 else 4
     peak, peak_kind = measured_peaks()
+    # the graph's own cost: the same 64 branches of kernels on 4x4 cavities
+    # with 6^2 DVs, whose kernels do almost nothing; its time per step
+    # bounds what a persistent kernel over all cases could save
+    from dugks_b200 import case as cs
+    tiny = [cs.cavity_case(4, 6) for _ in cases]
+    tsol = [dl.Solver(c, precision=prec) for c in tiny]
+    tb = dl.Batch(tsol, [c.dt for c in tiny])
+    tb.step(W)
+    tb.step(K)
+    floor_ms = tb.last_ms() / K
+    floor = {"ms_per_step": floor_ms, "kernels_per_step": tb.graph_kernels() // 2,
+             "us_per_kernel": 1e3 * floor_ms / max(1, tb.graph_kernels() // 2),
+             "share_of_batch_step": floor_ms / (t_ms / K),
+             "workload": "64 cavities of 4x4 cells x 6^2 DVs in the same graph structure"}
+    tb.close()
+    for s_ in tsol:
+        s_.close()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -343,6 +364,7 @@ def run_batch(args):
                 "d2h_bytes_per_step": sum(72 * c.n_cells for c in cases) // 2},
         "gpu_launches": launches,
         "graph_kernels_per_two_steps": batch.graph_kernels(),
+        "graph_floor": floor,
         "autotune": tuning,
         "step_roofline": {"bytes_per_update": 6 * rs, "achieved": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9,
                           "frac": 6 * rs * pairs / (t_ms / K / 1e3) / 1e9 / peak, "peak": peak,
@@ -371,6 +393,47 @@ def sphere_loads(solver, case, steps_done):
     return {"after_steps": steps_done, "drag_N": drag, "wall_heat_W": heat, "wall_area_m2": area,
             "mean_wall_heat_flux_W_m2": heat / area, "wall_mass_flux_kg_s": float(F[wall, 0].sum()),
             "note": "fluxes of step %d into the sphere wall" % (steps_done + 1)}
+
+
+def cube_line(n: int = 64, n1d: int = 20, kn: float = 0.1, steps: int = 40, timed: int = 5, device: int = 0):
+    """The mixed-precision configuration on one GPU: lid-driven cube of n^3
+    cells, n1d^3 Gauss-Hermite DVs, lid 50 m/s.  FP64 and FP32c (FP32
+    deviation storage, FP64 relaxation and moment sums) each advance
+    `steps` steps from the same uniform start; steps 3..2+timed are timed
+    with CUDA events; then FP32c's rho, U, T, q are compared with FP64's by
+    plain relative L2.  The two solvers run one after the other (the FP64
+    state and face values take about 160 GB at 64^3 x 20^3)."""
+    import numpy as np
+    from dugks_b200 import case as cs
+    from dugks_b200 import lib as dl
+    c = cs.cube_case(n, n1d, kn=kn)
+    nc, nv = c.n_cells, c.n_dv
+    out = {"workload": f"cube: {n}^3 lid-driven cube, {n1d}^3 GH DVs, Kn {kn}, lid 50 m/s",
+           "cells": nc, "n_dv": nv, "dt": c.dt, "steps": steps, "timed_steps": timed}
+    peak, peak_kind = measured_peaks()
+    mac = {}
+    for name, prec, rs in (("fp64", dl.FP64, 8), ("fp32c", dl.FP32C, 4)):
+        try:
+            s = dl.Solver(c, precision=prec, device=device)
+        except dl.DugksError as e:
+            out[name] = {"error": str(e)}
+            continue
+        s.step(2, c.dt)
+        st = s.step_timed(timed, c.dt)
+        s.step(steps - 2 - timed, c.dt)
+        mac[name] = s.macros()
+        ms = float(st[4]) / timed
+        out[name] = {"value": nc * nv / (ms / 1e3), "ms_per_step": ms,
+                     "pass_a_ms": float(st[0]) / timed, "pass_b_ms": float(st[2]) / timed,
+                     "step_roofline_frac": 6 * rs * nc * nv / (ms / 1e3) / 1e9 / peak}
+        s.close()
+        del s
+    if "fp64" in mac and "fp32c" in mac:
+        a, b = mac["fp32c"], mac["fp64"]
+        out["fp32c_rel_l2_vs_fp64"] = {k: float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k]))
+                                       for k in ("rho", "U", "T", "q")}
+        out["fp32c_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["fp32c"]["ms_per_step"]
+    return out
 
 
 def adjoint_case(n: int = 128, seed: int = 20261203):
@@ -704,6 +767,10 @@ def main():
         del s32
     else:
         del solver
+    if rank == 0 and world == 1 and not args.no_cube and args.workload == "ball" and not args.ndv1d:
+        # the mixed-precision configuration itself: FP32c against FP64 on the
+        # 64^3 x 20^3 cube
+        line["cube"] = cube_line(steps=max(8, args.cube_steps), device=local)
     if rank == 0 and world == 1 and not args.no_adjoint and args.workload == "ball":
         # the adjoint configuration (128x128 cavity, 32^2 DVs, FP64) over a
         # short horizon: forward + reverse steps with <= 64 snapshots

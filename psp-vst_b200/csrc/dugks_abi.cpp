@@ -122,6 +122,8 @@ int check_device_errors(dugks_handle* h) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (err[0] & 1) return set_error(h, DUGKS_ERR_NAN, "non-finite or non-positive rho/T in the cell macros");
     if (err[0] & 2) return set_error(h, DUGKS_ERR_TIMEOUT, "a bounded device wait ran out");
+    if (err[0] & 4)
+        return set_error(h, DUGKS_ERR_ARG, "an index in the device tables was out of range (bounds-checked build)");
     return DUGKS_OK;
 }
 
@@ -316,14 +318,19 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         if (!std::isfinite(x)) return fail(DUGKS_ERR_ARG, "dugks_create: singular least-squares system");
 
     // tiles: at most kMaxTile cells, kMaxLocal cells with the ring, and one
-    // item per thread; shrink until the largest tile fits
-    int tile = opt.tile_cells > 0 ? opt.tile_cells : dugks::kMaxTile;
-    tile = std::min(tile, dugks::kMaxTile);
-    for (;;) {
-        dugks::build_tiling(h, tile);
-        const bool fits = h->tiling.max_items <= dugks::kMaxItems && h->tiling.max_local <= dugks::kMaxLocal;
-        if (fits || tile <= 4) break;
-        tile = std::max(4, tile * 7 / 8);
+    // item per thread.  By default greedy tiles as large as those limits
+    // allow; a given tile_cells cuts uniform tiles, shrunk until the largest
+    // fits
+    if (opt.tile_cells > 0) {
+        int tile = std::min(opt.tile_cells, dugks::kMaxTile);
+        for (;;) {
+            dugks::build_tiling(h, tile);
+            const bool fits = h->tiling.max_items <= dugks::kMaxItems && h->tiling.max_local <= dugks::kMaxLocal;
+            if (fits || tile <= 4) break;
+            tile = std::max(4, tile * 7 / 8);
+        }
+    } else {
+        dugks::build_tiling(h, 0);
     }
     if (h->tiling.max_items > dugks::kMaxItems || h->tiling.max_local > dugks::kMaxLocal)
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: cells with too many faces for the tile layout");
@@ -492,12 +499,15 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     const size_t nvc = static_cast<size_t>(dm.nv_loc) * nC;
     const size_t nfv = static_cast<size_t>(dm.nv_loc) * std::max(dm.n_items, 1);
     unsigned char* p;
-    for (int i = 0; i < 2; ++i) {
-        if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
-        ds.g[i] = p;
-        if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
-        ds.h[i] = p;
-    }
+    // One state buffer.  Pass B reads each (DV, cell) entry of its own L0
+    // cells once and then writes it, and no kernel of a step reads the old
+    // state after pass B, so the update runs in place: g[1], h[1] alias
+    // g[0], h[0] and the step's buffer flip changes nothing.  This halves
+    // the state's HBM (the FP64 64^3 x 20^3 cube fits one B200 with it).
+    if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
+    ds.g[0] = ds.g[1] = p;
+    if ((st = dev_alloc(h, &p, nvc * rs))) return *out = h, st;
+    ds.h[0] = ds.h[1] = p;
     if ((st = dev_alloc(h, &p, nfv * rs))) return *out = h, st;
     ds.fvg = p;
     if ((st = dev_alloc(h, &p, nfv * rs))) return *out = h, st;

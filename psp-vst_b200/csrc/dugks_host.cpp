@@ -266,12 +266,79 @@ void rcb_order(const std::vector<double>& C, std::vector<int32_t>& idx, size_t b
     rcb_order(C, idx, b + nl, e, tile);
 }
 
+// Greedy tile boundaries over the RCB cell order: each tile takes the next
+// cells in order while it keeps at most kMaxTile L0 cells, kMaxLocal cells
+// with its ring and kMaxItems faces.  A pass CTA costs about the same
+// whatever its tile's size, so the fewest tiles that fit is the aim; tiles
+// end where the ring, not a fixed size, runs out.
+std::vector<int32_t> greedy_bounds(int nC, int nIF, const std::vector<int64_t>& owner,
+                                   const std::vector<int64_t>& neighbour, const std::vector<int32_t>& cfo,
+                                   const std::vector<int32_t>& cfl, const std::vector<int32_t>& perm,
+                                   const std::vector<int32_t>& iperm) {
+    std::vector<int32_t> bounds(1, 0);
+    std::vector<unsigned char> in_l0(nC, 0);
+    std::vector<int32_t> ring_cnt(nC, 0);  // L0 neighbours of a cell outside L0
+    std::vector<int32_t> fresh;
+    int b = 0, ring = 0, items = 0;
+    // fn(n) for every face of renumbered cell c: n the renumbered cell on
+    // the other side, -1 for a boundary face
+    auto others = [&](int c, auto&& fn) {
+        const int o = perm[c];
+        for (int k = cfo[o]; k < cfo[o + 1]; ++k) {
+            const int f = cfl[k];
+            if (f < nIF) fn(iperm[owner[f] == o ? neighbour[f] : owner[f]]);
+            else fn(-1);
+        }
+    };
+    for (int c = 0; c < nC; ++c) {
+        int d_items = 0, d_ring = ring_cnt[c] > 0 ? -1 : 0;
+        fresh.clear();
+        others(c, [&](int n) {
+            if (n < 0) {
+                ++d_items;
+            } else if (!in_l0[n]) {
+                ++d_items;
+                if (ring_cnt[n] == 0 && std::find(fresh.begin(), fresh.end(), n) == fresh.end()) {
+                    fresh.push_back(n);
+                    ++d_ring;
+                }
+            }
+        });
+        const int n0 = c - b;
+        const bool fits = n0 + 1 <= dugks::kMaxTile && n0 + 1 + ring + d_ring <= dugks::kMaxLocal &&
+                          items + d_items <= dugks::kMaxItems;
+        if (n0 > 0 && !fits) {
+            // close the tile [b, c); cell c starts the next one
+            for (int x = b; x < c; ++x) {
+                in_l0[x] = 0;
+                others(x, [&](int n) {
+                    if (n >= 0) ring_cnt[n] = 0;
+                });
+            }
+            bounds.push_back(c);
+            b = c;
+            ring = items = 0;
+            --c;
+            continue;
+        }
+        in_l0[c] = 1;
+        items += d_items;
+        ring += d_ring;
+        others(c, [&](int n) {
+            if (n >= 0 && !in_l0[n]) ++ring_cnt[n];
+        });
+    }
+    bounds.push_back(nC);
+    return bounds;
+}
+
 }  // namespace
 
 namespace dugks {
 
 // Tile layout.  Cells are renumbered by recursive coordinate bisection and
-// cut into tiles of `tile_cells` consecutive cells (L0).  Each tile also
+// cut into tiles of `tile_cells` consecutive cells (L0), or, with
+// tile_cells = 0, into the greedy tiles of greedy_bounds.  Each tile also
 // holds its ring L1 (face neighbours of L0 outside it), and one item per
 // face touching L0, sorted by item kind.  Gradient stencils and flux lists
 // are stored slot-major ([slot][cell]) so that consecutive threads read
@@ -281,7 +348,8 @@ void build_tiling(dugks_handle* h, int tile_cells) {
     const int nC = h->nC, nIF = h->nIF, nBF = h->nBF;
     t.perm.resize(nC);
     std::iota(t.perm.begin(), t.perm.end(), 0);
-    rcb_order(h->C, t.perm, 0, nC, tile_cells);
+    const bool greedy = tile_cells <= 0;
+    rcb_order(h->C, t.perm, 0, nC, greedy ? 4 : tile_cells);
     t.iperm.assign(nC, 0);
     for (int c = 0; c < nC; ++c) t.iperm[t.perm[c]] = c;
 
@@ -301,8 +369,16 @@ void build_tiling(dugks_handle* h, int tile_cells) {
         t.nf_max = std::max(t.nf_max, cfo[c + 1] - cfo[c]);
     }
 
-    t.tile_cells = tile_cells;
-    t.n_tiles = (nC + tile_cells - 1) / tile_cells;
+    std::vector<int32_t> bounds;
+    if (greedy) {
+        bounds = greedy_bounds(nC, nIF, h->owner, h->neighbour, cfo, cfl, t.perm, t.iperm);
+    } else {
+        for (int b = 0; b < nC; b += tile_cells) bounds.push_back(b);
+        bounds.push_back(nC);
+    }
+    t.n_tiles = static_cast<int>(bounds.size()) - 1;
+    t.tile_cells = 0;
+    for (int ti = 0; ti < t.n_tiles; ++ti) t.tile_cells = std::max(t.tile_cells, bounds[ti + 1] - bounds[ti]);
     t.tile_begin.assign(t.n_tiles + 1, 0);
     t.tile_loc_off.assign(t.n_tiles + 1, 0);
     t.tile_item_off.assign(t.n_tiles + 1, 0);
@@ -322,7 +398,7 @@ void build_tiling(dugks_handle* h, int tile_cells) {
         int kind, f;
     };
     for (int ti = 0; ti < t.n_tiles; ++ti) {
-        const int b = ti * tile_cells, e = std::min(nC, b + tile_cells), n0 = e - b;
+        const int b = bounds[ti], e = bounds[ti + 1], n0 = e - b;
         t.tile_begin[ti] = b;
         t.tile_loc_off[ti] = static_cast<int32_t>(t.loc_cells.size());
         std::vector<int32_t> l1;

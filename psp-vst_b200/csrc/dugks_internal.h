@@ -129,7 +129,7 @@ struct DevMesh {
 
 // Mutable device state
 struct DevState {
-    void* g[2];        // state g~ double buffer [nv][nC] (Real)
+    void* g[2];        // state g~ [nv][nC] (Real); g[1] aliases g[0]: pass B updates in place
     void* h[2];
     int cur;
     // face values [nv][n_items] (Real): pass A's upwind reconstruction at the

@@ -26,7 +26,8 @@ namespace {
 __device__ __forceinline__ void sum_face_partials(const StepArgs& a, int f, double* s) {
     const DevMesh& m = a.dm;
     for (int j = 0; j < 15; ++j) s[j] = 0.0;
-    const int i0 = __ldg(m.face_items + 2 * f), i1 = __ldg(m.face_items + 2 * f + 1);
+    const int i0 = chk(__ldg(m.face_items + 2 * f), 0, m.n_items, a.ds.err);
+    const int i1 = chk(__ldg(m.face_items + 2 * f + 1), -1, m.n_items, a.ds.err);
     for (int ch = 0; ch < a.chunks; ++ch) {
         const double* p0 = a.ds.partF + (static_cast<size_t>(ch) * m.n_items + i0) * kNM;
         for (int j = 0; j < 15; ++j) s[j] += p0[j];
@@ -72,7 +73,7 @@ __device__ __forceinline__ void write_face(const StepArgs& a, const Consts& k, i
     const size_t n = static_cast<size_t>(a.dm.n_items);
     double* fr = a.ds.facerec;
     for (int side = 0; side < 2; ++side) {
-        const int it = __ldg(a.dm.face_items + 2 * f + side);
+        const int it = chk(__ldg(a.dm.face_items + 2 * f + side), -1, a.dm.n_items, a.ds.err);
         if (it < 0) continue;
         fr[REC_UX * n + it] = U[0];
         fr[REC_UY * n + it] = U[1];
@@ -191,12 +192,14 @@ __device__ __forceinline__ void macro_flux_update(const StepArgs& a, const Const
     rE = rho * (0.5 * (U0[0] * U0[0] + U0[1] * U0[1] + U0[2] * U0[2]) + (k.Kin + 3) / 2.0 * k.R * cm[4]);
     const double V = __ldg(m.mf_V + c), dt = k.dt;
     for (int e = __ldg(m.mf_off + c); e < __ldg(m.mf_off + c + 1); ++e) {
-        const int code = __ldg(m.mf_ent + e), f = code >> 1;
+        const int code = __ldg(m.mf_ent + e), f = chk(code >> 1, 0, m.nIF + m.nBF, a.ds.err);
         const bool add = code & 1;
         const double* fm = a.ds.fm + static_cast<size_t>(f) * 9;
         const double rf = fm[0], Uf[3] = {fm[1], fm[2], fm[3]}, qf[3] = {fm[5], fm[6], fm[7]};
         const double* S = m.mf_Sf + 3 * static_cast<size_t>(f);
-        const double* Sm = f < m.nIF ? S : m.mf_Sf + 3 * static_cast<size_t>(__ldg(m.bface_patch_local + f - m.nIF));
+        const double* Sm = f < m.nIF ? S
+                                     : m.mf_Sf + 3 * static_cast<size_t>(chk(__ldg(m.bface_patch_local + f - m.nIF), 0,
+                                                                             m.nIF + m.nBF, a.ds.err));
         const double rUf[3] = {__dmul_rn(rf, Uf[0]), __dmul_rn(rf, Uf[1]), __dmul_rn(rf, Uf[2])};
         const double rEf = __dmul_rn(rf, __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(Uf[0], Uf[0]), __dmul_rn(Uf[1], Uf[1])),
                                                              __dmul_rn(Uf[2], Uf[2])),
@@ -449,8 +452,8 @@ __global__ void k_symmetry_in(const StepArgs a) {
     if (b >= m.nBF) return;
     const int axis = __ldg(m.bface_mirror + b);
     if (axis < 0) return;
-    const int it = __ldg(m.face_items + 2 * (m.nIF + b));
-    const int b0 = b - __ldg(m.bface_patch_local + b);
+    const int it = chk(__ldg(m.face_items + 2 * (m.nIF + b)), 0, m.n_items, a.ds.err);
+    const int b0 = chk(b - __ldg(m.bface_patch_local + b), 0, m.nBF, a.ds.err);
     const double S0[3] = {__ldg(m.bS + 3 * b0), __ldg(m.bS + 3 * b0 + 1), __ldg(m.bS + 3 * b0 + 2)};
     const double S[3] = {__ldg(m.bS + 3 * b), __ldg(m.bS + 3 * b + 1), __ldg(m.bS + 3 * b + 2)};
     Real* fg = reinterpret_cast<Real*>(a.ds.fvg);
@@ -500,7 +503,7 @@ __global__ void k_pressure_bc(const StepArgs a) {
     const int pt = __ldg(m.bface_ptype + b);
     if (pt != DUGKS_PATCH_PRESSURE_IN && pt != DUGKS_PATCH_PRESSURE_OUT) return;
     BRec* br = a.ds.brec + b;
-    const double* cm = a.ds.cm + static_cast<size_t>(__ldg(m.bface_owner + b)) * 9;
+    const double* cm = a.ds.cm + static_cast<size_t>(chk(__ldg(m.bface_owner + b), 0, m.nC, a.ds.err)) * 9;
     const double rhoi = cm[0], Ui[3] = {cm[1], cm[2], cm[3]}, Ti = cm[4];
     const double R = m.R, p = br->p;
     const double ai = sqrt(R * Ti * (m.K + 5) / (m.K + 3));

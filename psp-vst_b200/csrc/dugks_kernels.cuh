@@ -24,6 +24,23 @@ struct StepArgs {
 
 enum { STAGE_PASS_A = 0, STAGE_FACE_COMBINE = 1, STAGE_PASS_B = 2, STAGE_CELL_COMBINE = 3 };
 
+// Bounds-checked build (-DDUGKS_CHECK, libdugks_b200_check.so): every index
+// the kernels read from a device table is tested against its range before
+// use.  One outside [lo, hi) sets bit 2 (value 4) of the handle's error
+// flags and is replaced by lo, so the access stays in bounds; the host then
+// returns DUGKS_ERR_ARG.  In the normal build the check is the index itself.
+#ifdef DUGKS_CHECK
+__device__ __forceinline__ int chk(int i, int lo, int hi, int* err) {
+    if (i < lo || i >= hi) {
+        atomicOr(err, 4);
+        return lo;
+    }
+    return i;
+}
+#else
+__device__ __forceinline__ int chk(int i, int, int, int*) { return i; }
+#endif
+
 // one DUGKS step (fvDVM::evolution) on the handle's stream, or one stage
 // of it; `launches` (may be null) is incremented by the kernels launched
 cudaError_t launch_step(const StepArgs& a, int precision, cudaStream_t s, int* launches);

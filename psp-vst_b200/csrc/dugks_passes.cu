@@ -541,7 +541,7 @@ __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, in
 
 template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB>& sm, const BatchPos& bp,
-                                       const TileRange& t) {
+                                       const TileRange& t, int* err) {
     const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
     if (l >= t.n0) return;
     const int c = t.b + l;
@@ -574,8 +574,9 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
 #pragma unroll
             for (int q = 0; q < D; ++q) gx[q] = hx[q] = Real(0);
             for (int k = 0; k < m.nb_max; ++k) {
-                const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
-                if (n < 0) continue;
+                const int n0 = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
+                if (n0 < 0) continue;
+                const int n = chk(n0, 0, t.nloc, err);
                 const Real dg = gB[n] - g0, dh = hB[n] - h0;
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     load_dv_tables(m, sm.x1, sm.w1);
     const int l1 = threadIdx.x % kSL, p1 = threadIdx.x / kSL;
     const bool act1 = l1 < t.nloc;
-    const int c1 = act1 ? __ldg(m.loc_cells + t.loff + l1) : 0;
+    const int c1 = act1 ? chk(__ldg(m.loc_cells + t.loff + l1), 0, m.nC, a.ds.err) : 0;
     if (act1 && p1 == 0) {
         const double* cr = a.ds.cellrec;
         const size_t n = static_cast<size_t>(m.nC);
@@ -643,7 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 #pragma unroll
         for (int k = 0; k < kMaxRegStencil; ++k) {
             const int n = (l < t.n0 && k < m.nb_max) ? __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c) : -1;
-            sm.snb[k * kS0 + l] = n >= 0 ? n : l;
+            sm.snb[k * kS0 + l] = n >= 0 ? chk(n, 0, t.nloc, a.ds.err) : l;
 #pragma unroll
             for (int q = 0; q < D; ++q)
                 sm.sls[(k * D + q) * kS0 + l] =
@@ -653,7 +654,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const int it = threadIdx.x;
     const bool has_item = it < t.nit;
     Item v{};
-    if (has_item) v = load_item(m, t.ioff + it);
+    if (has_item) {
+        v = load_item(m, t.ioff + it);
+        v.la = chk(v.la, 0, t.nloc, a.ds.err);
+        if (v.kind != ITEM_MESH_BOUNDARY) v.lb = chk(v.lb, 0, t.nloc, a.ds.err);
+        else v.face = chk(v.face, 0, m.nBF, a.ds.err);
+        if (v.kind == ITEM_TB_OWN || v.kind == ITEM_TB_NEI) v.other = chk(v.other, 0, m.n_items, a.ds.err);
+    }
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
@@ -673,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
         stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href);
         __syncthreads();
-        stage2<D, Real, NB, FULL>(m, sm, bp, t);
+        stage2<D, Real, NB, FULL>(m, sm, bp, t, a.ds.err);
         __syncthreads();
         if (!has_item) continue;
         // stage 3
@@ -714,12 +721,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         } else if (v.kind != ITEM_MESH_BOUNDARY) {
             // tile-boundary face: this tile's side only, weighted 1 upwind,
             // 1/2 tangential, 0 downwind; the other tile adds its side.  The
-            // upwind tile writes the face value into both items' slots, so
-            // that pass B reads one slot; tangential halves stay in their
-            // own slots
+            // face value is written once, into the upwind side's slot (pass
+            // B of the downwind tile reads it there); tangential halves stay
+            // in their own slots
             const bool own_side = v.kind == ITEM_TB_OWN;
-            Real* og = fvg + static_cast<size_t>(bp.d0) * nI + v.other;
-            Real* oh = fvh + static_cast<size_t>(bp.d0) * nI + v.other;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 if (FULL || j < bp.nb) {
@@ -743,10 +748,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         row_add(rs, sm.w1[bp.ix0 + j], x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
                         fh[j * nI] = hh;
-                        if (up) {
-                            og[j * nI] = gg;
-                            oh[j * nI] = hh;
-                        }
                     }
                 }
             }
@@ -770,7 +771,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                 if (pt == DUGKS_PATCH_MIXED) {
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
                 } else {
-                    const int own = __ldg(m.bface_owner + v.face);
+                    const int own = chk(__ldg(m.bface_owner + v.face), 0, m.nC, a.ds.err);
                     const size_t n = static_cast<size_t>(m.nC);
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * n + own);
                 }
@@ -863,19 +864,40 @@ __device__ __forceinline__ float flip_sign(float v, unsigned neg) {
     return __int_as_float(__float_as_int(v) ^ static_cast<int>(neg << 31));
 }
 
-// cp.async of an item's own face-value slot and Maxwellian x factors for a
-// batch (each thread stages and later reads only its own item's entries)
-template <typename Real, int NB, bool FULL>
+// Where an item reads its face value from: its own slot, or, on a
+// tile-boundary face whose other side is upwind, the other side's slot
+// (pass A writes each upwind value once)
+struct SlotPick {
+    int other;          // the other side's item, -1: always the own slot
+    bool own_side;      // this side is the face's owner
+    double Sx, Sy, Sz;  // area vector
+};
+
+// cp.async of an item's face values and Maxwellian x factors for a batch
+// (each thread stages and later reads only its own item's entries)
+template <int D, typename Real, int NB, bool FULL>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
-                                            const Real* __restrict__ fvh, const double* __restrict__ ftab, size_t nI,
-                                            int it, int gi) {
-    const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
+                                            const Real* __restrict__ fvh, const double* __restrict__ ftab,
+                                            const double* __restrict__ X1, size_t nI, int it, int gi,
+                                            const SlotPick& sp) {
     const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
+    double p2 = 0, p3 = 0;
+    if (sp.other >= 0) {
+        p2 = __dmul_rn(__ldg(X1 + bp.iy), sp.Sy);
+        p3 = D == 3 ? __dmul_rn(__ldg(X1 + bp.iz), sp.Sz) : 0.0;
+    }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         if (FULL || j < bp.nb) {
-            cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
-            cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
+            int src = gi;
+            if (sp.other >= 0) {
+                // the same xi.S and thresholds as pass A's upwind choice
+                const double xs = xs_row(__ldg(X1 + bp.ix0 + j), sp.Sx, p2, p3);
+                if (sp.own_side ? xs < -kVSmall : xs >= kVSmall) src = sp.other;
+            }
+            const size_t at = static_cast<size_t>(bp.d0 + j) * nI + src;
+            cp_async(sm.st + j * kSI + it, fvg + at);
+            cp_async(sm.st + (NB + j) * kSI + it, fvh + at);
             cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
         }
     }
@@ -928,6 +950,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     if (has_item) {
         kind = __ldg(m.it_meta + gi) & 15;
         other = __ldg(m.it_other + gi);
+        if (kind == ITEM_TB_OWN || kind == ITEM_TB_NEI) other = chk(other, 0, m.n_items, a.ds.err);
 #pragma unroll
         for (int q = 0; q < 3; ++q) S[q] = __ldg(m.it_geo + q * nI + gi);
         stash_rec(sm.frec, kSI, it, a.ds.facerec, nI, gi);
@@ -946,7 +969,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
 #pragma unroll
     for (int s = 0; s < kRegFaces; ++s) {
         const int e = (has_cell && s < m.nf_max) ? __ldg(m.cf_item + static_cast<size_t>(s) * nC + c) : 0;
-        ent_off[s] = e == 0 ? kSI - 1 : (e > 0 ? e : -e) - 1;
+        ent_off[s] = e == 0 ? kSI - 1 : chk((e > 0 ? e : -e) - 1, 0, t.nit, a.ds.err);
         ent_neg[s] = e < 0 ? 1u : 0u;
     }
     if (threadIdx.x == kThreads - 1) {
@@ -955,6 +978,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             sm.Fh[j * kSI + kSI - 1] = Real(0);
         }
     }
+    const bool tb_item = kind == ITEM_TB_OWN || kind == ITEM_TB_NEI;
+    const SlotPick sp{tb_item ? other : -1, kind == ITEM_TB_OWN, S[0], S[1], S[2]};
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
@@ -965,7 +990,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
-        if (has_item) stage_items<Real, NB, FULL>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
+        if (has_item) stage_items<D, Real, NB, FULL>(sm, walk.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
         if (has_cell) fetch_cells<Real, NB, FULL>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
     }
     for (int k = 0; k < nbt; ++k, walk.next()) {
@@ -984,9 +1009,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             cp_wait_all();  // this item's staged entries of batch k
             const Real* sg = sm.st + it;
             if (kind != ITEM_MESH_BOUNDARY) {
-                // internal and tile-boundary faces: the staged slot holds the
-                // upwind face value; on an exactly tangential tile-boundary
-                // face it holds this side's half and the other slot the rest
+                // internal and tile-boundary faces: the staged value is the
+                // upwind face value (from the upwind side's slot); on an
+                // exactly tangential tile-boundary face it is this side's
+                // half and the other slot holds the rest
                 const bool tb = kind != ITEM_TILE_INTERNAL;
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
@@ -1018,7 +1044,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 // here; zero-gradient and symmetry ones come from the face-value
                 // buffer.  DVMsymmetry relaxes every DV once more
                 // (fvDVM.C:1445-1453).  Read per batch: boundary items are few.
-                const int face = __ldg(m.it_face + gi);
+                const int face = chk(__ldg(m.it_face + gi), 0, m.nBF, a.ds.err);
                 const int pt = __ldg(m.it_meta + gi) >> 4;
                 const bool stored_in = pt == DUGKS_PATCH_ZERO_GRADIENT || pt == DUGKS_PATCH_SYMMETRY ||
                                        pt == DUGKS_PATCH_DVM_SYMMETRY;
@@ -1030,7 +1056,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 if (pt == DUGKS_PATCH_MAXWELL_WALL || pt == DUGKS_PATCH_MIXED) {
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
                 } else {
-                    const int own = __ldg(m.bface_owner + face);
+                    const int own = chk(__ldg(m.bface_owner + face), 0, m.nC, a.ds.err);
                     for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * nC + own);
                 }
                 const double cyz = (q.Y - bU[1]) * (q.Y - bU[1]) + (q.Z - bU[2]) * (q.Z - bU[2]);
@@ -1077,7 +1103,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 }
             }
             // this thread has read its staged entries: stage the next batch
-            if (k + 1 < nbt) stage_items<Real, NB, FULL>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
+            if (k + 1 < nbt) stage_items<D, Real, NB, FULL>(sm, ahead.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
         }
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
@@ -1108,7 +1134,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     for (int s = kRegFaces; s < m.nf_max; ++s) {
                         const int e = __ldg(m.cf_item + static_cast<size_t>(s) * nC + c);
                         if (e != 0) {
-                            const int i = (e > 0 ? e : -e) - 1;
+                            const int i = chk((e > 0 ? e : -e) - 1, 0, t.nit, a.ds.err);
                             sg += e > 0 ? Fg[i] : -Fg[i];
                             sh += e > 0 ? Fh[i] : -Fh[i];
                         }

@@ -118,7 +118,7 @@ __device__ __forceinline__ void add_dv(double* acc, double w, const double xi[3]
 // row-factored pass's stage 2)
 template <int D, typename Real, int NB>
 __device__ __forceinline__ void stage2_gen(const DevMesh& m, const SmemAG<D, Real, NB>& sm, int nb,
-                                           const TileRange& t) {
+                                           const TileRange& t, int* err) {
     const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
     if (l >= t.n0) return;
     const int c = t.b + l;
@@ -143,8 +143,9 @@ __device__ __forceinline__ void stage2_gen(const DevMesh& m, const SmemAG<D, Rea
             }
         } else {
             for (int k = 0; k < m.nb_max; ++k) {
-                const int n = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
-                if (n < 0) continue;
+                const int n0 = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
+                if (n0 < 0) continue;
+                const int n = chk(n0, 0, t.nloc, err);
                 const Real dg = gB[n] - g0, dh = hB[n] - h0;
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a_gen(const StepArgs a) {
 
     const int l1 = threadIdx.x % kSL, p1 = threadIdx.x / kSL;
     const bool act1 = l1 < t.nloc;
-    const int c1 = act1 ? __ldg(m.loc_cells + t.loff + l1) : 0;
+    const int c1 = act1 ? chk(__ldg(m.loc_cells + t.loff + l1), 0, m.nC, a.ds.err) : 0;
     const Rec<double> cr1 = act1 ? rec_at(a.ds.cellrec, nC, c1) : Rec<double>{};
     if (threadIdx.x < kS0 && m.nb_max <= kMaxRegStencil) {
         const int l = threadIdx.x;
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a_gen(const StepArgs a) {
 #pragma unroll
         for (int k = 0; k < kMaxRegStencil; ++k) {
             const int n = (l < t.n0 && k < m.nb_max) ? __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c) : -1;
-            sm.snb[k * kS0 + l] = n >= 0 ? n : l;
+            sm.snb[k * kS0 + l] = n >= 0 ? chk(n, 0, t.nloc, a.ds.err) : l;
 #pragma unroll
             for (int q = 0; q < D; ++q)
                 sm.sls[(k * D + q) * kS0 + l] =
@@ -196,7 +197,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a_gen(const StepArgs a) {
     const int it = threadIdx.x;
     const bool has_item = it < t.nit;
     Item v{};
-    if (has_item) v = load_item(m, t.ioff + it);
+    if (has_item) {
+        v = load_item(m, t.ioff + it);
+        v.la = chk(v.la, 0, t.nloc, a.ds.err);
+        if (v.kind != ITEM_MESH_BOUNDARY) v.lb = chk(v.lb, 0, t.nloc, a.ds.err);
+        else v.face = chk(v.face, 0, m.nBF, a.ds.err);
+        if (v.kind == ITEM_TB_OWN || v.kind == ITEM_TB_NEI) v.other = chk(v.other, 0, m.n_items, a.ds.err);
+    }
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
@@ -248,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a_gen(const StepArgs a) {
             }
         }
         __syncthreads();
-        stage2_gen<D, Real, NB>(m, sm, nb, t);
+        stage2_gen<D, Real, NB>(m, sm, nb, t, a.ds.err);
         __syncthreads();
         if (!has_item) continue;
         // stage 3: reconstruction, face values, raw face moments
@@ -310,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a_gen(const StepArgs a) {
                     if (pt == DUGKS_PATCH_MIXED) {
                         for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
                     } else {
-                        const int own = __ldg(m.bface_owner + v.face);
+                        const int own = chk(__ldg(m.bface_owner + v.face), 0, m.nC, a.ds.err);
                         for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * nC + own);
                     }
                     const double cx = xi[0] - bU[0], cy = xi[1] - bU[1], cz = xi[2] - bU[2];
@@ -387,6 +394,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
         pt = __ldg(m.it_meta + gi) >> 4;
         other = __ldg(m.it_other + gi);
         face = __ldg(m.it_face + gi);
+        if (kind == ITEM_TB_OWN || kind == ITEM_TB_NEI) other = chk(other, 0, m.n_items, a.ds.err);
+        if (kind == ITEM_MESH_BOUNDARY) face = chk(face, 0, m.nBF, a.ds.err);
 #pragma unroll
         for (int q = 0; q < 3; ++q) S[q] = __ldg(m.it_geo + q * nI + gi);
     }
@@ -401,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
 #pragma unroll
     for (int s = 0; s < kRegFaces; ++s) {
         const int e = (has_cell && s < m.nf_max) ? __ldg(m.cf_item + static_cast<size_t>(s) * nC + c) : 0;
-        ent_off[s] = e == 0 ? kSI - 1 : (e > 0 ? e : -e) - 1;
+        ent_off[s] = e == 0 ? kSI - 1 : chk((e > 0 ? e : -e) - 1, 0, t.nit, a.ds.err);
         ent_neg[s] = e < 0 ? 1u : 0u;
     }
     if (threadIdx.x == kThreads - 1)
@@ -460,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
                     if (pt == DUGKS_PATCH_MAXWELL_WALL || pt == DUGKS_PATCH_MIXED) {
                         for (int i = 0; i < 3; ++i) bU[i] = __ldg(&br->U[i]);
                     } else {
-                        const int own = __ldg(m.bface_owner + face);
+                        const int own = chk(__ldg(m.bface_owner + face), 0, m.nC, a.ds.err);
                         for (int i = 0; i < 3; ++i) bU[i] = __ldg(a.ds.cellrec + (REC_UX + i) * nC + own);
                     }
                     const double cx = xi[0] - bU[0], cy = xi[1] - bU[1], cz = xi[2] - bU[2];
@@ -494,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b_gen(const StepArgs a) {
                 for (int s = kRegFaces; s < m.nf_max; ++s) {
                     const int e = __ldg(m.cf_item + static_cast<size_t>(s) * nC + c);
                     if (e != 0) {
-                        const int i = (e > 0 ? e : -e) - 1;
+                        const int i = chk((e > 0 ? e : -e) - 1, 0, t.nit, a.ds.err);
                         sg += e > 0 ? Fg[i] : -Fg[i];
                         sh += e > 0 ? Fh[i] : -Fh[i];
                     }

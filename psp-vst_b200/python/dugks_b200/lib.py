@@ -15,6 +15,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libdugks_b200.so"))
+# the bounds-checked build of the same sources (-DDUGKS_CHECK): indices read
+# from device tables are range-checked, a bad one returns DUGKS_ERR_ARG
+CHECK_LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libdugks_b200_check.so"))
 
 FP64 = 0
 FP32C = 1
@@ -226,8 +229,10 @@ class Solver:
     """fvDVM-shaped wrapper over one dugks_handle."""
 
     def __init__(self, case, precision: int = FP64, ls_weighting: int = LS_MAGSF, device: int = 0,
-                 tile_cells: int = 0, dv_chunks: int = 0, shard: Shard | None = None, macro_flux: bool | None = None):
-        self.lib = load()
+                 tile_cells: int = 0, dv_chunks: int = 0, shard: Shard | None = None, macro_flux: bool | None = None,
+                 lib_path: str | None = None):
+        # lib_path: another build of the library, e.g. CHECK_LIB_PATH
+        self.lib = load(lib_path)
         self.case = case
         fc = case.flat
         self._keep = []

@@ -1,0 +1,63 @@
+"""The bounds-checked build (libdugks_b200_check.so, -DDUGKS_CHECK) on small
+cases.
+
+Every index the kernels read from a device table (tile cells, gradient
+stencils, item sides, flux lists, boundary owners, the items of a face) is
+range-checked there; one out of range would set an error flag, be replaced
+by a safe index and make the call return DUGKS_ERR_ARG.  On these cases no
+check may fire, and the checked build must give bit for bit what the normal
+build gives (the checks only read).  Nothing here plants a bad index on the
+device: the host validates the mesh before building the tables
+(tests/test_failures.py)."""
+import os
+
+import numpy as np
+import pytest
+
+import golden_cases
+from dugks_b200 import case as cs
+from dugks_b200 import lib as dl
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(case, steps, **kw):
+    assert os.path.exists(dl.CHECK_LIB_PATH), "build the checked library (make -C psp-vst_b200/csrc)"
+    a = dl.Solver(case, **kw)
+    b = dl.Solver(case, lib_path=dl.CHECK_LIB_PATH, **kw)
+    a.step(steps, case.dt)
+    b.step(steps, case.dt)   # raises DugksError if a check fired
+    ma, mb = a.macros(), b.macros()
+    for k in ("rho", "U", "T", "q"):
+        assert np.array_equal(ma[k], mb[k]), k
+    ga, ha = a.state()
+    gb, hb = b.state()
+    assert np.array_equal(ga, gb) and np.array_equal(ha, hb)
+
+
+def test_checked_cavity8():
+    _same(cs.cavity_case(8, 8), 5)
+
+
+def test_checked_cavity_small_tiles_many_chunks():
+    _same(cs.cavity_case(12, 10), 4, tile_cells=7, dv_chunks=9)
+
+
+def test_checked_ball_far_field():
+    _same(cs.ball_case(4, 4, 1.12, 8, kn=0.1, mach=0.5), 3)
+
+
+def test_checked_demo_cavity():
+    _same(golden_cases.demo_cavity(), 2)
+
+
+def test_checked_boundary_types_and_fp32c():
+    P1 = cs.R_DEMO * 273.0    # pressure of argon at rho 1, T 273
+    sides = {"inlet": {"kind": "pressureIn", "p": 1.2 * P1, "T": 273.0},
+             "outlet": {"kind": "pressureOut", "p": P1, "T": 273.0},
+             "bottom": {"kind": "symmetryPlane"}, "top": {"kind": "zeroGradient"}}
+    c = cs.channel_case(12, 6, 8, sides=sides, flatten=False)
+    c.rho0 = np.full(c.n_cells, 1.0)
+    c.flatten()
+    _same(c, 3)
+    _same(c, 3, precision=dl.FP32C)
