@@ -64,6 +64,7 @@ dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
     a.chunks = h->chunks;
     a.chunk_begin = h->d_chunk_begin;
     dugks::pass_config(h->D, h->precision, h->n1d, &a);
+    a.hzero = h->h_zero ? 1 : 0;
     return a;
 }
 
@@ -512,6 +513,10 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     ds.fvg = p;
     if ((st = dev_alloc(h, &p, nfv * rs))) return *out = h, st;
     ds.fvh = p;
+    // face values start at zero: with h identically zero no pass writes fvh,
+    // and the symmetry pass reads its boundary slots
+    if (cudaMemset(ds.fvg, 0, nfv * rs) != cudaSuccess || cudaMemset(ds.fvh, 0, nfv * rs) != cudaSuccess)
+        return fail(DUGKS_ERR_CUDA, "cudaMemset of the face values");
     ds.cur = 0;
     if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
@@ -751,6 +756,7 @@ int dugks_set_macros(dugks_handle* h, const double* rho, const double* U, const 
     h->launches += h->nBF > 0 ? 3 : 2;
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->initialised = true;
+    h->h_zero = h->D == 3 && h->gas.K_inner == 0;
     h->last_step_ms = 0;
     return DUGKS_OK;
 }
@@ -978,6 +984,7 @@ struct dugks_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<int> launches_per_pair;   // per handle
+    std::vector<char> hzero;              // per handle, as captured
     int64_t graph_kernels = 0;
     double last_ms = 0;
     std::string last_error;
@@ -1061,6 +1068,7 @@ int dugks_batch_create(dugks_handle* const* handles, int32_t n, const double* dt
         dugks_handle* h = b->hs[i];
         cudaStreamWaitEvent(h->stream, b->fork, 0);
         const int cur0 = h->ds.cur;
+        b->hzero.push_back(h->h_zero ? 1 : 0);
         for (int k = 0; k < 2 && st == DUGKS_OK; ++k) {
             const dugks::StepArgs a = make_args(h, b->dt[i], b->dt[i]);
             if (cudaMemsetAsync(h->ds.co, 0, 2 * sizeof(double), h->stream) != cudaSuccess) st = DUGKS_ERR_CUDA;
@@ -1089,6 +1097,9 @@ int dugks_batch_step(dugks_batch* b, int32_t n_steps) {
     cudaError_t e = cudaSetDevice(b->device);
     if (e != cudaSuccess) return batch_fail(b, DUGKS_ERR_CUDA, cudaGetErrorString(e));
     const int pairs = n_steps / 2;
+    for (size_t i = 0; i < b->hs.size(); ++i)
+        if ((b->hs[i]->h_zero ? 1 : 0) != b->hzero[i])
+            return batch_fail(b, DUGKS_ERR_STATE, "dugks_batch_step: a handle's state was replaced since the batch was built");
     // handles' own queued work comes first
     for (dugks_handle* h : b->hs) {
         if ((e = cudaEventRecord(h->ev0, h->stream)) != cudaSuccess ||
@@ -1366,6 +1377,11 @@ int dugks_set_state(dugks_handle* h, const double* g, const double* hh, double d
     int st = state_io(h, nullptr, nullptr, g, hh, false);
     if (st) return st;
     if (!(dt_prev > 0)) return set_error(h, DUGKS_ERR_ARG, "dugks_set_state: dt_prev must be > 0");
+    // a nonzero h~ ends the g-only passes for this handle
+    if (h->h_zero) {
+        const size_t nvc = static_cast<size_t>(h->dm.nv_loc) * h->nC;
+        for (size_t i = 0; i < nvc && h->h_zero; ++i) h->h_zero = hh[i] == 0.0;
+    }
     dugks::StepArgs a = make_args(h, dt_prev, 0.0);
     a.dm.macro_flux = 0;   // the macros of given DFs are their moments (macroFlux yes: restore the step record)
     // a new state replaces a poisoned one: its own check starts clear

@@ -219,6 +219,10 @@ struct dugks_handle {
     double* d_hist = nullptr;       // time steps of the last adaptive call
     int32_t hist_cap = 0;
     bool initialised = false;
+    // h~ is identically zero: D = 3 and KInner = 0 make K + 3 - D = 0 in
+    // every formula that feeds h (initial state, equilibria, boundary
+    // DFs), so h stays zero unless dugks_set_state loads a nonzero h~
+    bool h_zero = false;
     double cellrec_dt = 0;          // time step the cell records' relax factors were built for
     long steps_done = 0;
     int64_t launches = 0;           // kernels launched by this handle

@@ -18,6 +18,9 @@ struct StepArgs {
     const double* dtp;
     const double* dtnp;
     int wideA, wideB;            // batch width of each pass: 1 wide, 0 narrow
+    // 1: h is identically zero (3-D, KInner = 0, h~ = 0 in the state): the
+    // tensor-DV passes carry g alone
+    int hzero;
     int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
 };

@@ -179,16 +179,21 @@ struct RowSums {
 
 __device__ __forceinline__ void row_zero(RowSums& r) { r.S0 = r.S1 = r.S2 = r.S3 = r.B0 = r.B1 = r.O = 0.0; }
 
+// HZ: h is identically zero (D = 3, KInner = 0); its sums stay zero
+template <bool HZ = false>
 __device__ __forceinline__ double row_add(RowSums& r, double wx, double x, double g, double h) {
-    const double a = wx * g, b = wx * h;
+    const double a = wx * g;
     r.S0 += a;
     const double ax = a * x;
     r.S1 += ax;
     const double ax2 = ax * x;
     r.S2 += ax2;
     r.S3 = fma(ax2, x, r.S3);
-    r.B0 += b;
-    r.B1 = fma(b, x, r.B1);
+    if constexpr (!HZ) {
+        const double b = wx * h;
+        r.B0 += b;
+        r.B1 = fma(b, x, r.B1);
+    }
     return a;
 }
 
@@ -430,28 +435,30 @@ __device__ __forceinline__ Item load_item(const DevMesh& m, int gi) {
 
 // reconstruction at the half step from local L0 cell l (fvDVM.C:832-836):
 // gbar+_l + grad_l . v,  v = Cf - C_l - xi dt/2
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool HZ = false>
 __device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l, Real vx, Real vy, Real vz, Real& g,
                                       Real& h) {
     const Real* Gg = sm.Gg + j * D * kS0 + l;
-    const Real* Gh = sm.Gh + j * D * kS0 + l;
     Real gg = fma(Gg[0], vx, sm.gB[j * kSL + l]);
-    Real hh = fma(Gh[0], vx, sm.hB[j * kSL + l]);
     gg = fma(Gg[kS0], vy, gg);
-    hh = fma(Gh[kS0], vy, hh);
-    if (D == 3) {
-        gg = fma(Gg[2 * kS0], vz, gg);
-        hh = fma(Gh[2 * kS0], vz, hh);
-    }
+    if (D == 3) gg = fma(Gg[2 * kS0], vz, gg);
     g = gg;
-    h = hh;
+    if constexpr (HZ) {
+        h = Real(0);
+    } else {
+        const Real* Gh = sm.Gh + j * D * kS0 + l;
+        Real hh = fma(Gh[0], vx, sm.hB[j * kSL + l]);
+        hh = fma(Gh[kS0], vy, hh);
+        if (D == 3) hh = fma(Gh[2 * kS0], vz, hh);
+        h = hh;
+    }
 }
 
 // ---------------------------------------------------------------------
 // Pass A stages
 // ---------------------------------------------------------------------
 // cp.async of batch bp's inputs of local cell l (thread part `part` of it)
-template <int D, typename Real, int NB, bool FULL>
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
                                        const Real* __restrict__ g, const Real* __restrict__ h,
                                        const double* __restrict__ ctab, int l, int part, int c, bool active,
@@ -466,7 +473,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
             const int j = part * H + jj;
             if (FULL || j < bp.nb) {
                 cp_async(sg + j * kSL + l, g + static_cast<size_t>(bp.d0 + j) * nC + c);
-                cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
+                if (!HZ) cp_async(sg + (NB + j) * kSL + l, h + static_cast<size_t>(bp.d0 + j) * nC + c);
                 if (!ex_res) cp_async(sx + j * kSL + l, ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
             }
         }
@@ -475,7 +482,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
     cp_commit();
 }
 
-template <int D, typename Real, int NB, bool FULL>
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
                                        int l, int part, bool active, double K3D, double c0h, bool ex_res,
                                        const double* gref, const double* href) {
@@ -503,43 +510,46 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
         if (FULL || j < bp.nb) {
             double go, ho;
             const double gr = dv_ref<Real>(gref, bp.d0 + j), hr = dv_ref<Real>(href, bp.d0 + j);
+            const double hin = HZ ? 0.0 : plus_ref<Real>(double(sg[(NB + j) * kSL + l]), hr);
             shk_relax<D, double>(s, sm.x1[bp.ix0 + j], sx[j * kSL + l], plus_ref<Real>(double(sg[j * kSL + l]), gr),
-                                 plus_ref<Real>(double(sg[(NB + j) * kSL + l]), hr), K3D, c0h, go, ho);
+                                 hin, K3D, c0h, go, ho);
             sm.gB[j * kSL + l] = Real(minus_ref<Real>(go, gr));
-            sm.hB[j * kSL + l] = Real(minus_ref<Real>(ho, hr));
+            if (!HZ) sm.hB[j * kSL + l] = Real(minus_ref<Real>(ho, hr));
         }
     }
 }
 
 
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool HZ>
 __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, int l, const int* nbi,
                                          const Real (*ls)[D], int nk) {
     const Real* gB = sm.gB + j * kSL;
     const Real* hB = sm.hB + j * kSL;
-    const Real g0 = gB[l], h0 = hB[l];
+    const Real g0 = gB[l], h0 = HZ ? Real(0) : hB[l];
     Real gx[D], hx[D];
 #pragma unroll
     for (int q = 0; q < D; ++q) gx[q] = hx[q] = Real(0);
 #pragma unroll
     for (int k = 0; k < kMaxRegStencil; ++k) {
         if (k < nk) {
-            const Real dg = gB[nbi[k]] - g0, dh = hB[nbi[k]] - h0;
+            const Real dg = gB[nbi[k]] - g0;
 #pragma unroll
-            for (int q = 0; q < D; ++q) {
-                gx[q] = fma(ls[k][q], dg, gx[q]);
-                hx[q] = fma(ls[k][q], dh, hx[q]);
+            for (int q = 0; q < D; ++q) gx[q] = fma(ls[k][q], dg, gx[q]);
+            if constexpr (!HZ) {
+                const Real dh = hB[nbi[k]] - h0;
+#pragma unroll
+                for (int q = 0; q < D; ++q) hx[q] = fma(ls[k][q], dh, hx[q]);
             }
         }
     }
 #pragma unroll
     for (int q = 0; q < D; ++q) {
         sm.Gg[(j * D + q) * kS0 + l] = gx[q];
-        sm.Gh[(j * D + q) * kS0 + l] = hx[q];
+        if (!HZ) sm.Gh[(j * D + q) * kS0 + l] = hx[q];
     }
 }
 
-template <int D, typename Real, int NB, bool FULL>
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB>& sm, const BatchPos& bp,
                                        const TileRange& t, int* err) {
     const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
@@ -560,7 +570,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
 #pragma unroll
         for (int jj = 0; jj < H; ++jj) {
             const int j = part + kParts0 * jj;
-            if (FULL || j < bp.nb) grad_one<D, Real, NB>(sm, j, l, nbi, ls, kMaxRegStencil);
+            if (FULL || j < bp.nb) grad_one<D, Real, NB, HZ>(sm, j, l, nbi, ls, kMaxRegStencil);
         }
     } else {
 #pragma unroll 1
@@ -569,7 +579,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
             if (!FULL && j >= bp.nb) break;
             const Real* gB = sm.gB + j * kSL;
             const Real* hB = sm.hB + j * kSL;
-            const Real g0 = gB[l], h0 = hB[l];
+            const Real g0 = gB[l], h0 = HZ ? Real(0) : hB[l];
             Real gx[D], hx[D];
 #pragma unroll
             for (int q = 0; q < D; ++q) gx[q] = hx[q] = Real(0);
@@ -577,7 +587,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
                 const int n0 = __ldg(m.grad_nb + static_cast<size_t>(k) * m.nC + c);
                 if (n0 < 0) continue;
                 const int n = chk(n0, 0, t.nloc, err);
-                const Real dg = gB[n] - g0, dh = hB[n] - h0;
+                const Real dg = gB[n] - g0, dh = HZ ? Real(0) : hB[n] - h0;
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
                     const Real lsq = Real(__ldg(m.grad_ls + (static_cast<size_t>(k) * 3 + q) * m.nC + c));
@@ -588,7 +598,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
 #pragma unroll
             for (int q = 0; q < D; ++q) {
                 sm.Gg[(j * D + q) * kS0 + l] = gx[q];
-                sm.Gh[(j * D + q) * kS0 + l] = hx[q];
+                if (!HZ) sm.Gh[(j * D + q) * kS0 + l] = hx[q];
             }
         }
     }
@@ -597,7 +607,10 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
 // ---------------------------------------------------------------------
 // Pass A: face reconstruction, raw face moments, face values
 // ---------------------------------------------------------------------
-template <int D, typename Real, int NB, bool FULL>
+// HZ: h is identically zero (D = 3 and KInner = 0 make K + 3 - D = 0 in
+// every h formula, fvDVM.C:414-426, :673-679, :1079-1092): the pass reads,
+// reconstructs and writes g alone; its results are those of the full pass
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -667,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
-    if (nbt > 0) stage0<D, Real, NB, FULL>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
+    if (nbt > 0) stage0<D, Real, NB, FULL, HZ>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const int buf = k & 1;
         const BatchPos bp = walk.pos();
@@ -675,12 +688,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         __syncthreads();  // batch k staged; the previous batch's stage 3 is done
         if (k + 1 < nbt) {
             ahead.next();
-            stage0<D, Real, NB, FULL>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
+            stage0<D, Real, NB, FULL, HZ>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
         }
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
-        stage1<D, Real, NB, FULL>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href);
+        stage1<D, Real, NB, FULL, HZ>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href);
         __syncthreads();
-        stage2<D, Real, NB, FULL>(m, sm, bp, t, a.ds.err);
+        stage2<D, Real, NB, FULL, HZ>(m, sm, bp, t, a.ds.err);
         __syncthreads();
         if (!has_item) continue;
         // stage 3
@@ -702,20 +715,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     const Real hx = hdt * Real(x);
                     Real gg, hh;
                     if (own_up || nei_up) {
-                        recon<D, Real, NB>(sm, j, own_up ? v.la : v.lb, Real(own_up ? v.da[0] : v.db[0]) - hx,
-                                           own_up ? ay : by, own_up ? az : bz, gg, hh);
+                        recon<D, Real, NB, HZ>(sm, j, own_up ? v.la : v.lb, Real(own_up ? v.da[0] : v.db[0]) - hx,
+                                               own_up ? ay : by, own_up ? az : bz, gg, hh);
                     } else {
                         // exactly tangential: both sides averaged (fvDVM.C:847-863)
                         Real g1, h1, g2, h2;
-                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hx, ay, az, g1, h1);
-                        recon<D, Real, NB>(sm, j, v.lb, Real(v.db[0]) - hx, by, bz, g2, h2);
+                        recon<D, Real, NB, HZ>(sm, j, v.la, Real(v.da[0]) - hx, ay, az, g1, h1);
+                        recon<D, Real, NB, HZ>(sm, j, v.lb, Real(v.db[0]) - hx, by, bz, g2, h2);
                         gg = Real(0.5) * (g2 + g1);
                         hh = Real(0.5) * (h2 + h1);
                     }
                     // FP32 storage: the deviations only; the reference part is added once below
-                    row_add(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
+                    row_add<HZ>(rs, sm.w1[bp.ix0 + j], x, double(gg), double(hh));
                     fg[j * nI] = gg;
-                    fh[j * nI] = hh;
+                    if (!HZ) fh[j * nI] = hh;
                 }
             }
         } else if (v.kind != ITEM_MESH_BOUNDARY) {
@@ -739,15 +752,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     if (up || tang) {
                         const Real cs = up ? Real(1) : Real(0.5);
                         Real gg, hh;
-                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                        recon<D, Real, NB, HZ>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         gg *= cs;
                         hh *= cs;
                         // this side's share of the face value and of its reference part
                         const double gr = double(cs) * dv_ref<Real>(m.gref, bp.d0 + j);
                         const double hr = double(cs) * dv_ref<Real>(m.href, bp.d0 + j);
-                        row_add(rs, sm.w1[bp.ix0 + j], x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
+                        row_add<HZ>(rs, sm.w1[bp.ix0 + j], x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
-                        fh[j * nI] = hh;
+                        if (!HZ) fh[j * nI] = hh;
                     }
                 }
             }
@@ -789,19 +802,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         if (zero_grad) {
                             // every DV: the owner cell's gbar+ (fvDVM.C:887-891)
                             gg = sm.gB[j * kSL + v.la];
-                            hh = sm.hB[j * kSL + v.la];
+                            hh = HZ ? Real(0) : sm.hB[j * kSL + v.la];
                         } else if (xs > -kVSmall) {
                             // outgoing and tangential: upwind from the owner
                             // (fvDVM.C:1013-1023); incoming ones are the mirror
                             // DVs' values, added by the symmetry pass after this one
-                            recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                            recon<D, Real, NB, HZ>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         } else {
                             continue;
                         }
                         const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
-                        row_add(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
+                        row_add<HZ>(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
-                        fh[j * nI] = hh;
+                        if (!HZ) fh[j * nI] = hh;
                     }
                 }
             } else
@@ -815,17 +828,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                     if (xs > 0) {
                         // outgoing: upwind from the owner (fvDVM.C:916-923, :950-961)
                         Real gg, hh;
-                        recon<D, Real, NB>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
+                        recon<D, Real, NB, HZ>(sm, j, v.la, Real(v.da[0]) - hdt * Real(x), ay, az, gg, hh);
                         const double aw =
-                            row_add(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
+                            row_add<HZ>(rs, wx, x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         if (wall) rs.O = fma(aw, xs, rs.O);
                         fg[j * nI] = gg;
-                        fh[j * nI] = hh;
+                        if (!HZ) fh[j * nI] = hh;
                     } else if (eq_in) {
                         const double cx = x - bU[0];
                         const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
                         // rounded as pass B rounds the same incoming DF
-                        row_add(rs, wx, x, plus_ref<Real>(double(Real(minus_ref<Real>(ge, gr))), gr),
+                        row_add<HZ>(rs, wx, x, plus_ref<Real>(double(Real(minus_ref<Real>(ge, gr))), gr),
                                 plus_ref<Real>(double(Real(minus_ref<Real>(ge * bHf, hr))), hr));
                     }
                     // incoming wall DFs enter through rho_w in the face combine
@@ -875,7 +888,7 @@ struct SlotPick {
 
 // cp.async of an item's face values and Maxwellian x factors for a batch
 // (each thread stages and later reads only its own item's entries)
-template <int D, typename Real, int NB, bool FULL>
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
                                             const Real* __restrict__ fvh, const double* __restrict__ ftab,
                                             const double* __restrict__ X1, size_t nI, int it, int gi,
@@ -897,7 +910,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
             }
             const size_t at = static_cast<size_t>(bp.d0 + j) * nI + src;
             cp_async(sm.st + j * kSI + it, fvg + at);
-            cp_async(sm.st + (NB + j) * kSI + it, fvh + at);
+            if (!HZ) cp_async(sm.st + (NB + j) * kSI + it, fvh + at);
             cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
         }
     }
@@ -906,7 +919,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const Bat
 
 // the L0 cell's g~, h~ and Maxwellian x factors of its DVs of a batch, into
 // registers one batch ahead
-template <typename Real, int NB, bool FULL>
+template <typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __restrict__ g, const Real* __restrict__ h,
                                             const double* __restrict__ ctab, size_t nC, int c, int part, Real* pg,
                                             Real* ph, double* pe) {
@@ -917,13 +930,14 @@ __device__ __forceinline__ void fetch_cells(const BatchPos& bp, const Real* __re
         if (FULL || j < bp.nb) {
             const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
             pg[jj] = __ldg(g + idx);
-            ph[jj] = __ldg(h + idx);
+            ph[jj] = HZ ? Real(0) : __ldg(h + idx);
             pe[jj] = __ldg(ctab + static_cast<size_t>(bp.ix0 + j) * nC + c);
         }
     }
 }
 
-template <int D, typename Real, int NB, bool FULL>
+// HZ: as for pass A, g alone (h stays identically zero)
+template <int D, typename Real, int NB, bool FULL, bool HZ>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -990,8 +1004,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
-        if (has_item) stage_items<D, Real, NB, FULL>(sm, walk.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
-        if (has_cell) fetch_cells<Real, NB, FULL>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
+        if (has_item) stage_items<D, Real, NB, FULL, HZ>(sm, walk.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
+        if (has_cell) fetch_cells<Real, NB, FULL, HZ>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
     }
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const BatchPos bp = walk.pos();
@@ -1019,11 +1033,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     if (FULL || j < bp.nb) {
                         const double x = sm.x1[bp.ix0 + j];
                         const double xs = xs_row(x, S[0], p2, p3);
-                        Real rg = sg[j * kSI], rh = sg[(NB + j) * kSI];
+                        Real rg = sg[j * kSI], rh = HZ ? Real(0) : sg[(NB + j) * kSI];
                         if (tb && !(xs >= kVSmall) && !(xs < -kVSmall)) {
                             const size_t o = static_cast<size_t>(bp.d0 + j) * nI + other;
                             rg += __ldg(fvg + o);
-                            rh += __ldg(fvh + o);
+                            if (!HZ) rh += __ldg(fvh + o);
                         }
                         const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                         double gf, hf;
@@ -1031,7 +1045,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                                              plus_ref<Real>(double(rh), hr), K3D, c0h, gf, hf);
                         // the reference part of the fluxes cancels over a closed cell (sum of +-Sf = 0)
                         sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
-                        sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
+                        if (!HZ) sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                     }
                 }
             } else {
@@ -1074,7 +1088,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                             shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                             sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
-                            sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
+                            if (!HZ) sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                         }
                     }
                 } else
@@ -1098,12 +1112,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             hf = plus_ref<Real>(double(Real(minus_ref<Real>(ge * bHf, hr))), hr);
                         }
                         sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
-                        sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
+                        if (!HZ) sm.Fh[j * kSI + it] = Real(xs * minus_ref<Real>(hf, hr));
                     }
                 }
             }
             // this thread has read its staged entries: stage the next batch
-            if (k + 1 < nbt) stage_items<D, Real, NB, FULL>(sm, ahead.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
+            if (k + 1 < nbt) stage_items<D, Real, NB, FULL, HZ>(sm, ahead.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
         }
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
@@ -1129,14 +1143,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
 #pragma unroll
                     for (int s = 0; s < kRegFaces; ++s) {
                         sg += flip_sign(Fg[ent_off[s]], ent_neg[s]);
-                        sh += flip_sign(Fh[ent_off[s]], ent_neg[s]);
+                        if (!HZ) sh += flip_sign(Fh[ent_off[s]], ent_neg[s]);
                     }
                     for (int s = kRegFaces; s < m.nf_max; ++s) {
                         const int e = __ldg(m.cf_item + static_cast<size_t>(s) * nC + c);
                         if (e != 0) {
                             const int i = chk((e > 0 ? e : -e) - 1, 0, t.nit, a.ds.err);
                             sg += e > 0 ? Fg[i] : -Fg[i];
-                            sh += e > 0 ? Fh[i] : -Fh[i];
+                            if (!HZ) sh += e > 0 ? Fh[i] : -Fh[i];
                         }
                     }
                     // the update in FP64, one rounding to the storage type; with a
@@ -1147,13 +1161,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                         Real(fma(-1.0 / 3, double(ht), fma(4.0 / 3, minus_ref<Real>(hb, hr), double(sh) * dtV)));
                     const size_t idx = static_cast<size_t>(bp.d0 + j) * nC + c;
                     gn[idx] = g_new;
-                    hn[idx] = h_new;
-                    row_add(rs, sm.w1[bp.ix0 + j], x, double(g_new), double(h_new));  // reference part below
+                    if (!HZ) hn[idx] = h_new;
+                    row_add<HZ>(rs, sm.w1[bp.ix0 + j], x, double(g_new), double(h_new));  // reference part below
                 }
             }
             row_fold<D>(acc, rs, q);
             // the next batch's cell inputs fly during the barrier and stage 3
-            if (k + 1 < nbt) fetch_cells<Real, NB, FULL>(ahead.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
+            if (k + 1 < nbt) fetch_cells<Real, NB, FULL, HZ>(ahead.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
         }
     }
     // the cell moments of a cell are split over kParts0 threads: reduce them
@@ -1199,17 +1213,26 @@ cudaError_t configure_gen(const StepArgs& a) {
     cudaError_t e = set_smem(k_pass_a_gen<D, Real, kNbGen>, a.smemA);
     return e != cudaSuccess ? e : set_smem(k_pass_b_gen<D, Real, kNbGen>, a.smemB);
 }
-template <int D, typename Real, int NA, int NBB>
-cudaError_t launch_nb(const StepArgs& a, bool pass_b, cudaStream_t s) {
+template <int D, typename Real, int NA, int NBB, bool HZ>
+cudaError_t launch_nb_h(const StepArgs& a, bool pass_b, cudaStream_t s) {
     const dim3 grid(a.dm.n_tiles, a.chunks);
     if (!pass_b) {
-        if (a.fullA) k_pass_a<D, Real, NA, true><<<grid, kThreads, a.smemA, s>>>(a);
-        else k_pass_a<D, Real, NA, false><<<grid, kThreads, a.smemA, s>>>(a);
+        if (a.fullA) k_pass_a<D, Real, NA, true, HZ><<<grid, kThreads, a.smemA, s>>>(a);
+        else k_pass_a<D, Real, NA, false, HZ><<<grid, kThreads, a.smemA, s>>>(a);
     } else {
-        if (a.fullB) k_pass_b<D, Real, NBB, true><<<grid, kThreads, a.smemB, s>>>(a);
-        else k_pass_b<D, Real, NBB, false><<<grid, kThreads, a.smemB, s>>>(a);
+        if (a.fullB) k_pass_b<D, Real, NBB, true, HZ><<<grid, kThreads, a.smemB, s>>>(a);
+        else k_pass_b<D, Real, NBB, false, HZ><<<grid, kThreads, a.smemB, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+// h identically zero (StepArgs::hzero) exists in 3-D only
+template <int D, typename Real, int NA, int NBB>
+cudaError_t launch_nb(const StepArgs& a, bool pass_b, cudaStream_t s) {
+    if constexpr (D == 3) {
+        if (a.hzero) return launch_nb_h<D, Real, NA, NBB, true>(a, pass_b, s);
+    }
+    return launch_nb_h<D, Real, NA, NBB, false>(a, pass_b, s);
 }
 
 template <int D, typename Real>
@@ -1230,10 +1253,22 @@ cudaError_t set_smem(K* kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 
+template <int D, typename Real, int NA, int NBB, bool HZ>
+cudaError_t configure_nb_h(const StepArgs& a, bool pass_b) {
+    if (!pass_b)
+        return a.fullA ? set_smem(k_pass_a<D, Real, NA, true, HZ>, a.smemA)
+                       : set_smem(k_pass_a<D, Real, NA, false, HZ>, a.smemA);
+    return a.fullB ? set_smem(k_pass_b<D, Real, NBB, true, HZ>, a.smemB)
+                   : set_smem(k_pass_b<D, Real, NBB, false, HZ>, a.smemB);
+}
+
 template <int D, typename Real, int NA, int NBB>
 cudaError_t configure_nb(const StepArgs& a, bool pass_b) {
-    if (!pass_b) return a.fullA ? set_smem(k_pass_a<D, Real, NA, true>, a.smemA) : set_smem(k_pass_a<D, Real, NA, false>, a.smemA);
-    return a.fullB ? set_smem(k_pass_b<D, Real, NBB, true>, a.smemB) : set_smem(k_pass_b<D, Real, NBB, false>, a.smemB);
+    cudaError_t e = configure_nb_h<D, Real, NA, NBB, false>(a, pass_b);
+    if constexpr (D == 3) {
+        if (e == cudaSuccess) e = configure_nb_h<D, Real, NA, NBB, true>(a, pass_b);
+    }
+    return e;
 }
 
 template <int D, typename Real>
