@@ -734,10 +734,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
         } else if (v.kind != ITEM_MESH_BOUNDARY) {
             // tile-boundary face: this tile's side only, weighted 1 upwind,
             // 1/2 tangential, 0 downwind; the other tile adds its side.  The
-            // face value is written once, into the upwind side's slot (pass
-            // B of the downwind tile reads it there); tangential halves stay
-            // in their own slots
+            // upwind tile writes the face value into both items' slots, so
+            // that each tile's pass B reads its own slot, coalesced (reading
+            // the other tile's slot instead cost pass B more than the
+            // second store costs here); tangential halves stay in their own
+            // slots
             const bool own_side = v.kind == ITEM_TB_OWN;
+            Real* og = fvg + static_cast<size_t>(bp.d0) * nI + v.other;
+            Real* oh = fvh + static_cast<size_t>(bp.d0) * nI + v.other;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 if (FULL || j < bp.nb) {
@@ -761,6 +765,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
                         row_add<HZ>(rs, sm.w1[bp.ix0 + j], x, plus_ref<Real>(double(gg), gr), plus_ref<Real>(double(hh), hr));
                         fg[j * nI] = gg;
                         if (!HZ) fh[j * nI] = hh;
+                        if (up) {
+                            og[j * nI] = gg;
+                            if (!HZ) oh[j * nI] = hh;
+                        }
                     }
                 }
             }
@@ -877,40 +885,19 @@ __device__ __forceinline__ float flip_sign(float v, unsigned neg) {
     return __int_as_float(__float_as_int(v) ^ static_cast<int>(neg << 31));
 }
 
-// Where an item reads its face value from: its own slot, or, on a
-// tile-boundary face whose other side is upwind, the other side's slot
-// (pass A writes each upwind value once)
-struct SlotPick {
-    int other;          // the other side's item, -1: always the own slot
-    bool own_side;      // this side is the face's owner
-    double Sx, Sy, Sz;  // area vector
-};
-
-// cp.async of an item's face values and Maxwellian x factors for a batch
-// (each thread stages and later reads only its own item's entries)
-template <int D, typename Real, int NB, bool FULL, bool HZ>
+// cp.async of an item's own face-value slot and Maxwellian x factors for a
+// batch (each thread stages and later reads only its own item's entries)
+template <typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
-                                            const Real* __restrict__ fvh, const double* __restrict__ ftab,
-                                            const double* __restrict__ X1, size_t nI, int it, int gi,
-                                            const SlotPick& sp) {
+                                            const Real* __restrict__ fvh, const double* __restrict__ ftab, size_t nI,
+                                            int it, int gi) {
+    const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
     const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
-    double p2 = 0, p3 = 0;
-    if (sp.other >= 0) {
-        p2 = __dmul_rn(__ldg(X1 + bp.iy), sp.Sy);
-        p3 = D == 3 ? __dmul_rn(__ldg(X1 + bp.iz), sp.Sz) : 0.0;
-    }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         if (FULL || j < bp.nb) {
-            int src = gi;
-            if (sp.other >= 0) {
-                // the same xi.S and thresholds as pass A's upwind choice
-                const double xs = xs_row(__ldg(X1 + bp.ix0 + j), sp.Sx, p2, p3);
-                if (sp.own_side ? xs < -kVSmall : xs >= kVSmall) src = sp.other;
-            }
-            const size_t at = static_cast<size_t>(bp.d0 + j) * nI + src;
-            cp_async(sm.st + j * kSI + it, fvg + at);
-            if (!HZ) cp_async(sm.st + (NB + j) * kSI + it, fvh + at);
+            cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
+            if (!HZ) cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
             cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
         }
     }
@@ -992,8 +979,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             sm.Fh[j * kSI + kSI - 1] = Real(0);
         }
     }
-    const bool tb_item = kind == ITEM_TB_OWN || kind == ITEM_TB_NEI;
-    const SlotPick sp{tb_item ? other : -1, kind == ITEM_TB_OWN, S[0], S[1], S[2]};
     double acc[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) acc[j] = 0.0;
@@ -1004,7 +989,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
-        if (has_item) stage_items<D, Real, NB, FULL, HZ>(sm, walk.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
+        if (has_item) stage_items<Real, NB, FULL, HZ>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
         if (has_cell) fetch_cells<Real, NB, FULL, HZ>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
     }
     for (int k = 0; k < nbt; ++k, walk.next()) {
@@ -1023,10 +1008,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             cp_wait_all();  // this item's staged entries of batch k
             const Real* sg = sm.st + it;
             if (kind != ITEM_MESH_BOUNDARY) {
-                // internal and tile-boundary faces: the staged value is the
-                // upwind face value (from the upwind side's slot); on an
-                // exactly tangential tile-boundary face it is this side's
-                // half and the other slot holds the rest
+                // internal and tile-boundary faces: the staged slot holds the
+                // upwind face value; on an exactly tangential tile-boundary
+                // face it holds this side's half and the other slot the rest
                 const bool tb = kind != ITEM_TILE_INTERNAL;
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
@@ -1117,7 +1101,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 }
             }
             // this thread has read its staged entries: stage the next batch
-            if (k + 1 < nbt) stage_items<D, Real, NB, FULL, HZ>(sm, ahead.pos(), fvg, fvh, ftab, m.X1, nI, it, gi, sp);
+            if (k + 1 < nbt) stage_items<Real, NB, FULL, HZ>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
         }
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
