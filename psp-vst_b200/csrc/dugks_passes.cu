@@ -485,7 +485,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 template <int D, typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
                                        int l, int part, bool active, double K3D, double c0h, bool ex_res,
-                                       const double* gref, const double* href) {
+                                       const double* gref, const double* href, double& ey, double& ez) {
     if (!active) return;
     Shk<double> s;
     s.Ux = sm.crec[CR_UX * kSL + l];
@@ -494,11 +494,16 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
     s.RTh = sm.crec[CR_RTH * kSL + l];
     s.omr = sm.crec[CR_OMR * kSL + l];
     // the y and z Maxwellian factors of the batch's row, as the combine
-    // kernels tabulate them (write_maxwell_tables): exp(-x^2/2 invRT)
+    // kernels tabulate them (write_maxwell_tables): exp(-x^2/2 invRT); the
+    // thread's cell is the same in every batch, so the g-only pass, which
+    // has the registers to spare, computes them on the row's first batch
+    // and keeps them for the others
     const double uy = sm.crec[CR_UY * kSL + l], uz = sm.crec[CR_UZ * kSL + l];
-    const double yy = q.Y - uy, zz = q.Z - uz;
-    const double ey = exp(-0.5 * yy * yy * s.invRT);
-    const double ez = D == 3 ? exp(-0.5 * zz * zz * s.invRT) : 1.0;
+    if (!HZ || bp.ix0 == 0) {
+        const double yy = q.Y - uy, zz = q.Z - uz;
+        ey = exp(-0.5 * yy * yy * s.invRT);
+        ez = D == 3 ? exp(-0.5 * zz * zz * s.invRT) : 1.0;
+    }
     shk_batch<D, double>(s, uy, uz, sm.crec[CR_QY * kSL + l], sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y,
                          q.Z, ey, ez);
     const Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
@@ -680,6 +685,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
 
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
+    double ey1 = 1.0, ez1 = 1.0;   // y, z Maxwellian factors of this thread's local cell and row
     if (nbt > 0) stage0<D, Real, NB, FULL, HZ>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const int buf = k & 1;
@@ -691,7 +697,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
             stage0<D, Real, NB, FULL, HZ>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
         }
         const RowConst q = row_const<D>(sm.x1, sm.w1, bp);
-        stage1<D, Real, NB, FULL, HZ>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href);
+        stage1<D, Real, NB, FULL, HZ>(sm, buf, bp, q, l1, p1, act1, K3D, c0h, ex_res, m.gref, m.href, ey1, ez1);
         __syncthreads();
         stage2<D, Real, NB, FULL, HZ>(m, sm, bp, t, a.ds.err);
         __syncthreads();
