@@ -63,8 +63,8 @@ dugks::StepArgs make_args(const dugks_handle* h, double dt, double dt_next) {
     a.dt_next = dt_next;
     a.chunks = h->chunks;
     a.chunk_begin = h->d_chunk_begin;
-    dugks::pass_config(h->D, h->precision, h->n1d, &a);
     a.hzero = h->h_zero ? 1 : 0;
+    dugks::pass_config(h->D, h->precision, h->n1d, &a);
     return a;
 }
 

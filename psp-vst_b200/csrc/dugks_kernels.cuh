@@ -21,6 +21,7 @@ struct StepArgs {
     // 1: h is identically zero (3-D, KInner = 0, h~ = 0 in the state): the
     // tensor-DV passes carry g alone
     int hzero;
+    int wideA16;                 // g-only pass A in batches of 16 DVs (16 nodes per dimension)
     int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
 };

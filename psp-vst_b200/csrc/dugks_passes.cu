@@ -268,8 +268,14 @@ __device__ __forceinline__ void shk_relax(const Shk<Real>& s, Real x, Real ex, R
 // ---------------------------------------------------------------------
 enum { CR_UX, CR_UY, CR_UZ, CR_INVRT, CR_QX, CR_QY, CR_QZ, CR_RTH, CR_OMR, CR_R, CR_N };
 
-template <int D, typename Real, int NB>
+template <int D, typename Real, int NB, bool HZ = false>
 struct SmemA {
+    // DF arrays per local cell: g~ and h~, or g~ alone when h is identically zero
+    static constexpr int NH = HZ ? 1 : 2;
+    // rows of stgx: [2][NB] staged per batch, or the resident table [n1d];
+    // the g-only 16-wide pass runs on DV sets of at most NB nodes per
+    // dimension and keeps the resident table only
+    static constexpr int XR = (HZ && NB >= 16) ? NB : 2 * NB;
     double* x1;     // [kMaxN1d] 1-D nodes
     double* w1;     // [kMaxN1d] 1-D weights
     double* crec;   // [CR_N][kSL] records of the local cells
@@ -277,40 +283,41 @@ struct SmemA {
     // dimension, the whole table [n1d][kSL] is loaded once per CTA (e_x does
     // not depend on the row); otherwise [2][NB][kSL] staged per batch
     double* stgx;
-    Real* stg;      // [2][2][NB][kSL] staged g~, h~
+    Real* stg;      // [2][NH][NB][kSL] staged g~ (and h~)
     Real* gB;       // [NB][kSL] gbar+
-    Real* hB;
+    Real* hB;       // (null when h is identically zero)
     Real* Gg;       // [NB][D][kS0] gradients of the L0 cells
-    Real* Gh;
+    Real* Gh;       // (null when h is identically zero)
     int* snb;       // [kMaxRegStencil][kS0] gradient stencils of the L0 cells: local neighbour
     Real* sls;      // [kMaxRegStencil][D][kS0] and least-squares vector
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) + static_cast<size_t>(kMaxRegStencil) * kS0 * sizeof(int) +
-               (static_cast<size_t>(CR_N) * kSL + 2 * NB * kSL) * sizeof(double) +
-               (2 * 2 * static_cast<size_t>(NB) * kSL + 2 * NB * kSL + 2 * NB * D * kS0 +
+               (static_cast<size_t>(CR_N) * kSL + static_cast<size_t>(XR) * kSL) * sizeof(double) +
+               (2 * NH * static_cast<size_t>(NB) * kSL + NH * NB * kSL + NH * NB * D * kS0 +
                 static_cast<size_t>(kMaxRegStencil) * D * kS0) *
                    sizeof(Real);
     }
 };
 
-template <int D, typename Real, int NB>
-__device__ __forceinline__ SmemA<D, Real, NB> carve_a(unsigned char* base) {
-    SmemA<D, Real, NB> s;
+template <int D, typename Real, int NB, bool HZ = false>
+__device__ __forceinline__ SmemA<D, Real, NB, HZ> carve_a(unsigned char* base) {
+    using S = SmemA<D, Real, NB, HZ>;
+    S s;
     s.x1 = reinterpret_cast<double*>(base);
     s.w1 = s.x1 + kMaxN1d;
     s.crec = s.w1 + kMaxN1d;
     s.stgx = s.crec + CR_N * kSL;
-    Real* p = reinterpret_cast<Real*>(s.stgx + 2 * NB * kSL);
+    Real* p = reinterpret_cast<Real*>(s.stgx + S::XR * kSL);
     s.stg = p;
-    p += 2 * 2 * NB * kSL;
+    p += 2 * S::NH * NB * kSL;
     s.gB = p;
     p += NB * kSL;
-    s.hB = p;
-    p += NB * kSL;
+    s.hB = HZ ? nullptr : p;
+    if (!HZ) p += NB * kSL;
     s.Gg = p;
     p += NB * D * kS0;
-    s.Gh = p;
-    p += NB * D * kS0;
+    s.Gh = HZ ? nullptr : p;
+    if (!HZ) p += NB * D * kS0;
     s.sls = p;
     p += kMaxRegStencil * D * kS0;
     s.snb = reinterpret_cast<int*>(p);
@@ -436,7 +443,7 @@ __device__ __forceinline__ Item load_item(const DevMesh& m, int gi) {
 // reconstruction at the half step from local L0 cell l (fvDVM.C:832-836):
 // gbar+_l + grad_l . v,  v = Cf - C_l - xi dt/2
 template <int D, typename Real, int NB, bool HZ = false>
-__device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l, Real vx, Real vy, Real vz, Real& g,
+__device__ __forceinline__ void recon(const SmemA<D, Real, NB, HZ>& sm, int j, int l, Real vx, Real vy, Real vz, Real& g,
                                       Real& h) {
     const Real* Gg = sm.Gg + j * D * kS0 + l;
     Real gg = fma(Gg[0], vx, sm.gB[j * kSL + l]);
@@ -459,13 +466,13 @@ __device__ __forceinline__ void recon(const SmemA<D, Real, NB>& sm, int j, int l
 // ---------------------------------------------------------------------
 // cp.async of batch bp's inputs of local cell l (thread part `part` of it)
 template <int D, typename Real, int NB, bool FULL, bool HZ>
-__device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp,
+__device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB, HZ>& sm, int buf, const BatchPos& bp,
                                        const Real* __restrict__ g, const Real* __restrict__ h,
                                        const double* __restrict__ ctab, int l, int part, int c, bool active,
                                        bool ex_res) {
     if (active) {
         constexpr int H = NB / kPartsL;
-        Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
+        Real* sg = sm.stg + static_cast<size_t>(buf) * SmemA<D, Real, NB, HZ>::NH * NB * kSL;
         double* sx = sm.stgx + static_cast<size_t>(buf) * NB * kSL;
         const size_t nC = static_cast<size_t>(m.nC);
 #pragma unroll
@@ -483,7 +490,7 @@ __device__ __forceinline__ void stage0(const DevMesh& m, const SmemA<D, Real, NB
 }
 
 template <int D, typename Real, int NB, bool FULL, bool HZ>
-__device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, const BatchPos& bp, const RowConst& q,
+__device__ __forceinline__ void stage1(const SmemA<D, Real, NB, HZ>& sm, int buf, const BatchPos& bp, const RowConst& q,
                                        int l, int part, bool active, double K3D, double c0h, bool ex_res,
                                        const double* gref, const double* href, double& ey, double& ez) {
     if (!active) return;
@@ -506,7 +513,7 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
     }
     shk_batch<D, double>(s, uy, uz, sm.crec[CR_QY * kSL + l], sm.crec[CR_QZ * kSL + l], sm.crec[CR_R * kSL + l], q.Y,
                          q.Z, ey, ez);
-    const Real* sg = sm.stg + static_cast<size_t>(buf) * 2 * NB * kSL;
+    const Real* sg = sm.stg + static_cast<size_t>(buf) * SmemA<D, Real, NB, HZ>::NH * NB * kSL;
     const double* sx = sm.stgx + (ex_res ? bp.ix0 : buf * NB) * kSL;
     constexpr int H = NB / kPartsL;
 #pragma unroll
@@ -526,7 +533,7 @@ __device__ __forceinline__ void stage1(const SmemA<D, Real, NB>& sm, int buf, co
 
 
 template <int D, typename Real, int NB, bool HZ>
-__device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, int l, const int* nbi,
+__device__ __forceinline__ void grad_one(const SmemA<D, Real, NB, HZ>& sm, int j, int l, const int* nbi,
                                          const Real (*ls)[D], int nk) {
     const Real* gB = sm.gB + j * kSL;
     const Real* hB = sm.hB + j * kSL;
@@ -555,7 +562,7 @@ __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB>& sm, int j, in
 }
 
 template <int D, typename Real, int NB, bool FULL, bool HZ>
-__device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB>& sm, const BatchPos& bp,
+__device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB, HZ>& sm, const BatchPos& bp,
                                        const TileRange& t, int* err) {
     const int l = threadIdx.x % kS0, part = threadIdx.x / kS0;
     if (l >= t.n0) return;
@@ -619,7 +626,7 @@ template <int D, typename Real, int NB, bool FULL, bool HZ>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SmemA<D, Real, NB> sm = carve_a<D, Real, NB>(smem_raw);
+    const SmemA<D, Real, NB, HZ> sm = carve_a<D, Real, NB, HZ>(smem_raw);
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
@@ -1206,6 +1213,12 @@ cudaError_t configure_gen(const StepArgs& a) {
 template <int D, typename Real, int NA, int NBB, bool HZ>
 cudaError_t launch_nb_h(const StepArgs& a, bool pass_b, cudaStream_t s) {
     const dim3 grid(a.dm.n_tiles, a.chunks);
+    if constexpr (HZ) {
+        if (!pass_b && a.wideA16) {
+            k_pass_a<D, Real, 16, true, true><<<grid, kThreads, a.smemA, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
     if (!pass_b) {
         if (a.fullA) k_pass_a<D, Real, NA, true, HZ><<<grid, kThreads, a.smemA, s>>>(a);
         else k_pass_a<D, Real, NA, false, HZ><<<grid, kThreads, a.smemA, s>>>(a);
@@ -1257,6 +1270,8 @@ cudaError_t configure_nb(const StepArgs& a, bool pass_b) {
     cudaError_t e = configure_nb_h<D, Real, NA, NBB, false>(a, pass_b);
     if constexpr (D == 3) {
         if (e == cudaSuccess) e = configure_nb_h<D, Real, NA, NBB, true>(a, pass_b);
+        if (e == cudaSuccess && !pass_b)
+            e = set_smem(k_pass_a<D, Real, 16, true, true>, SmemA<D, Real, 16, true>::bytes());
     }
     return e;
 }
@@ -1312,6 +1327,14 @@ void pass_config(int D, int precision, int n1d, StepArgs* a) {
     } else {
         if (D == 3) smem_d<3, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
         else smem_d<2, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
+    }
+    // g-only pass A in batches of 16 DVs (a whole row) for 16 nodes per
+    // dimension: half the per-batch work and barriers per DV, and the
+    // shared memory the h arrays would take holds the wider batch
+    a->wideA16 = 0;
+    if (D == 3 && a->hzero && n1d == 16) {
+        a->wideA16 = 1;
+        a->smemA = f64 ? SmemA<3, double, 16, true>::bytes() : SmemA<3, float, 16, true>::bytes();
     }
 }
 
