@@ -56,6 +56,9 @@ def parse():
                    help="steps after which the cube sub-line compares FP32c with FP64")
     p.add_argument("--cpu-sample-ndv", type=int, default=8, help="1-D DV count of the CPU baseline sample")
     p.add_argument("--ndv1d", type=int, default=0, help="override the 1-D DV count (profiling of small cases)")
+    p.add_argument("--ball-m", type=int, default=24,
+                   help="--workload ball: cells per cube-face edge (profiling of small cases; default 24)")
+    p.add_argument("--ball-nr", type=int, default=32, help="--workload ball: radial cells (default 32)")
     p.add_argument("--cube-n", type=int, default=64, help="--workload cube: cells per side")
     p.add_argument("--kn", type=float, default=0.1, help="--workload cube: Knudsen number")
     p.add_argument("--tune", action="store_true",
@@ -74,16 +77,17 @@ def parse():
     return a
 
 
-def build_case(name, ndv1d=0, cube_n=64, kn=0.1, geometry=None):
+def build_case(name, ndv1d=0, cube_n=64, kn=0.1, geometry=None, ball_m=24, ball_nr=32):
     """The workload's case and its config description.  geometry: a
     function of the PolyMesh giving its cell and face geometry (default:
     the library's dugks_mesh_geometry; the reference arm passes the
     oracle's restatement, which gives the same numbers bit for bit)."""
     from dugks_b200 import case as cs
     if name == "ball":
-        c = cs.ball_case(24, 32, 1.12, ndv1d or 16, kn=0.1, mach=0.5, flatten=False)
-        cfg = {"workload": "ball: cubed sphere 6x24x24x32 (110592 cells), stretch 1.12, r 1..10, 16^3 GH DVs, "
-                           "far field Ma 0.5, Kn 0.1 (diameter), diffuse isothermal wall"}
+        c = cs.ball_case(ball_m, ball_nr, 1.12, ndv1d or 16, kn=0.1, mach=0.5, flatten=False)
+        cfg = {"workload": f"ball: cubed sphere 6x{ball_m}x{ball_m}x{ball_nr} ({6 * ball_m * ball_m * ball_nr} cells), "
+                           f"stretch 1.12, r 1..10, {ndv1d or 16}^3 GH DVs, far field Ma 0.5, Kn 0.1 (diameter), "
+                           "diffuse isothermal wall"}
     elif name == "cube":
         c = cs.cube_case(cube_n, ndv1d or 20, kn=kn, flatten=False)
         cfg = {"workload": f"cube: {cube_n}^3 lid-driven cube, {ndv1d or 20}^3 GH DVs, Kn {kn}, lid 50 m/s"}
@@ -116,9 +120,11 @@ def run_config(cfg, precision, world, shard, nv_loc, nc):
 
 def profiled_traffic(kernel: str, precision: str):
     """DRAM bytes per cell.DV update of a pass kernel, from the committed
-    ncu summary of the same kernel on the ball mesh (captured at 8^3 DVs;
-    traffic scales with the DV count), or None."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_ball110592_dv512_{precision}.md")
+    ncu summary of the same kernel with the same 16^3 DV set on a smaller
+    cubed sphere (6 x 16^3 = 24,576 cells; the full launch is too large to
+    capture; traffic per update is set by the tile layout, alike on both
+    meshes), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_ball24576_dv4096_{precision}.md")
     try:
         with open(path) as f:
             for ln in f:
@@ -603,7 +609,8 @@ def run_reference(args):
         return
     import oracle_bind as ob
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn, geometry=ob.geometry)
+    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn, geometry=ob.geometry,
+                           ball_m=args.ball_m, ball_nr=args.ball_nr)
     nc, nv = case.n_cells, case.n_dv
     K, W = args.steps, max(3, args.warmup)
     config = run_config(cfg, args.precision, world, args.dv_shard and world > 1, nv, nc)
@@ -674,7 +681,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     from dugks_b200 import lib as dl
-    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn)
+    case, cfg = build_case(args.workload, args.ndv1d, args.cube_n, args.kn, ball_m=args.ball_m,
+                           ball_nr=args.ball_nr)
     prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
     shard = None
     if world > 1 and args.dv_shard:
@@ -745,7 +753,8 @@ def main():
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": kbytes,
-                     "traffic_source": "ncu DRAM read+write of the same kernel at 8^3 DVs, scaled by DVs"
+                     "traffic_source": "ncu DRAM read+write per update of the same kernel on a 6x16^3 cubed "
+                                       "sphere with the same DV set, times this launch's updates"
                      if traffic is not None else None},
         "step_roofline": {"bytes_per_update": 3 * arr * rs, "h_identically_zero": arr == 1,
                           "achieved": step_bytes / (t_ms / K / 1e3) / 1e9,
@@ -776,7 +785,8 @@ def main():
         del s32
     else:
         del solver
-    if rank == 0 and world == 1 and not args.no_cube and args.workload == "ball" and not args.ndv1d:
+    default_ball = args.workload == "ball" and not args.ndv1d and args.ball_m == 24 and args.ball_nr == 32
+    if rank == 0 and world == 1 and not args.no_cube and default_ball:
         # the mixed-precision configuration itself: FP32c against FP64 on the
         # 64^3 x 20^3 cube
         line["cube"] = cube_line(steps=max(8, args.cube_steps), device=local)
