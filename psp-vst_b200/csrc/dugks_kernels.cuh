@@ -22,6 +22,7 @@ struct StepArgs {
     // tensor-DV passes carry g alone
     int hzero;
     int wideA16;                 // g-only pass A in batches of 16 DVs (16 nodes per dimension)
+    int wideB16;                 // g-only pass B likewise (FP32 storage)
     int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
 };

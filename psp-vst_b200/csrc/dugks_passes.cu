@@ -324,35 +324,38 @@ __device__ __forceinline__ SmemA<D, Real, NB, HZ> carve_a(unsigned char* base) {
     return s;
 }
 
-template <typename Real, int NB>
+template <typename Real, int NB, bool HZ = false>
 struct SmemB {
+    // DF arrays per item: g and h, or g alone when h is identically zero
+    static constexpr int NH = HZ ? 1 : 2;
     double* x1;
     double* w1;
     double* frec;  // [CR_N][kSI] face records of the items
     double* crec;  // [CR_N][kS0] records of the L0 cells
     double* stx;   // [NB][kSI] staged e_x of the items
-    Real* st;      // [2][NB][kSI] staged face values g, h of the items
+    Real* st;      // [NH][NB][kSI] staged face values g (and h) of the items
     Real* Fg;      // [NB][kSI] fluxes xi.S g_f of the items
-    Real* Fh;
+    Real* Fh;      // (null when h is identically zero)
     double* red;   // end-of-CTA reduction of the split cell moments (aliases stx and st)
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) +
                (static_cast<size_t>(CR_N) * (kSI + kS0) + static_cast<size_t>(NB) * kSI) * sizeof(double) +
-               4 * static_cast<size_t>(NB) * kSI * sizeof(Real);
+               2 * NH * static_cast<size_t>(NB) * kSI * sizeof(Real);
     }
 };
 
-template <typename Real, int NB>
-__device__ __forceinline__ SmemB<Real, NB> carve_b(unsigned char* base) {
-    SmemB<Real, NB> s;
+template <typename Real, int NB, bool HZ = false>
+__device__ __forceinline__ SmemB<Real, NB, HZ> carve_b(unsigned char* base) {
+    using S = SmemB<Real, NB, HZ>;
+    S s;
     s.x1 = reinterpret_cast<double*>(base);
     s.w1 = s.x1 + kMaxN1d;
     s.frec = s.w1 + kMaxN1d;
     s.crec = s.frec + CR_N * kSI;
     s.stx = s.crec + CR_N * kS0;
     s.st = reinterpret_cast<Real*>(s.stx + NB * kSI);
-    s.Fg = s.st + 2 * NB * kSI;
-    s.Fh = s.Fg + NB * kSI;
+    s.Fg = s.st + S::NH * NB * kSI;
+    s.Fh = HZ ? nullptr : s.Fg + NB * kSI;
     s.red = s.stx;
     return s;
 }
@@ -901,7 +904,7 @@ __device__ __forceinline__ float flip_sign(float v, unsigned neg) {
 // cp.async of an item's own face-value slot and Maxwellian x factors for a
 // batch (each thread stages and later reads only its own item's entries)
 template <typename Real, int NB, bool FULL, bool HZ>
-__device__ __forceinline__ void stage_items(const SmemB<Real, NB>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
+__device__ __forceinline__ void stage_items(const SmemB<Real, NB, HZ>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
                                             const Real* __restrict__ fvh, const double* __restrict__ ftab, size_t nI,
                                             int it, int gi) {
     const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
@@ -941,7 +944,7 @@ template <int D, typename Real, int NB, bool FULL, bool HZ>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SmemB<Real, NB> sm = carve_b<Real, NB>(smem_raw);
+    const SmemB<Real, NB, HZ> sm = carve_b<Real, NB, HZ>(smem_raw);
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
@@ -989,7 +992,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     if (threadIdx.x == kThreads - 1) {
         for (int j = 0; j < NB; ++j) {
             sm.Fg[j * kSI + kSI - 1] = Real(0);
-            sm.Fh[j * kSI + kSI - 1] = Real(0);
+            if (!HZ) sm.Fh[j * kSI + kSI - 1] = Real(0);
         }
     }
     double acc[15];
@@ -1135,7 +1138,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                     shk_relax<D, double>(cs, x, pe[jj], plus_ref<Real>(double(gt), gr), plus_ref<Real>(double(ht), hr),
                                          K3D, c0h, gb, hb);
                     const Real* Fg = sm.Fg + j * kSI;
-                    const Real* Fh = sm.Fh + j * kSI;
+                    const Real* Fh = HZ ? nullptr : sm.Fh + j * kSI;
                     Real sg = 0, sh = 0;
 #pragma unroll
                     for (int s = 0; s < kRegFaces; ++s) {
@@ -1218,6 +1221,12 @@ cudaError_t launch_nb_h(const StepArgs& a, bool pass_b, cudaStream_t s) {
             k_pass_a<D, Real, 16, true, true><<<grid, kThreads, a.smemA, s>>>(a);
             return cudaGetLastError();
         }
+        if constexpr (sizeof(Real) == 4) {
+            if (pass_b && a.wideB16) {
+                k_pass_b<D, Real, 16, true, true><<<grid, kThreads, a.smemB, s>>>(a);
+                return cudaGetLastError();
+            }
+        }
     }
     if (!pass_b) {
         if (a.fullA) k_pass_a<D, Real, NA, true, HZ><<<grid, kThreads, a.smemA, s>>>(a);
@@ -1272,6 +1281,10 @@ cudaError_t configure_nb(const StepArgs& a, bool pass_b) {
         if (e == cudaSuccess) e = configure_nb_h<D, Real, NA, NBB, true>(a, pass_b);
         if (e == cudaSuccess && !pass_b)
             e = set_smem(k_pass_a<D, Real, 16, true, true>, SmemA<D, Real, 16, true>::bytes());
+        if constexpr (sizeof(Real) == 4) {
+            if (e == cudaSuccess && pass_b)
+                e = set_smem(k_pass_b<D, Real, 16, true, true>, SmemB<Real, 16, true>::bytes());
+        }
     }
     return e;
 }
@@ -1331,10 +1344,16 @@ void pass_config(int D, int precision, int n1d, StepArgs* a) {
     // g-only pass A in batches of 16 DVs (a whole row) for 16 nodes per
     // dimension: half the per-batch work and barriers per DV, and the
     // shared memory the h arrays would take holds the wider batch
-    a->wideA16 = 0;
+    a->wideA16 = a->wideB16 = 0;
     if (D == 3 && a->hzero && n1d == 16) {
         a->wideA16 = 1;
         a->smemA = f64 ? SmemA<3, double, 16, true>::bytes() : SmemA<3, float, 16, true>::bytes();
+        // pass B likewise with FP32 storage (in FP64 the 16-wide staging does
+        // not fit in shared memory)
+        if (!f64) {
+            a->wideB16 = 1;
+            a->smemB = SmemB<float, 16, true>::bytes();
+        }
     }
 }
 
