@@ -1084,7 +1084,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                             const double xs = xs_row(x, S[0], p2, p3);
                             const double gr = dv_ref<Real>(m.gref, bp.d0 + j), hr = dv_ref<Real>(m.href, bp.d0 + j);
                             double gf = plus_ref<Real>(double(sg[j * kSI]), gr);
-                            double hf = plus_ref<Real>(double(sg[(NB + j) * kSI]), hr);
+                            double hf = plus_ref<Real>(double(HZ ? Real(0) : sg[(NB + j) * kSI]), hr);
                             if (xs > 0) shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                             shk_relax<D, double>(fs, x, sx[j * kSI], gf, hf, K3D, c0h, gf, hf);
                             sm.Fg[j * kSI + it] = Real(xs * minus_ref<Real>(gf, gr));
@@ -1101,10 +1101,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                         double gf, hf;
                         if (xs > 0) {
                             shk_relax<D, double>(fs, x, sx[j * kSI], plus_ref<Real>(double(sg[j * kSI]), gr),
-                                                 plus_ref<Real>(double(sg[(NB + j) * kSI]), hr), K3D, c0h, gf, hf);
+                                                 plus_ref<Real>(double(HZ ? Real(0) : sg[(NB + j) * kSI]), hr), K3D, c0h, gf, hf);
                         } else if (stored_in) {
                             gf = plus_ref<Real>(double(sg[j * kSI]), gr);
-                            hf = plus_ref<Real>(double(sg[(NB + j) * kSI]), hr);
+                            hf = plus_ref<Real>(double(HZ ? Real(0) : sg[(NB + j) * kSI]), hr);
                         } else {
                             const double cx = x - bU[0];
                             const double ge = bK * exp(-0.5 * (cx * cx + cyz) * bInv);
