@@ -284,7 +284,9 @@ struct SmemA {
     // not depend on the row); otherwise [2][NB][kSL] staged per batch
     double* stgx;
     Real* stg;      // [2][NH][NB][kSL] staged g~ (and h~)
-    Real* gB;       // [NB][kSL] gbar+
+    // FP32 storage: gbar+ is double-buffered by batch parity ([2][NB][kSL])
+    static constexpr int GB = sizeof(Real) == 4 ? 2 : 1;
+    Real* gB;       // [GB][NB][kSL] gbar+
     Real* hB;       // (null when h is identically zero)
     Real* Gg;       // [NB][D][kS0] gradients of the L0 cells
     Real* Gh;       // (null when h is identically zero)
@@ -293,7 +295,7 @@ struct SmemA {
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) + static_cast<size_t>(kMaxRegStencil) * kS0 * sizeof(int) +
                (static_cast<size_t>(CR_N) * kSL + static_cast<size_t>(XR) * kSL) * sizeof(double) +
-               (2 * NH * static_cast<size_t>(NB) * kSL + NH * NB * kSL + NH * NB * D * kS0 +
+               (2 * NH * static_cast<size_t>(NB) * kSL + GB * NH * NB * kSL + NH * NB * D * kS0 +
                 static_cast<size_t>(kMaxRegStencil) * D * kS0) *
                    sizeof(Real);
     }
@@ -311,9 +313,9 @@ __device__ __forceinline__ SmemA<D, Real, NB, HZ> carve_a(unsigned char* base) {
     s.stg = p;
     p += 2 * S::NH * NB * kSL;
     s.gB = p;
-    p += NB * kSL;
+    p += S::GB * NB * kSL;
     s.hB = HZ ? nullptr : p;
-    if (!HZ) p += NB * kSL;
+    if (!HZ) p += S::GB * NB * kSL;
     s.Gg = p;
     p += NB * D * kS0;
     s.Gh = HZ ? nullptr : p;
@@ -629,7 +631,11 @@ template <int D, typename Real, int NB, bool FULL, bool HZ>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const DevMesh& m = a.dm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SmemA<D, Real, NB, HZ> sm = carve_a<D, Real, NB, HZ>(smem_raw);
+    SmemA<D, Real, NB, HZ> sm = carve_a<D, Real, NB, HZ>(smem_raw);
+    // FP32 storage: gbar+ double-buffered by batch parity, so stage 1 of a
+    // batch overwrites no buffer the previous batch's stage 3 still reads,
+    // and the loop needs no barrier before stage 1
+    constexpr bool kDbl = SmemA<D, Real, NB, HZ>::GB == 2;
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);
@@ -697,11 +703,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     double ey1 = 1.0, ez1 = 1.0;   // y, z Maxwellian factors of this thread's local cell and row
     if (nbt > 0) stage0<D, Real, NB, FULL, HZ>(m, sm, 0, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
+    if constexpr (kDbl) __syncthreads();  // the CTA set-up above is visible to every thread
     for (int k = 0; k < nbt; ++k, walk.next()) {
         const int buf = k & 1;
         const BatchPos bp = walk.pos();
+        // this thread's staged entries of batch k (stage 1 reads only what the
+        // same thread staged)
         cp_wait_all();
-        __syncthreads();  // batch k staged; the previous batch's stage 3 is done
+        if constexpr (kDbl) {
+            const SmemA<D, Real, NB, HZ> s0 = carve_a<D, Real, NB, HZ>(smem_raw);
+            sm.gB = s0.gB + buf * NB * kSL;
+            if (!HZ) sm.hB = s0.hB + buf * NB * kSL;
+        } else {
+            __syncthreads();  // the previous batch's stage 3 is done with gbar+ (and the set-up is visible)
+        }
         if (k + 1 < nbt) {
             ahead.next();
             stage0<D, Real, NB, FULL, HZ>(m, sm, buf ^ 1, ahead.pos(), g, h, ctab, l1, p1, c1, act1, ex_res);
