@@ -634,8 +634,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_a(const StepArgs a) {
     SmemA<D, Real, NB, HZ> sm = carve_a<D, Real, NB, HZ>(smem_raw);
     // FP32 storage: gbar+ double-buffered by batch parity, so stage 1 of a
     // batch overwrites no buffer the previous batch's stage 3 still reads,
-    // and the loop needs no barrier before stage 1
-    constexpr bool kDbl = SmemA<D, Real, NB, HZ>::GB == 2;
+    // and the loop needs no barrier before stage 1.  Used where it costs no
+    // register spills (2-D, and 3-D rows that do not split into whole
+    // batches); measured 1.96 -> 1.68 ms on a 256^2 x 28^2 cavity, while the
+    // spilling 3-D 16-wide variant lost 4 %
+    constexpr bool kDbl = SmemA<D, Real, NB, HZ>::GB == 2 && (D == 2 || !FULL);
     const TileRange t = tile_range(m, a.chunk_begin);
     const Real* g = reinterpret_cast<const Real*>(a.ds.g[a.ds.cur]);
     const Real* h = reinterpret_cast<const Real*>(a.ds.h[a.ds.cur]);

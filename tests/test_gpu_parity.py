@@ -276,3 +276,18 @@ def test_errors_are_reported_not_fatal():
     with pytest.raises(dl.DugksError):
         s.df(np.array([10 ** 6], dtype=np.int32))
     s.step(1, c.dt)  # still usable
+
+
+def test_fp32c_rows_not_whole_batches():
+    # 6 nodes per dimension: DV rows do not split into whole 8-DV batches
+    # (the guarded passes; with FP32 storage pass A double-buffers gbar+)
+    c = cs.cube_case(6, 6, kn=0.1)
+    f64, f32 = dl.Solver(c), dl.Solver(c, precision=dl.FP32C)
+    f64.step(30, c.dt)
+    f32.step(30, c.dt)
+    a, b = f32.macros(), f64.macros()
+    for k in ("rho", "U", "T"):
+        err = float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k]))
+        assert err <= 1e-6, (k, err)
+    errs = ob.macro_errors(a, b, c.gas["R"], floor=1e-2)
+    assert errs["q"] <= 5e-6, errs
