@@ -129,6 +129,24 @@ struct View {
 };
 
 ADJ_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// loads of arrays a kernel only reads: on the device through the read-only
+// data path, which also lets the compiler issue the next DV's loads before
+// this DV's stores (the per-chunk DV loops are otherwise serialised by them)
+ADJ_HD double ro(const double* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+ADJ_HD int32_t ro(const int32_t* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
 ADJ_HD double magsqr3(const double* a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }
 
 // xi . Sf as the reference evaluates it: each product rounded, the sums
@@ -671,9 +689,9 @@ struct RRelax {
             const double* xi = v.xi + 3 * i;
             const double xs = xs_of(xi, S);
             const size_t id = at(i, v.nF, f);
-            const double lgo = v.lg[at(i, v.nC, ow)], lho = v.lh[at(i, v.nC, ow)];
-            const double lgn = v.lg[at(i, v.nC, ne)], lhn = v.lh[at(i, v.nC, ne)];
-            const double pg = v.fg[id], ph = v.fh[id];
+            const double lgo = ro(v.lg + at(i, v.nC, ow)), lho = ro(v.lh + at(i, v.nC, ow));
+            const double lgn = ro(v.lg + at(i, v.nC, ne)), lhn = ro(v.lh + at(i, v.nC, ne));
+            const double pg = ro(v.fg + id), ph = ro(v.fh + id);
             double a_g = xs * (dtVn * lgn - dtVo * lgo);
             double a_h = xs * (dtVn * lhn - dtVo * lho);
             const bool rel = !bnd || xs > 0;
@@ -870,18 +888,19 @@ struct RHalf {
         for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
             const size_t cb = at(i, v.nC, 0), id = cb + c;
             double abg = v.og[id], abh = v.oh[id];
-            const double gc[3] = {v.aGg[id], v.aGg[n + id], v.aGg[2 * n + id]};
-            const double hc[3] = {v.aGh[id], v.aGh[n + id], v.aGh[2 * n + id]};
+            const double gc[3] = {ro(v.aGg + id), ro(v.aGg + n + id), ro(v.aGg + 2 * n + id)};
+            const double hc[3] = {ro(v.aGh + id), ro(v.aGh + n + id), ro(v.aGh + 2 * n + id)};
             for (int en = e0; en < e1; ++en) {
-                const int f = v.cf_ent[en] >> 1;
+                const int ent = ro(v.cf_ent + en);
+                const int f = ent >> 1;
                 if (f >= v.nIF) break;
-                const bool is_nei = v.cf_ent[en] & 1;
-                const int o = is_nei ? v.own[f] : v.nei[f];  // the other cell of the face
+                const bool is_nei = ent & 1;
+                const int o = is_nei ? ro(v.own + f) : ro(v.nei + f);  // the other cell of the face
                 const size_t io = cb + o;
-                const double go[3] = {v.aGg[io], v.aGg[n + io], v.aGg[2 * n + io]};
-                const double ho[3] = {v.aGh[io], v.aGh[n + io], v.aGh[2 * n + io]};
-                const double* P = v.lsP + 3 * f;
-                const double* N = v.lsN + 3 * f;
+                const double go[3] = {ro(v.aGg + io), ro(v.aGg + n + io), ro(v.aGg + 2 * n + io)};
+                const double ho[3] = {ro(v.aGh + io), ro(v.aGh + n + io), ro(v.aGh + 2 * n + io)};
+                const double P[3] = {ro(v.lsP + 3 * f), ro(v.lsP + 3 * f + 1), ro(v.lsP + 3 * f + 2)};
+                const double N[3] = {ro(v.lsN + 3 * f), ro(v.lsN + 3 * f + 1), ro(v.lsN + 3 * f + 2)};
                 // s_f = lsP . aG_own - lsN . aG_nei; the neighbour adds it, the owner subtracts it
                 if (is_nei) {
                     abg += dot3(P, go) - dot3(N, gc);
@@ -893,13 +912,13 @@ struct RHalf {
             }
             const ShkEntity::DV d = e.at(v.xi + 3 * i);
             const double gEq = e.g(d), hEq = e.h(d);
-            s[0] += (gEq - v.g[id]) * abg + (hEq - v.h[id]) * abh;
+            s[0] += (gEq - ro(v.g + id)) * abg + (hEq - ro(v.h + id)) * abh;
             double t[9] = {0};
             e.rev(d, r * abg, r * abh, t);
             for (int k = 0; k < 8; ++k) s[1 + k] += t[k];
             s[5] += t[8];  // h^S of a cell is scaled by the cell's own T
-            v.og[id] = -1.0 / 3 * v.lg[id] + (1.0 - r) * abg;
-            v.oh[id] = -1.0 / 3 * v.lh[id] + (1.0 - r) * abh;
+            v.og[id] = -1.0 / 3 * ro(v.lg + id) + (1.0 - r) * abg;
+            v.oh[id] = -1.0 / 3 * ro(v.lh + id) + (1.0 - r) * abh;
         }
         double* p = v.pc + (static_cast<size_t>(ch) * v.nC + c) * kP;
         for (int k = 0; k < 9; ++k) p[k] = s[k];

@@ -70,3 +70,18 @@ def test_nonzero_h_state_leaves_g_only_passes():
     orc.step(6, c.dt)
     hs, ho = _check(b, orc, c.gas["R"])
     assert np.any(hs) and ob.rel_l2(hs, ho) <= TOL
+
+
+@pytest.mark.parametrize("precision", [dl.FP64, dl.FP32C])
+def test_g_only_passes_twenty_nodes(precision):
+    # 20 nodes per dimension (the mixed-precision configuration's DV set):
+    # the g-only passes in batches of 10 DVs
+    c = cs.cube_case(4, 20, kn=0.1)
+    gpu, orc = dl.Solver(c, precision=precision), ob.Oracle(c)
+    gpu.step(4, c.dt)
+    orc.step(4, c.dt)
+    if precision == dl.FP64:
+        _check(gpu, orc, c.gas["R"])
+    else:
+        errs = ob.macro_errors(gpu.macros(), orc.macros(), c.gas["R"], floor=1e-2)
+        assert max(errs.values()) <= 5e-6, errs
