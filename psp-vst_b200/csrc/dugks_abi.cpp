@@ -1244,9 +1244,13 @@ int dugks_get_macros(dugks_handle* h, double* rho, double* U, double* T, double*
     if (!h) return DUGKS_ERR_ARG;
     if (!h->initialised) return set_error(h, DUGKS_ERR_STATE, "dugks_get_macros before dugks_set_macros");
     const int nC = h->nC;
-    std::vector<double> cm(static_cast<size_t>(nC) * 9);
-    CUDA_TRY(h, cudaMemcpyAsync(cm.data(), h->ds.cm, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const size_t bytes = static_cast<size_t>(nC) * 9 * sizeof(double);
+    // a pinned staging buffer, kept by the handle: the copy runs at the
+    // link's speed instead of through a pageable bounce buffer every step
+    if (!h->host_cm) CUDA_TRY(h, cudaMallocHost(reinterpret_cast<void**>(&h->host_cm), bytes));
+    CUDA_TRY(h, cudaMemcpyAsync(h->host_cm, h->ds.cm, bytes, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const double* cm = h->host_cm;
     const std::vector<int32_t>& perm = h->tiling.perm;
     for (int c = 0; c < nC; ++c) {
         const int o = perm[c];
@@ -1418,6 +1422,7 @@ void dugks_destroy(dugks_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->nccl_comm) nccl_api().comm_destroy(static_cast<ncclComm_t>(h->nccl_comm));
     for (void* p : h->allocations) cudaFree(p);
+    if (h->host_cm) cudaFreeHost(h->host_cm);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -227,6 +227,7 @@ struct dugks_handle {
     long steps_done = 0;
     int64_t launches = 0;           // kernels launched by this handle
     double last_step_ms = 0;
+    double* host_cm = nullptr;      // pinned staging of the cell macros (dugks_get_macros)
     std::string last_error;
 };
 
