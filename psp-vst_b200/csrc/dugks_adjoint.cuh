@@ -232,14 +232,11 @@ ADJ_HD void shakhov_rev(const View& v, const double* xi, const double* U, double
 ADJ_HD void recon_vec(const View& v, int f, int c, const double* xi, double* d) {
     for (int k = 0; k < 3; ++k) d[k] = v.Cf[3 * f + k] - v.C[3 * c + k] - 0.5 * xi[k] * v.dt;
 }
-// in 2-D the z components of the gradient and of d are exactly zero (empty
-// direction, xi_z = 0), so the 2-D record neither stores nor reads them
 ADJ_HD double recon(const View& v, double phi, const double* G, size_t stride, size_t id, int f, int c,
                     const double* xi) {
     double d[3];
     recon_vec(v, f, c, xi, d);
-    const double s = ro(G + id) * d[0] + ro(G + stride + id) * d[1];
-    return phi + (v.D == 3 ? s + ro(G + 2 * stride + id) * d[2] : s);
+    return phi + (G[id] * d[0] + G[stride + id] * d[1] + G[2 * stride + id] * d[2]);
 }
 
 // macro record from the raw moments m (M0, M1[3], W, V3[3], M2[6]);
@@ -458,7 +455,7 @@ struct FGrad {
             }
         }
         const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        for (int k = 0; k < v.D; ++k) {
+        for (int k = 0; k < 3; ++k) {
             v.Gg[k * n + idx] = gg[k];
             v.Gh[k * n + idx] = gh[k];
         }
@@ -865,7 +862,7 @@ struct RGradAdj {
             }
         }
         const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        for (int k = 0; k < v.D; ++k) {
+        for (int k = 0; k < 3; ++k) {
             v.aGg[k * n + idx] = Gg[k];
             v.aGh[k * n + idx] = Gh[k];
         }
@@ -891,9 +888,8 @@ struct RHalf {
         for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
             const size_t cb = at(i, v.nC, 0), id = cb + c;
             double abg = v.og[id], abh = v.oh[id];
-            const bool d3 = v.D == 3;
-            const double gc[3] = {ro(v.aGg + id), ro(v.aGg + n + id), d3 ? ro(v.aGg + 2 * n + id) : 0.0};
-            const double hc[3] = {ro(v.aGh + id), ro(v.aGh + n + id), d3 ? ro(v.aGh + 2 * n + id) : 0.0};
+            const double gc[3] = {ro(v.aGg + id), ro(v.aGg + n + id), ro(v.aGg + 2 * n + id)};
+            const double hc[3] = {ro(v.aGh + id), ro(v.aGh + n + id), ro(v.aGh + 2 * n + id)};
             for (int en = e0; en < e1; ++en) {
                 const int ent = ro(v.cf_ent + en);
                 const int f = ent >> 1;
@@ -901,8 +897,8 @@ struct RHalf {
                 const bool is_nei = ent & 1;
                 const int o = is_nei ? ro(v.own + f) : ro(v.nei + f);  // the other cell of the face
                 const size_t io = cb + o;
-                const double go[3] = {ro(v.aGg + io), ro(v.aGg + n + io), d3 ? ro(v.aGg + 2 * n + io) : 0.0};
-                const double ho[3] = {ro(v.aGh + io), ro(v.aGh + n + io), d3 ? ro(v.aGh + 2 * n + io) : 0.0};
+                const double go[3] = {ro(v.aGg + io), ro(v.aGg + n + io), ro(v.aGg + 2 * n + io)};
+                const double ho[3] = {ro(v.aGh + io), ro(v.aGh + n + io), ro(v.aGh + 2 * n + io)};
                 const double P[3] = {ro(v.lsP + 3 * f), ro(v.lsP + 3 * f + 1), ro(v.lsP + 3 * f + 2)};
                 const double N[3] = {ro(v.lsN + 3 * f), ro(v.lsN + 3 * f + 1), ro(v.lsN + 3 * f + 2)};
                 // s_f = lsP . aG_own - lsN . aG_nei; the neighbour adds it, the owner subtracts it
