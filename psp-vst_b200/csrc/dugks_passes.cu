@@ -541,7 +541,7 @@ template <int D, typename Real, int NB, bool HZ>
 __device__ __forceinline__ void grad_one(const SmemA<D, Real, NB, HZ>& sm, int j, int l, const int* nbi,
                                          const Real (*ls)[D], int nk) {
     const Real* gB = sm.gB + j * kSL;
-    const Real* hB = sm.hB + j * kSL;
+    const Real* hB = HZ ? nullptr : sm.hB + j * kSL;
     const Real g0 = gB[l], h0 = HZ ? Real(0) : hB[l];
     Real gx[D], hx[D];
 #pragma unroll
@@ -595,7 +595,7 @@ __device__ __forceinline__ void stage2(const DevMesh& m, const SmemA<D, Real, NB
             const int j = part + kParts0 * jj;
             if (!FULL && j >= bp.nb) break;
             const Real* gB = sm.gB + j * kSL;
-            const Real* hB = sm.hB + j * kSL;
+            const Real* hB = HZ ? nullptr : sm.hB + j * kSL;
             const Real g0 = gB[l], h0 = HZ ? Real(0) : hB[l];
             Real gx[D], hx[D];
 #pragma unroll
