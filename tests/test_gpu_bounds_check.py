@@ -67,5 +67,5 @@ def test_checked_boundary_types_and_fp32c():
 def test_checked_wide_batches(precision):
     # the g-only passes in 16-DV (16 nodes per dimension) and 10-DV (20
     # nodes) batches
-    _same(cs.ball_case(3, 3, 1.12, 16, kn=0.1, mach=0.5), 2, precision=precision)
+    _same(cs.ball_case(2, 3, 1.12, 16, kn=0.1, mach=0.5), 2, precision=precision)
     _same(cs.cube_case(4, 20, kn=0.1), 2, precision=precision)
