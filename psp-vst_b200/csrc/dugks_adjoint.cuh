@@ -481,6 +481,46 @@ struct FGrad {
     }
 };
 
+// 2 over a DV chunk: the same per-DV arithmetic as FGrad, the cell's face
+// list and least-squares vectors from the read-only path
+struct FGradC {
+    View v;
+    ADJ_HD void operator()(int64_t idx) const {
+        const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
+        const size_t n = static_cast<size_t>(v.nv) * v.nC;
+        const int e0 = v.cf_off[c], e1 = v.cf_off[c + 1];
+        for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
+            const size_t base = at(i, v.nC, 0), cid = base + c;
+            double gg[3] = {0, 0, 0}, gh[3] = {0, 0, 0};
+            for (int e = e0; e < e1; ++e) {
+                const int ent = ro(v.cf_ent + e);
+                const int f = ent >> 1;
+                if (f >= v.nIF) break;
+                const int ow = ro(v.own + f), ne = ro(v.nei + f);
+                const double dg = ro(v.gbp + base + ne) - ro(v.gbp + base + ow);
+                const double dh = ro(v.hbp + base + ne) - ro(v.hbp + base + ow);
+                if (ent & 1) {
+                    for (int k = 0; k < 3; ++k) {
+                        const double l = ro(v.lsN + 3 * f + k);
+                        gg[k] -= l * dg;
+                        gh[k] -= l * dh;
+                    }
+                } else {
+                    for (int k = 0; k < 3; ++k) {
+                        const double l = ro(v.lsP + 3 * f + k);
+                        gg[k] += l * dg;
+                        gh[k] += l * dh;
+                    }
+                }
+            }
+            for (int k = 0; k < 3; ++k) {
+                v.Gg[k * n + cid] = gg[k];
+                v.Gh[k * n + cid] = gh[k];
+            }
+        }
+    }
+};
+
 // 3: face values at the half step (wall incoming DVs come in stage 5)
 struct FFace {
     View v;
@@ -1122,7 +1162,7 @@ template <class Ex>
 int record_step(Ex& ex, const View& v) {
     int st;
     if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FHalfC{v}))) return st;
-    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nC, FGrad{v}))) return st;
+    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FGradC{v}))) return st;
     if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nF, FFaceC{v}))) return st;
     if (v.nBF > 0) {
         if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nBF, FWallOut{v}))) return st;
