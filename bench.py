@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32c", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the short adjoint measurement of the default run")
+    p.add_argument("--no-batch", action="store_true", help="skip the short batch measurement of the default run")
     p.add_argument("--no-cube", action="store_true",
                    help="skip the mixed-precision sub-line of the default run (64^3 cube, 20^3 DVs, FP64 and FP32c)")
     p.add_argument("--cube-steps", type=int, default=40,
@@ -304,11 +305,21 @@ def run_batch(args):
     import torch
     from dugks_b200 import lib as dl
     torch.cuda.set_device(0)
+    prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
+    print(json.dumps(batch_line(args.steps, args.warmup, prec, args.tune)), flush=True)
+
+
+def batch_line(steps: int, warmup: int, prec: int, tune: bool = False) -> dict:
+    """The batch of batch_cases() through one CUDA graph, timed with CUDA
+    events over `steps` steps after `warmup`; the same cases stepped one at
+    a time; end to end with every case's macros to the host; and the
+    graph's own cost on cases whose kernels do almost nothing."""
+    import torch
+    from dugks_b200 import lib as dl
     seed = 20261203
     cases = batch_cases(seed)
-    prec = dl.FP64 if args.precision == "fp64" else dl.FP32C
     tuning = None
-    if args.tune:
+    if tune:
         t0 = time.perf_counter()
         best, table = dl.tune_batch(cases, [c.dt for c in cases], precision=prec)
         tuning = {"chosen": {"tile_cells": best["tile_cells"], "chunk_scale": best["chunk_scale"]},
@@ -317,8 +328,8 @@ def run_batch(args):
     else:
         solvers = [dl.Solver(c, precision=prec) for c in cases]
     pairs = sum(c.n_cells * c.n_dv for c in cases)
-    K = max(2, args.steps - args.steps % 2)
-    W = max(4, args.warmup + args.warmup % 2)
+    K = max(2, steps - steps % 2)
+    W = max(4, warmup + warmup % 2)
     batch = dl.Batch(solvers, [c.dt for c in cases])
     batch.step(W)
     torch.cuda.synchronize()
@@ -385,7 +396,9 @@ def run_batch(args):
         "clocks": clocks,
     }
     batch.close()
-    print(json.dumps(line), flush=True)
+    for s_ in solvers:
+        s_.close()
+    return line
 
 
 def sphere_loads(solver, case, steps_done):
@@ -798,6 +811,15 @@ def main():
         line["adjoint"] = {k: sub[k] for k in ("value", "unit", "steps", "ms_per_step", "adjoint", "J", "gradient",
                                                 "gpu_launches")}
         line["adjoint"]["workload"] = sub["config"]["workload"]
+    if rank == 0 and world == 1 and not args.no_batch and args.workload == "ball":
+        # the batched configuration: 64 seeded cavities through one graph,
+        # beside the same cases stepped one at a time
+        sub = batch_line(8, 4, dl.FP32C)
+        line["batch"] = {k: sub[k] for k in ("value", "unit", "steps", "ms_per_step", "one_at_a_time", "e2e",
+                                              "gpu_launches", "graph_kernels_per_two_steps", "graph_floor",
+                                              "step_roofline", "dtype")}
+        line["batch"]["workload"] = sub["config"]["workload"]
+        line["batch"]["pairs"] = sub["config"]["pairs"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_sample_ndv, 2, 1)
     if rank == 0:

@@ -414,24 +414,9 @@ struct FInBy {
     }
 };
 
-// 1: gbar+ and hbar+ of every (DV, cell)
+// 1: gbar+ and hbar+ per (cell, DV chunk): the cell's record, relax factor
+// and Shakhov constants once for the chunk's DVs
 struct FHalf {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int i = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const double* m = v.cm + 9 * static_cast<size_t>(c);
-        const double tau = tau_of(v, m[4], m[0]);
-        const double r = 1.5 * v.dt / (2.0 * tau + v.dt);
-        const ShkEntity e(v, m + 1, m[4], m[0], m + 5, m[4]);
-        const ShkEntity::DV d = e.at(v.xi + 3 * i);
-        v.gbp[idx] = (1.0 - r) * v.g[idx] + r * e.g(d);
-        v.hbp[idx] = (1.0 - r) * v.h[idx] + r * e.h(d);
-    }
-};
-
-// 1 over a DV chunk: the cell's record, relax factor and Shakhov constants
-// once for the chunk's DVs (the per-(DV, cell) form recomputed them per DV)
-struct FHalfC {
     View v;
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
@@ -481,46 +466,6 @@ struct FGrad {
     }
 };
 
-// 2 over a DV chunk: the same per-DV arithmetic as FGrad, the cell's face
-// list and least-squares vectors from the read-only path
-struct FGradC {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        const int e0 = v.cf_off[c], e1 = v.cf_off[c + 1];
-        for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
-            const size_t base = at(i, v.nC, 0), cid = base + c;
-            double gg[3] = {0, 0, 0}, gh[3] = {0, 0, 0};
-            for (int e = e0; e < e1; ++e) {
-                const int ent = ro(v.cf_ent + e);
-                const int f = ent >> 1;
-                if (f >= v.nIF) break;
-                const int ow = ro(v.own + f), ne = ro(v.nei + f);
-                const double dg = ro(v.gbp + base + ne) - ro(v.gbp + base + ow);
-                const double dh = ro(v.hbp + base + ne) - ro(v.hbp + base + ow);
-                if (ent & 1) {
-                    for (int k = 0; k < 3; ++k) {
-                        const double l = ro(v.lsN + 3 * f + k);
-                        gg[k] -= l * dg;
-                        gh[k] -= l * dh;
-                    }
-                } else {
-                    for (int k = 0; k < 3; ++k) {
-                        const double l = ro(v.lsP + 3 * f + k);
-                        gg[k] += l * dg;
-                        gh[k] += l * dh;
-                    }
-                }
-            }
-            for (int k = 0; k < 3; ++k) {
-                v.Gg[k * n + cid] = gg[k];
-                v.Gh[k * n + cid] = gh[k];
-            }
-        }
-    }
-};
-
 // 3: face values at the half step (wall incoming DVs come in stage 5)
 struct FFace {
     View v;
@@ -557,62 +502,6 @@ struct FFace {
             const double gi = v.brho[b] * eq_by_rho(v, xi, v.cm + 9 * static_cast<size_t>(ow) + 1, Tb);
             v.fg[idx] = gi;
             v.fh[idx] = gi * (v.R * Tb) * static_cast<double>(v.K + 3 - v.D);
-        }
-    }
-};
-
-// 3 over a DV chunk: the face's geometry (area vector, Cf - C of both
-// sides, the sides themselves) once for the chunk's DVs; the same
-// arithmetic per DV as FFace
-struct FFaceC {
-    View v;
-    ADJ_HD double rec(double phi, const double* G, size_t n, size_t id, const double* dc, const double* xi) const {
-        double d[3];
-        for (int k = 0; k < 3; ++k) d[k] = dc[k] - 0.5 * xi[k] * v.dt;
-        return phi + (ro(G + id) * d[0] + ro(G + n + id) * d[1] + ro(G + 2 * n + id) * d[2]);
-    }
-    ADJ_HD void operator()(int64_t idx) const {
-        const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
-        const double S[3] = {v.S[3 * f], v.S[3 * f + 1], v.S[3 * f + 2]};
-        const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        const bool internal = f < v.nIF;
-        const int ow = v.own[f], ne = internal ? v.nei[f] : ow;
-        double dO[3], dN[3];
-        for (int k = 0; k < 3; ++k) {
-            dO[k] = v.Cf[3 * f + k] - v.C[3 * ow + k];
-            dN[k] = v.Cf[3 * f + k] - v.C[3 * ne + k];
-        }
-        const int b = f - v.nIF;
-        const bool far = !internal && v.btype[b] == 2;
-        const double Tb = far ? v.bT[b] : 0.0, rb = far ? v.brho[b] : 0.0;
-        for (int i = chunk_lo(v.nv, v.nchF, ch); i < chunk_lo(v.nv, v.nchF, ch + 1); ++i) {
-            const double* xi = v.xi + 3 * i;
-            const double xs = xs_of(xi, S);
-            const size_t id = at(i, v.nF, f);
-            const size_t cb = at(i, v.nC, 0);
-            if (internal) {
-                if (xs >= kVSmall) {
-                    v.fg[id] = rec(ro(v.gbp + cb + ow), v.Gg, n, cb + ow, dO, xi);
-                    v.fh[id] = rec(ro(v.hbp + cb + ow), v.Gh, n, cb + ow, dO, xi);
-                } else if (xs < -kVSmall) {
-                    v.fg[id] = rec(ro(v.gbp + cb + ne), v.Gg, n, cb + ne, dN, xi);
-                    v.fh[id] = rec(ro(v.hbp + cb + ne), v.Gh, n, cb + ne, dN, xi);
-                } else {
-                    double dn = rec(0.0, v.Gg, n, cb + ne, dN, xi);
-                    double d_o = rec(0.0, v.Gg, n, cb + ow, dO, xi);
-                    v.fg[id] = 0.5 * (((ro(v.gbp + cb + ne) + dn) + ro(v.gbp + cb + ow)) + d_o);
-                    dn = rec(0.0, v.Gh, n, cb + ne, dN, xi);
-                    d_o = rec(0.0, v.Gh, n, cb + ow, dO, xi);
-                    v.fh[id] = 0.5 * (((ro(v.hbp + cb + ne) + dn) + ro(v.hbp + cb + ow)) + d_o);
-                }
-            } else if (xs > 0) {
-                v.fg[id] = rec(ro(v.gbp + cb + ow), v.Gg, n, cb + ow, dO, xi);
-                v.fh[id] = rec(ro(v.hbp + cb + ow), v.Gh, n, cb + ow, dO, xi);
-            } else if (far) {
-                const double gi = rb * eq_by_rho(v, xi, v.cm + 9 * static_cast<size_t>(ow) + 1, Tb);
-                v.fg[id] = gi;
-                v.fh[id] = gi * (v.R * Tb) * static_cast<double>(v.K + 3 - v.D);
-            }
         }
     }
 };
@@ -874,9 +763,7 @@ struct RFaceMom {
     View v;
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
-        // the face's coefficient record in registers for the chunk's DVs
-        double co[kCo];
-        for (int k = 0; k < kCo; ++k) co[k] = ro(v.fco + kCo * static_cast<size_t>(f) + k);
+        const double* co = v.fco + kCo * static_cast<size_t>(f);
         const bool bnd = f >= v.nIF;
         const int b = f - v.nIF;
         const int type = bnd ? v.btype[b] : 0;
@@ -985,52 +872,6 @@ struct RGradAdj {
         }
         v.og[idx] = dg;
         v.oh[idx] = dh;
-    }
-};
-
-// R4 over a DV chunk: the same per-DV arithmetic as RGradAdj, the cell's
-// face list and geometry read once per chunk from the read-only path
-struct RGradAdjC {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        const int e0 = v.cf_off[c], e1 = v.cf_off[c + 1];
-        for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
-            const double* xi = v.xi + 3 * i;
-            const size_t cid = at(i, v.nC, c);
-            double Gg[3] = {0, 0, 0}, Gh[3] = {0, 0, 0};
-            double dg = 4.0 / 3 * ro(v.lg + cid), dh = 4.0 / 3 * ro(v.lh + cid);
-            for (int e = e0; e < e1; ++e) {
-                const int ent = ro(v.cf_ent + e);
-                const int f = ent >> 1;
-                const bool is_nei = ent & 1;
-                const double S[3] = {ro(v.S + 3 * f), ro(v.S + 3 * f + 1), ro(v.S + 3 * f + 2)};
-                const double xs = xs_of(xi, S);
-                double share;
-                if (f >= v.nIF) share = xs > 0 ? 1.0 : 0.0;
-                else if (xs >= kVSmall) share = is_nei ? 0.0 : 1.0;
-                else if (xs < -kVSmall) share = is_nei ? 1.0 : 0.0;
-                else share = 0.5;
-                if (share == 0.0) continue;
-                const size_t id = at(i, v.nF, f);
-                const double a_g = share * ro(v.ag + id), a_h = share * ro(v.ah + id);
-                double d[3];
-                for (int k = 0; k < 3; ++k) d[k] = ro(v.Cf + 3 * f + k) - ro(v.C + 3 * c + k) - 0.5 * xi[k] * v.dt;
-                dg += a_g;
-                dh += a_h;
-                for (int k = 0; k < 3; ++k) {
-                    Gg[k] += a_g * d[k];
-                    Gh[k] += a_h * d[k];
-                }
-            }
-            for (int k = 0; k < 3; ++k) {
-                v.aGg[k * n + cid] = Gg[k];
-                v.aGh[k * n + cid] = Gh[k];
-            }
-            v.og[cid] = dg;
-            v.oh[cid] = dh;
-        }
     }
 };
 
@@ -1161,9 +1002,9 @@ struct RInBy {
 template <class Ex>
 int record_step(Ex& ex, const View& v) {
     int st;
-    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FHalfC{v}))) return st;
-    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FGradC{v}))) return st;
-    if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nF, FFaceC{v}))) return st;
+    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FHalf{v}))) return st;
+    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nC, FGrad{v}))) return st;
+    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nF, FFace{v}))) return st;
     if (v.nBF > 0) {
         if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nBF, FWallOut{v}))) return st;
         if ((st = ex.run(v.nBF, FWallRho{v}))) return st;
@@ -1189,7 +1030,7 @@ int reverse_step(Ex& ex, const View& v) {
         if ((st = ex.run(v.nBF, RBoundary{v}))) return st;
         if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nBF, RWallOut{v}))) return st;
     }
-    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, RGradAdjC{v}))) return st;
+    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nC, RGradAdj{v}))) return st;
     if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, RHalf{v}))) return st;
     if ((st = ex.run(v.nC, RCellMac{v}))) return st;
     if (v.fold) return ex.run(static_cast<int64_t>(v.nv) * v.nC, RCellMom{v});
