@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -28,8 +29,18 @@ namespace adj = dugks::adj;
 
 constexpr int kBlock = 256;
 
+// CTAs of 256 threads a functor asks to keep resident per SM (a register cap)
+template <class F, class = void>
+struct MinCtas {
+    static constexpr int value = 1;
+};
 template <class F>
-__global__ void __launch_bounds__(kBlock) k_adjoint(F f, int64_t n) {
+struct MinCtas<F, std::void_t<decltype(F::kMinCtas)>> {
+    static constexpr int value = F::kMinCtas;
+};
+
+template <class F>
+__global__ void __launch_bounds__(kBlock, MinCtas<F>::value) k_adjoint(F f, int64_t n) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) f(i);
 }

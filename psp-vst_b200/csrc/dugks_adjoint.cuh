@@ -877,9 +877,31 @@ struct RGradAdj {
 
 // R5: per (cell, DV chunk): the gradient's adjoint into gbar+, the half
 // step's reverse into the state adjoint, and the cell's Shakhov and
-// relax-factor sums
+// relax-factor sums.  A cell with at most kRegF internal faces keeps its
+// face list (face, other cell, side) in registers for the chunk's DVs and
+// walks it unrolled, so the neighbours' gradient-adjoint loads of all its
+// faces are independent of one another; cells with more faces walk the
+// list from memory.  Either way the faces are added in list order.
 struct RHalf {
     View v;
+    static constexpr int kRegF = 6;
+    static constexpr int kMinCtas = 2;  // 16 warps per SM
+    ADJ_HD void face_add(size_t cb, size_t n, int f, int o, bool is_nei, const double* gc, const double* hc,
+                         double& abg, double& abh) const {
+        const size_t io = cb + o;
+        const double go[3] = {ro(v.aGg + io), ro(v.aGg + n + io), ro(v.aGg + 2 * n + io)};
+        const double ho[3] = {ro(v.aGh + io), ro(v.aGh + n + io), ro(v.aGh + 2 * n + io)};
+        const double P[3] = {ro(v.lsP + 3 * f), ro(v.lsP + 3 * f + 1), ro(v.lsP + 3 * f + 2)};
+        const double N[3] = {ro(v.lsN + 3 * f), ro(v.lsN + 3 * f + 1), ro(v.lsN + 3 * f + 2)};
+        // s_f = lsP . aG_own - lsN . aG_nei; the neighbour adds it, the owner subtracts it
+        if (is_nei) {
+            abg += dot3(P, go) - dot3(N, gc);
+            abh += dot3(P, ho) - dot3(N, hc);
+        } else {
+            abg -= dot3(P, gc) - dot3(N, go);
+            abh -= dot3(P, hc) - dot3(N, ho);
+        }
+    }
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
         const double* m = v.cm + 9 * static_cast<size_t>(c);
@@ -888,30 +910,38 @@ struct RHalf {
         const ShkEntity e(v, m + 1, m[4], m[0], m + 5, m[4]);
         const size_t n = static_cast<size_t>(v.nv) * v.nC;
         const int e0 = v.cf_off[c], e1 = v.cf_off[c + 1];
+        // the internal faces lead the cell's list
+        int nf = 0;
+        while (e0 + nf < e1 && (ro(v.cf_ent + e0 + nf) >> 1) < v.nIF) ++nf;
+        const bool reg = nf <= kRegF;
+        int rf[kRegF], ro_[kRegF];
+        unsigned rn = 0;
+#pragma unroll
+        for (int q = 0; q < kRegF; ++q) {
+            rf[q] = 0;
+            ro_[q] = 0;
+            if (reg && q < nf) {
+                const int ent = ro(v.cf_ent + e0 + q);
+                rf[q] = ent >> 1;
+                if (ent & 1) rn |= 1u << q;
+                ro_[q] = (ent & 1) ? ro(v.own + rf[q]) : ro(v.nei + rf[q]);  // the other cell of the face
+            }
+        }
         double s[9] = {0};
         for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
             const size_t cb = at(i, v.nC, 0), id = cb + c;
             double abg = v.og[id], abh = v.oh[id];
             const double gc[3] = {ro(v.aGg + id), ro(v.aGg + n + id), ro(v.aGg + 2 * n + id)};
             const double hc[3] = {ro(v.aGh + id), ro(v.aGh + n + id), ro(v.aGh + 2 * n + id)};
-            for (int en = e0; en < e1; ++en) {
-                const int ent = ro(v.cf_ent + en);
-                const int f = ent >> 1;
-                if (f >= v.nIF) break;
-                const bool is_nei = ent & 1;
-                const int o = is_nei ? ro(v.own + f) : ro(v.nei + f);  // the other cell of the face
-                const size_t io = cb + o;
-                const double go[3] = {ro(v.aGg + io), ro(v.aGg + n + io), ro(v.aGg + 2 * n + io)};
-                const double ho[3] = {ro(v.aGh + io), ro(v.aGh + n + io), ro(v.aGh + 2 * n + io)};
-                const double P[3] = {ro(v.lsP + 3 * f), ro(v.lsP + 3 * f + 1), ro(v.lsP + 3 * f + 2)};
-                const double N[3] = {ro(v.lsN + 3 * f), ro(v.lsN + 3 * f + 1), ro(v.lsN + 3 * f + 2)};
-                // s_f = lsP . aG_own - lsN . aG_nei; the neighbour adds it, the owner subtracts it
-                if (is_nei) {
-                    abg += dot3(P, go) - dot3(N, gc);
-                    abh += dot3(P, ho) - dot3(N, hc);
-                } else {
-                    abg -= dot3(P, gc) - dot3(N, go);
-                    abh -= dot3(P, hc) - dot3(N, ho);
+            if (reg) {
+#pragma unroll
+                for (int q = 0; q < kRegF; ++q)
+                    if (q < nf) face_add(cb, n, rf[q], ro_[q], (rn >> q) & 1u, gc, hc, abg, abh);
+            } else {
+                for (int en = e0; en < e0 + nf; ++en) {
+                    const int ent = ro(v.cf_ent + en);
+                    const int f = ent >> 1;
+                    face_add(cb, n, f, (ent & 1) ? ro(v.own + f) : ro(v.nei + f), ent & 1, gc, hc, abg, abh);
                 }
             }
             const ShkEntity::DV d = e.at(v.xi + 3 * i);
