@@ -250,7 +250,9 @@ int dugks_dv_range(const dugks_handle* h, int32_t* first_dv, int32_t* n_dv_local
 
 /* One step of a sharded handle with host-side reduction, in three calls:
  *   phase 0 (dt): face reconstruction and raw face moments of this shard;
- *   phase 1: face macros, face relaxation, update, raw cell moments;
+ *   phase 1: face macros, face relaxation, update, raw cell moments (with a
+ *            DV list and macro_flux, followed by the cell moments of the
+ *            update's flux term);
  *   phase 2: cell macros; the step is complete.
  * After phases 0 and 1, *part / *n_part are a DEVICE buffer of doubles that
  * the host replaces, in place, by its sum over all shards before the next

@@ -168,8 +168,6 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
         return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create: n_solution_dims must be 2 or 3");
     if (dvl) {
         if (dvl->n_dv < 1 || !dvl->xi || !dvl->weights) return fail(DUGKS_ERR_ARG, "dugks_create_dv_list: empty DV list");
-        if (opt.macro_flux && shard && shard->world > 1)
-            return fail(DUGKS_ERR_UNSUPPORTED, "dugks_create_dv_list: macroFlux yes is not built for DV shards");
     } else if (dv->n_per_dim < 1 || !dv->xis || !dv->weights) {
         return fail(DUGKS_ERR_ARG, "dugks_create: empty DV set");
     }
@@ -521,6 +519,8 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
     if ((st = dev_alloc(h, &ds.partF, static_cast<size_t>(chunks) * dm.n_items * dugks::kNM)) ||
         (st = dev_alloc(h, &ds.partC, static_cast<size_t>(chunks) * nC * dugks::kNM)) ||
         (dvl && opt.macro_flux && (st = dev_alloc(h, &ds.partX, static_cast<size_t>(chunks) * nC * dugks::kFX))) ||
+        (dvl && opt.macro_flux && shard &&
+         (st = dev_alloc(h, &ds.redC, static_cast<size_t>(nC) * (dugks::kNM + dugks::kFX)))) ||
         (st = dev_alloc(h, &ds.cellrec, static_cast<size_t>(dugks::REC_N) * nC)) ||
         (st = dev_alloc(h, &ds.facerec, static_cast<size_t>(dugks::REC_N) * dm.n_items)) ||
         (st = dev_alloc(h, &ds.ctab, static_cast<size_t>(h->D) * h->n1d * nC)) ||
@@ -769,6 +769,32 @@ struct AdaptCall {
     double max_co, max_dt;
 };
 
+// The cell partials of a sharded handle summed over its DV chunks, ready for
+// the reduction over the shards: partC's first chunk, or (DV-list macroFlux)
+// redC, which gathers the cell moments and the flux-term moments so that one
+// reduction covers both.  *one is pointed at what the cell combine reads.
+static int gather_cell_partials(dugks_handle* h, dugks::StepArgs* one, double** buf, size_t* n, int* launches) {
+    const size_t nm = static_cast<size_t>(h->nC) * dugks::kNM;
+    CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partC, h->chunks, nm, h->stream));
+    if (h->chunks > 1) ++*launches;
+    if (!h->ds.redC) {
+        *buf = h->ds.partC;
+        *n = nm;
+        return DUGKS_OK;
+    }
+    const size_t nx = static_cast<size_t>(h->nC) * dugks::kFX;
+    CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partX, h->chunks, nx, h->stream));
+    if (h->chunks > 1) ++*launches;
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.redC, h->ds.partC, nm * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->ds.redC + nm, h->ds.partX, nx * sizeof(double), cudaMemcpyDeviceToDevice,
+                                h->stream));
+    one->ds.partC = h->ds.redC;
+    one->ds.partX = h->ds.redC + nm;
+    *buf = h->ds.redC;
+    *n = nm + nx;
+    return DUGKS_OK;
+}
+
 // One step's stages on the handle's stream.  A sharded handle sums its DV
 // chunks and all-reduces the raw moments before each combine, which then
 // read one chunk.  sev (5 events, or null) are recorded before pass A and
@@ -798,11 +824,10 @@ static int enqueue_step(dugks_handle* h, const dugks::StepArgs& a, cudaEvent_t* 
     CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, launches));
     if (sev) CUDA_TRY(h, cudaEventRecord(sev[3], h->stream));
     if (sh) {
-        const size_t n = static_cast<size_t>(h->nC) * dugks::kNM;
-        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partC, h->chunks, n, h->stream));
-        if (h->chunks > 1) ++*launches;
-        const int st = shard_allreduce(h, h->ds.partC, n);
-        if (st) return st;
+        double* buf = nullptr;
+        size_t n = 0;
+        int st = gather_cell_partials(h, &one, &buf, &n, launches);
+        if (st || (st = shard_allreduce(h, buf, n))) return st;
     }
     CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, launches));
     if (sev) CUDA_TRY(h, cudaEventRecord(sev[4], h->stream));
@@ -953,14 +978,18 @@ int dugks_shard_phase(dugks_handle* h, int32_t phase, double dt, double** part, 
         one.chunks = 1;
         CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_FACE_COMBINE, h->stream, &launches));
         CUDA_TRY(h, dugks::launch_stage(a, h->precision, dugks::STAGE_PASS_B, h->stream, &launches));
-        const size_t n = static_cast<size_t>(h->nC) * dugks::kNM;
-        CUDA_TRY(h, dugks::launch_sum_chunks(h->ds.partC, h->chunks, n, h->stream));
-        if (h->chunks > 1) ++launches;
-        *part = h->ds.partC;
+        double* buf = nullptr;
+        size_t n = 0;
+        if (int st = gather_cell_partials(h, &one, &buf, &n, &launches)) return st;
+        *part = buf;
         *n_part = static_cast<int64_t>(n);
     } else {
         dugks::StepArgs one = make_args(h, h->shard_dt, 0.0);
         one.chunks = 1;
+        if (h->ds.redC) {
+            one.ds.partC = h->ds.redC;
+            one.ds.partX = h->ds.redC + static_cast<size_t>(h->nC) * dugks::kNM;
+        }
         CUDA_TRY(h, dugks::launch_stage(one, h->precision, dugks::STAGE_CELL_COMBINE, h->stream, &launches));
         h->cellrec_dt = 0.0;   // the next phase 0 sets the relax factors for its dt
         h->ds.cur = 1 - h->ds.cur;

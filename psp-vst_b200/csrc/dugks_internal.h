@@ -140,6 +140,7 @@ struct DevState {
     double* partF;     // [chunks][n_items][kNM]
     double* partC;     // [chunks][nC][kNM]
     double* partX;     // [chunks][nC][kFX] DV-list macroFlux: moments of the flux term (else null)
+    double* redC;      // sharded DV-list macroFlux: [nC][kNM] cell moments then [nC][kFX] flux moments, reduced together
     double* cellrec;   // [REC_N][nC]
     // face records in item order (each face's record is written to its one
     // or two items, so that a tile reads its faces' records contiguously)

@@ -88,9 +88,6 @@ def test_velocity_mesh_shards_and_refusals():
         orc.evolution(c.dt)
     errs = ob.macro_errors(shards[0].macros(), orc.macros(), c.gas["R"])
     assert max(errs.values()) <= 1e-10, errs
-    with pytest.raises(dl.DugksError) as e:
-        dl.Solver(c, macro_flux=True, shard=dl.shard(0, 2))
-    assert e.value.code == 7
     s = cs.channel_case(6, 3, 6, sides={"top": {"kind": "symmetryPlane"}}, flatten=False)
     s.use_velocity_mesh(meshgen.velocity_box(6, 1600.0, 2))
     s.flatten()
@@ -122,3 +119,32 @@ def test_velocity_mesh_macro_flux(which):
     plain = dl.Solver(c)
     plain.step(8, c.dt)
     assert not np.array_equal(plain.macros()["rho"], gpu.macros()["rho"])
+
+
+# macroFlux yes on a velocity mesh over DV shards: the flux-term moments are
+# reduced over the shards together with the cell moments
+@pytest.mark.parametrize("world", [2, 3])
+def test_velocity_mesh_macro_flux_shards(world):
+    c = _vmesh_cavity()
+    shards = [dl.Solver(c, macro_flux=True, shard=dl.shard(r, world), dv_chunks=2) for r in range(world)]
+    sh.step_local(shards, 6, c.dt)
+    plain = dl.Solver(c, macro_flux=True)
+    plain.step(6, c.dt)
+    orc = ob.Oracle(c, macro_flux=True)
+    for _ in range(6):
+        orc.evolution(c.dt)
+    for s in shards:
+        e_plain = ob.macro_errors(s.macros(), plain.macros(), c.gas["R"])
+        assert max(e_plain.values()) <= 1e-12, e_plain
+        e_orc = ob.macro_errors(s.macros(), orc.macros(), c.gas["R"])
+        assert max(e_orc.values()) <= 1e-10, e_orc
+
+
+def test_velocity_mesh_macro_flux_nccl_one_rank_is_the_unsharded_step():
+    c = _vmesh_cavity()
+    a = dl.Solver(c, macro_flux=True, shard=dl.shard(0, 1, dl.nccl_unique_id()), dv_chunks=3)
+    b = dl.Solver(c, macro_flux=True, dv_chunks=3)
+    a.step(5, c.dt)
+    b.step(5, c.dt)
+    for k in ("rho", "U", "T", "q"):
+        assert np.array_equal(a.macros()[k], b.macros()[k]), k
