@@ -418,6 +418,7 @@ struct FInBy {
 // and Shakhov constants once for the chunk's DVs
 struct FHalf {
     View v;
+    static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
         const double* m = v.cm + 9 * static_cast<size_t>(c);
@@ -469,6 +470,7 @@ struct FGrad {
 // 3: face values at the half step (wall incoming DVs come in stage 5)
 struct FFace {
     View v;
+    static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int i = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const double* xi = v.xi + 3 * i;
@@ -555,6 +557,7 @@ struct FWallIn {
 // 6: raw moments of the face values, per DV chunk (slots 0..13)
 struct FFaceMom {
     View v;
+    static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         double m[14] = {0};
@@ -581,6 +584,7 @@ struct FFaceMac {
 // raw moments of the state, per DV chunk, and the cell macro records
 struct FCellMom {
     View v;
+    static constexpr int kMinCtas = 3;  // 24 warps per SM: at most 80 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
         double m[14] = {0};
@@ -672,6 +676,7 @@ struct FBoundaryFlux {
 // sums per DV chunk, and the objective
 struct RRelax {
     View v;
+    static constexpr int kMinCtas = 2;  // 16 warps per SM: at most 128 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const bool bnd = f >= v.nIF;
@@ -761,6 +766,7 @@ struct RFaceMac {
 // U_b or the owner U (2..4)
 struct RFaceMom {
     View v;
+    static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
     ADJ_HD void operator()(int64_t idx) const {
         const int ch = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const double* co = v.fco + kCo * static_cast<size_t>(f);
@@ -885,7 +891,7 @@ struct RGradAdj {
 struct RHalf {
     View v;
     static constexpr int kRegF = 6;
-    static constexpr int kMinCtas = 2;  // 16 warps per SM
+    static constexpr int kMinCtas = 2;  // 16 warps per SM: at most 128 registers
     ADJ_HD void face_add(size_t cb, size_t n, int f, int o, bool is_nei, const double* gc, const double* hc,
                          double& abg, double& abh) const {
         const size_t io = cb + o;
