@@ -219,6 +219,20 @@ def cavity_case(n: int = 61, n_dv: int = 28, kn: float = 0.075, u_lid: float = 5
     return c.flatten(geometry) if flatten else c
 
 
+def refined_cavity_case(n: int = 8, n_dv: int = 8, kn: float = 0.075, u_lid: float = 50.0, T_wall: float = 273.0,
+                        T0: float = 273.0, flatten: bool = True, geometry=None) -> Case:
+    """The cavity of cavity_case on meshgen.refined_cavity(n): 2:1 refined
+    squares beside octagons with eight internal faces."""
+    c = cavity_case(2, n_dv, kn=kn, u_lid=u_lid, T_wall=T_wall, T0=T0, flatten=False)
+    c.mesh = meshgen.refined_cavity(n)
+    nc = c.mesh.n_cells
+    c.name = f"refined_cavity{n}x{n}_dv{n_dv}"
+    c.rho0 = np.full(nc, float(c.rho0[0]))
+    c.U0 = np.zeros((nc, 3))
+    c.T0 = np.full(nc, float(c.T0[0]))
+    return c.flatten(geometry) if flatten else c
+
+
 def channel_case(nx: int = 24, ny: int = 12, n_dv: int = 16, sides: dict | None = None, kn: float = 0.1,
                  T0: float = 273.0, U0: tuple = (0.0, 0.0, 0.0), flatten: bool = True, geometry=None) -> Case:
     """2-D channel [0, 2] x [0, 1] of argon at rest (or U0); ``sides`` maps

@@ -16,6 +16,11 @@ Workloads:
   between spheres of radius r0 and r1, equiangular cube-face mapping and
   geometric radial stretching; patches ``wall`` (r = r0) and ``farField``
   (r = r1).
+* ``refined_cavity(n)`` -- the cavity's domain as n x n squares of which
+  every other one (checkerboard) is split into 2 x 2: the unsplit squares
+  are octagons with a hanging node on every side, so an interior one has
+  eight internal faces (ten with front and back), as a 2:1 refined
+  OpenFOAM mesh has.
 """
 from __future__ import annotations
 
@@ -131,6 +136,100 @@ def hexes_to_polymesh(points: np.ndarray, cells: np.ndarray, classify, patch_def
                     face_points=allv.reshape(-1).astype(np.int64), owner=owner.astype(np.int64),
                     neighbour=nei.astype(np.int64), n_cells=nc, patches=patches,
                     n_solution_dims=n_solution_dims)
+
+
+def polygons_to_polymesh(points2d: np.ndarray, cells: list, classify, patch_defs: list[tuple[str, str]],
+                         thickness: float = 0.1) -> PolyMesh:
+    """Build a one-cell-thick 2-D polyMesh from polygon cells.
+
+    ``cells[c]`` lists cell c's vertices (indices into ``points2d``)
+    counter-clockwise; neighbouring cells must share whole edges.  Every
+    edge becomes a quad face extruded to ``thickness``; each cell also gets
+    a front (z = 0) and a back (z = thickness) face, both classified like
+    the edge faces: ``classify(face_centres) -> patch index`` of
+    ``patch_defs``.
+    """
+    pts2 = np.asarray(points2d, dtype=np.float64)
+    npt = len(pts2)
+    points = np.concatenate([np.column_stack([pts2, np.zeros(npt)]),
+                             np.column_stack([pts2, np.full(npt, thickness)])])
+    edge_cell = {}
+    internal, boundary = [], []
+    for c, poly in enumerate(cells):
+        for k in range(len(poly)):
+            a, b = int(poly[k]), int(poly[(k + 1) % len(poly)])
+            if (b, a) in edge_cell:
+                o = edge_cell.pop((b, a))
+                # the owner is the lower cell; the face keeps the owner's
+                # counter-clockwise edge direction, so its normal leaves the owner
+                if o[0] < c:
+                    internal.append((o[0], c, o[1], o[2]))
+                else:
+                    internal.append((c, o[0], a, b))
+            else:
+                edge_cell[(a, b)] = (c, a, b)
+    for (a, b), (c, _, _) in edge_cell.items():
+        boundary.append((c, [a, b, b + npt, a + npt]))
+    for c, poly in enumerate(cells):
+        boundary.append((c, [int(v) for v in poly[::-1]]))          # front, normal -z
+        boundary.append((c, [int(v) + npt for v in poly]))          # back, normal +z
+    internal.sort(key=lambda f: (f[0], f[1]))
+    faces = [[a, b, b + npt, a + npt] for (_, _, a, b) in internal]
+    owner = [f[0] for f in internal]
+    neighbour = [f[1] for f in internal]
+    bcent = np.array([points[fv].mean(axis=0) for _, fv in boundary])
+    pid = np.asarray(classify(bcent), dtype=np.int64)
+    if np.any((pid < 0) | (pid >= len(patch_defs))):
+        raise ValueError("unclassified boundary faces")
+    patches = []
+    for k, (name, ptype) in enumerate(patch_defs):
+        sel = sorted(np.nonzero(pid == k)[0], key=lambda i: boundary[i][0])
+        patches.append({"name": name, "type": ptype, "startFace": len(faces), "nFaces": len(sel)})
+        for i in sel:
+            owner.append(boundary[i][0])
+            faces.append(boundary[i][1])
+    offs = np.concatenate([[0], np.cumsum([len(f) for f in faces])]).astype(np.int64)
+    return PolyMesh(points=np.ascontiguousarray(points), face_offsets=offs,
+                    face_points=np.concatenate(faces).astype(np.int64), owner=np.asarray(owner, dtype=np.int64),
+                    neighbour=np.asarray(neighbour, dtype=np.int64), n_cells=len(cells), patches=patches,
+                    n_solution_dims=2)
+
+
+def refined_cavity(n: int, thickness: float = 0.1) -> PolyMesh:
+    """[0,1]^2 x [0, thickness] as n x n squares, those with i + j even split
+    into 2 x 2; the others are octagons through the midpoints of their
+    sides.  Patches as ``cavity``: movingWall (y = 1), fixedWalls,
+    frontAndBack (empty)."""
+    m = 2 * n + 1                                   # lattice of half squares
+
+    def pid(i, j):
+        return j * m + i
+
+    X, Y = np.meshgrid(np.linspace(0.0, 1.0, m), np.linspace(0.0, 1.0, m))
+    pts = np.column_stack([X.ravel(), Y.ravel()])
+    cells = []
+    for j in range(n):
+        for i in range(n):
+            I, J = 2 * i, 2 * j
+            if (i + j) % 2 == 0:
+                for dj in (0, 1):
+                    for di in (0, 1):
+                        a, b = I + di, J + dj
+                        cells.append([pid(a, b), pid(a + 1, b), pid(a + 1, b + 1), pid(a, b + 1)])
+            else:
+                cells.append([pid(I, J), pid(I + 1, J), pid(I + 2, J), pid(I + 2, J + 1), pid(I + 2, J + 2),
+                              pid(I + 1, J + 2), pid(I, J + 2), pid(I, J + 1)])
+    tol = 1e-9
+
+    def classify(c):
+        out = np.full(len(c), 1, dtype=np.int64)       # fixedWalls
+        out[np.abs(c[:, 1] - 1.0) < tol] = 0           # movingWall
+        out[(np.abs(c[:, 2]) < tol) | (np.abs(c[:, 2] - thickness) < tol)] = 2
+        return out
+
+    return polygons_to_polymesh(pts, cells, classify,
+                                [("movingWall", "wall"), ("fixedWalls", "wall"), ("frontAndBack", "empty")],
+                                thickness)
 
 
 def _box_hexes(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float):

@@ -67,13 +67,19 @@ def _vmesh_cavity():
     return c.flatten()
 
 
-@pytest.mark.parametrize("which", ["ball3d", "vmesh"])
+@pytest.mark.parametrize("which", ["ball3d", "vmesh", "refined"])
 def test_adjoint_matches_tangent_in_3d_and_on_a_velocity_mesh(which):
     """The 3-D far-field ball (cubed sphere 6x4x4x4, 6^3 DVs; objective: energy
-    flux through every face, drag through the sphere) and a cavity on a
-    jittered unstructured velocity mesh (100 DVs): tangent = projected
-    adjoint to 1e-9."""
-    c = cs.ball_case(4, 4, 1.12, 6, kn=0.1, mach=0.5) if which == "ball3d" else _vmesh_cavity()
+    flux through every face, drag through the sphere), a cavity on a
+    jittered unstructured velocity mesh (100 DVs) and a 2:1 refined cavity
+    whose octagon cells have eight internal faces (more than the reverse
+    keeps in registers): tangent = projected adjoint to 1e-9."""
+    if which == "ball3d":
+        c = cs.ball_case(4, 4, 1.12, 6, kn=0.1, mach=0.5)
+    elif which == "vmesh":
+        c = _vmesh_cavity()
+    else:
+        c = cs.refined_cavity_case(6, 8, kn=0.1)
     hw, fw, _ = ac.objective_weights(c)
     r = dl.Solver(c, tile_cells=32).adjoint(4, c.dt, hw, fw, max_snapshots=2)
     Jt, _, _, _ = ob.Oracle(c).tangent(4, c.dt, hw, fw)

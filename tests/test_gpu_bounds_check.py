@@ -51,6 +51,11 @@ def test_checked_ball_far_field():
     _same(cs.ball_case(4, 4, 1.12, 8, kn=0.1, mach=0.5), 3)
 
 
+def test_checked_refined_cavity():
+    # octagon cells: the general stencil and flux-list paths
+    _same(cs.refined_cavity_case(6, 8), 3, tile_cells=12, dv_chunks=2)
+
+
 def test_checked_demo_cavity():
     _same(golden_cases.demo_cavity(), 2)
 

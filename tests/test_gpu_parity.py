@@ -76,6 +76,17 @@ def test_cavity_newton_cotes_parallel_faces():
     _run(c, 6, tile_cells=11, dv_chunks=3)
 
 
+@pytest.mark.parametrize("tile_cells,dv_chunks", [(0, 0), (16, 3)])
+def test_refined_cavity_octagon_cells(tile_cells, dv_chunks):
+    # 2:1 refined squares beside octagons with eight internal faces (ten in
+    # all): more neighbours than the gradient stencil and more faces than the
+    # flux list hold in registers, so the passes take their general paths
+    c = cs.refined_cavity_case(8, 8)
+    _run(c, 20, tile_cells=tile_cells, dv_chunks=dv_chunks)
+    _run(c, 8, tol=TOL32, check_faces=False, floor=1e-2, precision=dl.FP32C, tile_cells=tile_cells,
+         dv_chunks=dv_chunks)
+
+
 def test_cube_fp64_multi_tile():
     c = cs.cube_case(6, 6, kn=0.1)
     _run(c, 6, tile_cells=16, dv_chunks=2)

@@ -21,8 +21,9 @@ def _check_topology(pm):
     return g
 
 
-@pytest.mark.parametrize("pm", [meshgen.cavity(7), meshgen.cube(4), meshgen.cubed_sphere(4, 3)],
-                         ids=["cavity", "cube", "sphere"])
+@pytest.mark.parametrize("pm", [meshgen.cavity(7), meshgen.cube(4), meshgen.cubed_sphere(4, 3),
+                                meshgen.refined_cavity(5)],
+                         ids=["cavity", "cube", "sphere", "refined"])
 def test_generators_and_geometry(pm):
     g = _check_topology(pm)
     p = dl.mesh_geometry(pm)
@@ -54,3 +55,23 @@ def test_cubed_sphere_counts():
     r = meshgen.radial_stations(32, 1.12, 1.0, 10.0)
     assert abs(r[0] - 1) < 1e-15 and abs(r[-1] - 10) < 1e-12
     assert np.allclose(np.diff(r)[1:] / np.diff(r)[:-1], 1.12)
+
+
+def test_refined_cavity_cells_and_faces():
+    # n x n squares, every other one split into 2 x 2: 4 fine cells per split
+    # square; an interior octagon has eight internal faces, and with front and
+    # back ten faces in all
+    n = 6
+    pm = meshgen.refined_cavity(n)
+    split = sum((i + j) % 2 == 0 for i in range(n) for j in range(n))
+    assert pm.n_cells == 4 * split + (n * n - split)
+    nif = pm.n_internal_faces
+    internal = np.bincount(np.concatenate([pm.owner[:nif], pm.neighbour]), minlength=pm.n_cells)
+    faces = np.bincount(pm.owner, minlength=pm.n_cells) + np.bincount(pm.neighbour, minlength=pm.n_cells)
+    assert internal.max() == 8 and faces.max() == 10
+    g = _check_topology(pm)
+    assert abs(g["V"].sum() - 0.1) < 1e-14
+    # the octagons keep the square's centroid
+    octagon = np.nonzero(internal == 8)[0]
+    c = g["C"][octagon, :2] * n
+    assert np.max(np.abs(c - (np.floor(c) + 0.5))) < 1e-12
