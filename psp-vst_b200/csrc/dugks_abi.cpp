@@ -233,6 +233,16 @@ static int create_impl(const dugks_mesh* mesh, const dugks_dv_set* dv, const dug
             h->bface_patch_local[b] = b - h->patch_start[p];
         }
     }
+    // the boundary relaxation of h takes the internal-face temperature at the
+    // face's patch-local index (fvDVM.C:1367, :1413; macroFlux the internal
+    // Sf there, :1668-1669); a patch with more faces than the mesh has
+    // internal faces would read past them, which the reference leaves undefined
+    for (int p = 0; p < h->nP; ++p)
+        if (h->patch_start[p + 1] - h->patch_start[p] > nIF)
+            return fail(DUGKS_ERR_UNSUPPORTED,
+                        "dugks_create: patch " + std::to_string(p) + " has " +
+                            std::to_string(h->patch_start[p + 1] - h->patch_start[p]) + " faces, more than the " +
+                            std::to_string(nIF) + " internal faces its patch-local indices address");
     if (nBF > 0 && (!bc->rho || !bc->U || !bc->T)) return fail(DUGKS_ERR_ARG, "dugks_create: missing BC values");
     h->bc_rho.assign(bc->rho, bc->rho + nBF);
     h->bc_U.assign(bc->U, bc->U + 3 * static_cast<size_t>(nBF));

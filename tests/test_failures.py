@@ -22,8 +22,9 @@ from dugks_b200 import lib as dl
 ERR_ARG, ERR_NAN = 1, 5
 
 
-def _create(fl, n_cells, **over):
-    """dugks_create on the flattened arrays of a case, with some replaced."""
+def _create(fl, n_cells, dvs=None, **over):
+    """dugks_create on the flattened arrays of a case, with some replaced
+    (dvs: a 1-D DV set (xis, weights, xi_max) instead of the case's)."""
     lib = dl.load()
     a = {k: np.ascontiguousarray(v) for k, v in fl.items() if isinstance(v, np.ndarray)}
     a.update({k: np.ascontiguousarray(v) for k, v in over.items()})
@@ -31,8 +32,9 @@ def _create(fl, n_cells, **over):
                    dl.ptr(a["neighbour"], C.c_int64), dl.ptr(a["C"]), dl.ptr(a["V"]), dl.ptr(a["Cf"]),
                    dl.ptr(a["Sf"]), len(a["patch_type"]), dl.ptr(a["patch_start"], C.c_int32))
     c = cs.cavity_case(4, 6)
-    xis, ws = np.ascontiguousarray(c.xis), np.ascontiguousarray(c.weights)
-    dv = dl.DVSet(len(xis), dl.ptr(xis), dl.ptr(ws), c.xi_max)
+    x, w, xmax = dvs if dvs is not None else (c.xis, c.weights, c.xi_max)
+    xis, ws = np.ascontiguousarray(x, dtype=np.float64), np.ascontiguousarray(w, dtype=np.float64)
+    dv = dl.DVSet(len(xis), dl.ptr(xis), dl.ptr(ws), xmax)
     gas = dl.Gas(c.gas["R"], c.gas["omega"], c.gas["Tref"], c.gas["muRef"], c.gas["Pr"], 0)
     bc = dl.BC(dl.ptr(a["patch_type"], C.c_int32), dl.ptr(a["rho_b"]), dl.ptr(a["U_b"]), dl.ptr(a["T_b"]))
     h = C.c_void_p()
@@ -45,6 +47,25 @@ def _create(fl, n_cells, **over):
 def _flat():
     c = cs.cavity_case(4, 6)
     return c.flat, c.n_cells
+
+
+def test_more_than_64_nodes_per_dimension_is_refused():
+    fl, n = _flat()
+    x = np.linspace(-2400.0, 2400.0, 65)
+    st, msg = _create(fl, n, dvs=(x, np.full(65, x[1] - x[0]), 2400.0))
+    assert (st, msg) == (7, "dugks_create: more than 64 DV nodes per dimension")
+
+
+@pytest.mark.parametrize("n", [1, 2])
+def test_patch_larger_than_the_internal_faces_is_refused(n):
+    # the boundary relaxation reads the internal-face T at each face's
+    # patch-local index (fvDVM.C:1367): a 1 x 1 cavity has no internal face, a
+    # 2 x 2 one 4 internal faces and 6 fixed-wall faces
+    c = cs.cavity_case(n, 6, flatten=False)
+    c.dt = 1e-5
+    c.flatten()
+    st, msg = _create(c.flat, c.n_cells)
+    assert st == 7 and "more than the" in msg, (st, msg)
 
 
 def test_neighbour_out_of_range_is_refused():

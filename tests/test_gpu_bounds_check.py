@@ -56,6 +56,16 @@ def test_checked_refined_cavity():
     _same(cs.refined_cavity_case(6, 8), 3, tile_cells=12, dv_chunks=2)
 
 
+def test_checked_largest_dv_rows():
+    # 64 nodes per dimension (2-D and 3-D)
+    for c in (cs.cavity_case(4, 8, flatten=False), cs.cube_case(3, 8, flatten=False)):
+        x = np.linspace(-2400.0, 2400.0, 64)
+        w = np.full(64, x[1] - x[0])
+        w[0] = w[-1] = 0.5 * w[0]
+        c.xis, c.weights, c.xi_max = x, w, 2400.0
+        _same(c.flatten(), 2)
+
+
 def test_checked_demo_cavity():
     _same(golden_cases.demo_cavity(), 2)
 

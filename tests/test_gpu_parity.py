@@ -87,6 +87,27 @@ def test_refined_cavity_octagon_cells(tile_cells, dv_chunks):
          dv_chunks=dv_chunks)
 
 
+def _uniform_dvs(c, n, xi_max):
+    """n uniform nodes per dimension on [-xi_max, xi_max], trapezoid weights."""
+    x = np.linspace(-xi_max, xi_max, n)
+    w = np.full(n, x[1] - x[0])
+    w[0] = w[-1] = 0.5 * w[0]
+    c.xis, c.weights, c.xi_max = x, w, xi_max
+    return c.flatten()
+
+
+@pytest.mark.parametrize("which", ["cavity", "cube"])
+def test_largest_dv_rows(which):
+    # 64 nodes per dimension, the most the passes' DV tables hold: 4,096 DVs
+    # on a 4 x 4 cavity, 262,144 on a 3^3 cube (g only there)
+    if which == "cavity":
+        c = _uniform_dvs(cs.cavity_case(4, 8, flatten=False), 64, 2400.0)
+        _run(c, 6)
+        _run(c, 6, tol=TOL32, check_faces=False, floor=1e-2, precision=dl.FP32C)
+    else:
+        _run(_uniform_dvs(cs.cube_case(3, 8, flatten=False), 64, 2400.0), 3)
+
+
 def test_cube_fp64_multi_tile():
     c = cs.cube_case(6, 6, kn=0.1)
     _run(c, 6, tile_cells=16, dv_chunks=2)
