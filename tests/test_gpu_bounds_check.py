@@ -18,6 +18,7 @@ import pytest
 import golden_cases
 from dugks_b200 import case as cs
 from dugks_b200 import lib as dl
+from dugks_b200 import meshgen
 
 pytestmark = pytest.mark.gpu
 
@@ -52,8 +53,12 @@ def test_checked_ball_far_field():
 
 
 def test_checked_refined_cavity():
-    # octagon cells: the general stencil and flux-list paths
+    # octagon cells: the general stencil and flux-list paths, of the factored
+    # passes and of the DV-list passes
     _same(cs.refined_cavity_case(6, 8), 3, tile_cells=12, dv_chunks=2)
+    c = cs.refined_cavity_case(6, 8, flatten=False)
+    c.use_velocity_mesh(meshgen.velocity_box(8, 1600.0, 2, jitter=0.2))
+    _same(c.flatten(), 3, tile_cells=12, dv_chunks=2)
 
 
 def test_checked_largest_dv_rows():

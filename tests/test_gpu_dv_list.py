@@ -61,6 +61,15 @@ def test_jittered_velocity_mesh_3d_far_field_ball():
     _parity(c, 6, tile_cells=32, dv_chunks=3)
 
 
+def test_velocity_mesh_on_octagon_cells():
+    # the general-DV passes on a 2:1 refined cavity: octagons with eight
+    # internal faces take their stencil and flux-list fallbacks
+    c = cs.refined_cavity_case(6, 8, flatten=False)
+    c.use_velocity_mesh(meshgen.velocity_box(8, 1600.0, 2, jitter=0.2))
+    c.flatten()
+    _parity(c, 8, tile_cells=12, dv_chunks=2)
+
+
 def test_fp32c_velocity_mesh():
     _parity(_vmesh_cavity(), 8, tol=5e-6, floor=1e-2, precision=dl.FP32C)
 
