@@ -24,6 +24,7 @@ struct StepArgs {
     int wideA16;                 // g-only pass A in batches of 16 DVs (16 nodes per dimension)
     int wideB16;                 // g-only pass B likewise (FP32 storage)
     int row10;                   // g-only passes in batches of 10 DVs (20 nodes per dimension)
+    int row20;                   // FP32 storage: g-only passes in batches of a whole 20-node row
     int fullA, fullB;            // 1: every DV row splits into whole batches
     size_t smemA, smemB;         // dynamic shared memory of the passes
 };

@@ -1245,6 +1245,14 @@ cudaError_t launch_nb_h(const StepArgs& a, bool pass_b, cudaStream_t s) {
                 return cudaGetLastError();
             }
         }
+        if constexpr (sizeof(Real) == 4) {
+            // FP32 storage, 20 nodes per dimension: a whole row per batch
+            if (a.row20) {
+                if (!pass_b) k_pass_a<D, Real, 20, true, true><<<grid, kThreads, a.smemA, s>>>(a);
+                else k_pass_b<D, Real, 20, true, true><<<grid, kThreads, a.smemB, s>>>(a);
+                return cudaGetLastError();
+            }
+        }
         // 20 nodes per dimension: two batches of 10 per row (guarded: 10 DVs
         // do not split evenly over the threads of a cell)
         if (a.row10) {
@@ -1312,6 +1320,9 @@ cudaError_t configure_nb(const StepArgs& a, bool pass_b) {
         if constexpr (sizeof(Real) == 4) {
             if (e == cudaSuccess && pass_b)
                 e = set_smem(k_pass_b<D, Real, 16, true, true>, SmemB<Real, 16, true>::bytes());
+            if (e == cudaSuccess)
+                e = pass_b ? set_smem(k_pass_b<D, Real, 20, true, true>, SmemB<Real, 20, true>::bytes())
+                           : set_smem(k_pass_a<D, Real, 20, true, true>, SmemA<D, Real, 20, true>::bytes());
         }
     }
     return e;
@@ -1372,12 +1383,20 @@ void pass_config(int D, int precision, int n1d, StepArgs* a) {
     // g-only pass A in batches of 16 DVs (a whole row) for 16 nodes per
     // dimension: half the per-batch work and barriers per DV, and the
     // shared memory the h arrays would take holds the wider batch
-    a->wideA16 = a->wideB16 = a->row10 = 0;
+    a->wideA16 = a->wideB16 = a->row10 = a->row20 = 0;
     if (D == 3 && a->hzero && n1d == 20) {
-        // both passes in batches of 10 DVs: two per row instead of 8 + 8 + 4
-        a->row10 = 1;
-        a->smemA = f64 ? SmemA<3, double, 10, true>::bytes() : SmemA<3, float, 10, true>::bytes();
-        a->smemB = f64 ? SmemB<double, 10, true>::bytes() : SmemB<float, 10, true>::bytes();
+        if (f64) {
+            // both passes in batches of 10 DVs: two per row instead of 8 + 8 + 4
+            a->row10 = 1;
+            a->smemA = SmemA<3, double, 10, true>::bytes();
+            a->smemB = SmemB<double, 10, true>::bytes();
+        } else {
+            // FP32 storage: a whole row per batch (the 20-wide FP64 staging
+            // does not fit in shared memory)
+            a->row20 = 1;
+            a->smemA = SmemA<3, float, 20, true>::bytes();
+            a->smemB = SmemB<float, 20, true>::bytes();
+        }
     }
     if (D == 3 && a->hzero && n1d == 16) {
         a->wideA16 = 1;

@@ -75,7 +75,8 @@ def test_nonzero_h_state_leaves_g_only_passes():
 @pytest.mark.parametrize("precision", [dl.FP64, dl.FP32C])
 def test_g_only_passes_twenty_nodes(precision):
     # 20 nodes per dimension (the mixed-precision configuration's DV set):
-    # the g-only passes in batches of 10 DVs
+    # the g-only passes in batches of 10 DVs (FP64) or of a whole row (FP32
+    # storage)
     c = cs.cube_case(4, 20, kn=0.1)
     gpu, orc = dl.Solver(c, precision=precision), ob.Oracle(c)
     gpu.step(4, c.dt)
