@@ -330,18 +330,26 @@ template <typename Real, int NB, bool HZ = false>
 struct SmemB {
     // DF arrays per item: g and h, or g alone when h is identically zero
     static constexpr int NH = HZ ? 1 : 2;
+    // rows of stx: e_x of the items does not depend on the row, so a DV set
+    // of at most XR nodes per dimension keeps the whole table [n1d][kSI],
+    // loaded once per CTA; larger sets stage [NB][kSI] per batch.  Where h is
+    // identically zero, 8-DV batches keep 16 rows in the shared memory h
+    // would take (16- and 20-wide batches hold a whole row already; for
+    // 10-DV batches on 20-node sets the resident table measured slower than
+    // staging)
+    static constexpr int XR = (HZ && 2 * NB <= 16) ? 2 * NB : NB;
     double* x1;
     double* w1;
     double* frec;  // [CR_N][kSI] face records of the items
     double* crec;  // [CR_N][kS0] records of the L0 cells
-    double* stx;   // [NB][kSI] staged e_x of the items
+    double* stx;   // [XR][kSI] e_x of the items: the resident table, or staged per batch
     Real* st;      // [NH][NB][kSI] staged face values g (and h) of the items
     Real* Fg;      // [NB][kSI] fluxes xi.S g_f of the items
     Real* Fh;      // (null when h is identically zero)
     double* red;   // end-of-CTA reduction of the split cell moments (aliases stx and st)
     static constexpr size_t bytes() {
         return 2 * kMaxN1d * sizeof(double) +
-               (static_cast<size_t>(CR_N) * (kSI + kS0) + static_cast<size_t>(NB) * kSI) * sizeof(double) +
+               (static_cast<size_t>(CR_N) * (kSI + kS0) + static_cast<size_t>(XR) * kSI) * sizeof(double) +
                2 * NH * static_cast<size_t>(NB) * kSI * sizeof(Real);
     }
 };
@@ -355,7 +363,7 @@ __device__ __forceinline__ SmemB<Real, NB, HZ> carve_b(unsigned char* base) {
     s.frec = s.w1 + kMaxN1d;
     s.crec = s.frec + CR_N * kSI;
     s.stx = s.crec + CR_N * kS0;
-    s.st = reinterpret_cast<Real*>(s.stx + NB * kSI);
+    s.st = reinterpret_cast<Real*>(s.stx + S::XR * kSI);
     s.Fg = s.st + S::NH * NB * kSI;
     s.Fh = HZ ? nullptr : s.Fg + NB * kSI;
     s.red = s.stx;
@@ -924,7 +932,7 @@ __device__ __forceinline__ float flip_sign(float v, unsigned neg) {
 template <typename Real, int NB, bool FULL, bool HZ>
 __device__ __forceinline__ void stage_items(const SmemB<Real, NB, HZ>& sm, const BatchPos& bp, const Real* __restrict__ fvg,
                                             const Real* __restrict__ fvh, const double* __restrict__ ftab, size_t nI,
-                                            int it, int gi) {
+                                            int it, int gi, bool x_res) {
     const size_t base = static_cast<size_t>(bp.d0) * nI + gi;
     const size_t tb = static_cast<size_t>(bp.ix0) * nI + gi;
 #pragma unroll
@@ -932,7 +940,7 @@ __device__ __forceinline__ void stage_items(const SmemB<Real, NB, HZ>& sm, const
         if (FULL || j < bp.nb) {
             cp_async(sm.st + j * kSI + it, fvg + base + j * nI);
             if (!HZ) cp_async(sm.st + (NB + j) * kSI + it, fvh + base + j * nI);
-            cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
+            if (!x_res) cp_async(sm.stx + j * kSI + it, ftab + tb + j * nI);
         }
     }
     cp_commit();
@@ -990,6 +998,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
         for (int q = 0; q < 3; ++q) S[q] = __ldg(m.it_geo + q * nI + gi);
         stash_rec(sm.frec, kSI, it, a.ds.facerec, nI, gi);
     }
+    // e_x of this thread's item for every node, when the table fits (each
+    // thread reads back only its own item's column)
+    // (a variant whose table is only a batch wide stages: decided at compile time)
+    constexpr int kXR = SmemB<Real, NB, HZ>::XR;
+    const bool x_res = (kXR > NB || NB >= 16) && m.n1d <= kXR;
+    if (x_res && has_item)
+        for (int ix = 0; ix < m.n1d; ++ix) sm.stx[ix * kSI + it] = __ldg(ftab + static_cast<size_t>(ix) * nI + gi);
     // L0 cell of stage 4 (kParts0 threads per cell, DVs interleaved)
     const int lc = threadIdx.x % kS0, part = threadIdx.x / kS0;
     const bool has_cell = lc < t.n0;
@@ -1023,7 +1038,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
     BatchWalk<D, NB> walk(t.r0, m.n1d, m.row_base), ahead(t.r0, m.n1d, m.row_base);
     const int nbt = (t.r1 - t.r0) * walk.nbr;
     if (nbt > 0) {
-        if (has_item) stage_items<Real, NB, FULL, HZ>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi);
+        if (has_item) stage_items<Real, NB, FULL, HZ>(sm, walk.pos(), fvg, fvh, ftab, nI, it, gi, x_res);
         if (has_cell) fetch_cells<Real, NB, FULL, HZ>(walk.pos(), g, h, ctab, nC, c, part, pg, ph, pe);
     }
     for (int k = 0; k < nbt; ++k, walk.next()) {
@@ -1038,7 +1053,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
             const double ey = __ldg(ftab + static_cast<size_t>(m.n1d + bp.iy) * nI + gi);
             const double ez = D == 3 ? __ldg(ftab + static_cast<size_t>(2 * m.n1d + bp.iz) * nI + gi) : 1.0;
             const Shk<double> fs = shk_from<D, double>(sm.frec, kSI, it, q, ey, ez);
-            const double* sx = sm.stx + it;
+            const double* sx = sm.stx + (x_res ? bp.ix0 * kSI : 0) + it;
             cp_wait_all();  // this item's staged entries of batch k
             const Real* sg = sm.st + it;
             if (kind != ITEM_MESH_BOUNDARY) {
@@ -1135,7 +1150,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_b(const StepArgs a) {
                 }
             }
             // this thread has read its staged entries: stage the next batch
-            if (k + 1 < nbt) stage_items<Real, NB, FULL, HZ>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi);
+            if (k + 1 < nbt) stage_items<Real, NB, FULL, HZ>(sm, ahead.pos(), fvg, fvh, ftab, nI, it, gi, x_res);
         }
         __syncthreads();
         // stage 4: g~ <- -g~/3 + 4/3 gbar+ - dt/V sum_f (+-)(xi.S) g_f, cell moments
