@@ -1395,6 +1395,19 @@ void pass_config(int D, int precision, int n1d, StepArgs* a) {
         if (D == 3) smem_d<3, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
         else smem_d<2, float>(a->wideA, a->wideB, &a->smemA, &a->smemB);
     }
+    // the g-only instantiations' own sizes (no h arrays; pass B keeps its
+    // items' e_x table resident in part of that room)
+    if (D == 3 && a->hzero) {
+        using WD = Width<double>;
+        using WF = Width<float>;
+        if (f64) {
+            a->smemA = a->wideA ? SmemA<3, double, WD::A1, true>::bytes() : SmemA<3, double, WD::A0, true>::bytes();
+            a->smemB = a->wideB ? SmemB<double, WD::B1, true>::bytes() : SmemB<double, WD::B0, true>::bytes();
+        } else {
+            a->smemA = a->wideA ? SmemA<3, float, WF::A1, true>::bytes() : SmemA<3, float, WF::A0, true>::bytes();
+            a->smemB = a->wideB ? SmemB<float, WF::B1, true>::bytes() : SmemB<float, WF::B0, true>::bytes();
+        }
+    }
     // g-only pass A in batches of 16 DVs (a whole row) for 16 nodes per
     // dimension: half the per-batch work and barriers per DV, and the
     // shared memory the h arrays would take holds the wider batch
