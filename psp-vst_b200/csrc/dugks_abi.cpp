@@ -1482,4 +1482,17 @@ int rebuild_cell_records(dugks_handle* h) {
     return DUGKS_OK;
 }
 
+int record_face_values(dugks_handle* h, double dt) {
+    const StepArgs a = make_args(h, dt, 0.0);
+    int launches = 0;
+    if (h->cellrec_dt != dt) {
+        CUDA_TRY(h, launch_cell_prep(a, h->stream));
+        ++launches;
+        h->cellrec_dt = dt;   // the relax factors are now dt's
+    }
+    CUDA_TRY(h, launch_stage(a, h->precision, STAGE_PASS_A, h->stream, &launches));
+    h->launches += launches;
+    return DUGKS_OK;
+}
+
 }  // namespace dugks

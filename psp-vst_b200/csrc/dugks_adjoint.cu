@@ -60,6 +60,8 @@ struct GpuEx {
         ADJ_TRY(h, cudaGetLastError());
         return DUGKS_OK;
     }
+    // the tiled pass A of the recorded step, into the handle's face-value buffer
+    int pass_a(const adj::View& v) { return dugks::record_face_values(h, v.dt); }
 };
 
 // device allocations of one run, freed together
@@ -262,8 +264,11 @@ int prepare(dugks_handle* h, const dugks_objective* obj, const char* who, Arena&
     v.brho = d_brho;
     v.ha = d_ha;
     v.fw = d_fw;
-    if ((st = ar.get(h, &v.gbp, nvc)) || (st = ar.get(h, &v.hbp, nvc)) || (st = ar.get(h, &v.Gg, 3 * nvc)) ||
-        (st = ar.get(h, &v.Gh, 3 * nvc)) || (st = ar.get(h, &v.fg, nvf)) || (st = ar.get(h, &v.fh, nvf)) ||
+    v.fvg = static_cast<const double*>(h->ds.fvg);
+    v.fvh = static_cast<const double*>(h->ds.fvh);
+    v.fitems = h->dm.face_items;
+    v.nI = h->dm.n_items;
+    if ((st = ar.get(h, &v.fg, nvf)) || (st = ar.get(h, &v.fh, nvf)) ||
         (st = ar.get(h, &v.pf, static_cast<size_t>(v.nchF) * nF * adj::kP)) || (st = ar.get(h, &v.rhow, nBF)) ||
         (st = ar.get(h, &v.inby, nBF)) || (st = ar.get(h, &v.fmac, static_cast<size_t>(nF) * adj::kMac)) ||
         (st = ar.zeros(h, &v.Jb, nBF)))

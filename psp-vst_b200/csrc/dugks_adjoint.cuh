@@ -91,11 +91,13 @@ struct View {
     const double* g;        // [nv][nC]
     const double* h;
     const double* cm;       // [nC][9] rho U T q tau the step starts from
+    // the tiled pass A's face-value buffer [nv][n_items] and the items of
+    // every face ([nF][2], -1: none), from which the record takes its face values
+    const double* fvg;
+    const double* fvh;
+    const int32_t* fitems;
+    int64_t nI;
     // forward record of the step
-    double* gbp;            // [nv][nC]
-    double* hbp;
-    double* Gg;             // [3][nv][nC]
-    double* Gh;
     double* fg;             // [nv][nF] face values before the relaxation
     double* fh;
     double* pf;             // [nchF][nF][kP]
@@ -414,60 +416,13 @@ struct FInBy {
     }
 };
 
-// 1: gbar+ and hbar+ per (cell, DV chunk): the cell's record, relax factor
-// and Shakhov constants once for the chunk's DVs
-struct FHalf {
-    View v;
-    static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
-    ADJ_HD void operator()(int64_t idx) const {
-        const int ch = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const double* m = v.cm + 9 * static_cast<size_t>(c);
-        const double tau = tau_of(v, m[4], m[0]);
-        const double r = 1.5 * v.dt / (2.0 * tau + v.dt);
-        const ShkEntity e(v, m + 1, m[4], m[0], m + 5, m[4]);
-        for (int i = chunk_lo(v.nv, v.nchC, ch); i < chunk_lo(v.nv, v.nchC, ch + 1); ++i) {
-            const size_t id = at(i, v.nC, c);
-            const ShkEntity::DV d = e.at(v.xi + 3 * i);
-            v.gbp[id] = (1.0 - r) * ro(v.g + id) + r * e.g(d);
-            v.hbp[id] = (1.0 - r) * ro(v.h + id) + r * e.h(d);
-        }
-    }
-};
-
-// 2: least-squares gradients; the cell's faces in face order, as the
-// reference's face loop adds them
-struct FGrad {
-    View v;
-    ADJ_HD void operator()(int64_t idx) const {
-        const int i = static_cast<int>(idx / v.nC), c = static_cast<int>(idx % v.nC);
-        const size_t base = at(i, v.nC, 0);
-        double gg[3] = {0, 0, 0}, gh[3] = {0, 0, 0};
-        for (int e = v.cf_off[c]; e < v.cf_off[c + 1]; ++e) {
-            const int f = v.cf_ent[e] >> 1;
-            if (f >= v.nIF) break;
-            const int ow = v.own[f], ne = v.nei[f];
-            const double dg = v.gbp[base + ne] - v.gbp[base + ow], dh = v.hbp[base + ne] - v.hbp[base + ow];
-            if (v.cf_ent[e] & 1) {
-                for (int k = 0; k < 3; ++k) {
-                    gg[k] -= v.lsN[3 * f + k] * dg;
-                    gh[k] -= v.lsN[3 * f + k] * dh;
-                }
-            } else {
-                for (int k = 0; k < 3; ++k) {
-                    gg[k] += v.lsP[3 * f + k] * dg;
-                    gh[k] += v.lsP[3 * f + k] * dh;
-                }
-            }
-        }
-        const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        for (int k = 0; k < 3; ++k) {
-            v.Gg[k * n + idx] = gg[k];
-            v.Gh[k * n + idx] = gh[k];
-        }
-    }
-};
-
-// 3: face values at the half step (wall incoming DVs come in stage 5)
+// 1-3: the face values at the half step (wall incoming DVs come in stage 5)
+// from the tiled pass A of the step (gbar+, the least-squares gradients and
+// the upwind reconstruction, fvDVM.C:648-683, discreteVelocity.C:366-369,
+// fvDVM.C:755-1029), gathered from item to face order.  A tile-boundary face
+// has an item in each tile: the upwind tile writes the value into both, and
+// on an exactly tangential face each holds its own side's half.  Far-field
+// incoming DVs are not stored by pass A: rho_b M(U_owner, T_b) here.
 struct FFace {
     View v;
     static constexpr int kMinCtas = 4;  // 32 warps per SM: at most 64 registers
@@ -475,30 +430,22 @@ struct FFace {
         const int i = static_cast<int>(idx / v.nF), f = static_cast<int>(idx % v.nF);
         const double* xi = v.xi + 3 * i;
         const double xs = xs_of(xi, v.S + 3 * f);
-        const size_t n = static_cast<size_t>(v.nv) * v.nC;
-        const size_t cb = at(i, v.nC, 0);
+        const size_t r = static_cast<size_t>(i) * static_cast<size_t>(v.nI);
+        const int it0 = v.fitems[2 * f], it1 = v.fitems[2 * f + 1];
         if (f < v.nIF) {
-            const int ow = v.own[f], ne = v.nei[f];
-            if (xs >= kVSmall) {
-                v.fg[idx] = recon(v, v.gbp[cb + ow], v.Gg, n, cb + ow, f, ow, xi);
-                v.fh[idx] = recon(v, v.hbp[cb + ow], v.Gh, n, cb + ow, f, ow, xi);
-            } else if (xs < -kVSmall) {
-                v.fg[idx] = recon(v, v.gbp[cb + ne], v.Gg, n, cb + ne, f, ne, xi);
-                v.fh[idx] = recon(v, v.hbp[cb + ne], v.Gh, n, cb + ne, f, ne, xi);
-            } else {
-                double dn = recon(v, 0.0, v.Gg, n, cb + ne, f, ne, xi);
-                double d_o = recon(v, 0.0, v.Gg, n, cb + ow, f, ow, xi);
-                v.fg[idx] = 0.5 * (((v.gbp[cb + ne] + dn) + v.gbp[cb + ow]) + d_o);
-                dn = recon(v, 0.0, v.Gh, n, cb + ne, f, ne, xi);
-                d_o = recon(v, 0.0, v.Gh, n, cb + ow, f, ow, xi);
-                v.fh[idx] = 0.5 * (((v.hbp[cb + ne] + dn) + v.hbp[cb + ow]) + d_o);
+            double g = v.fvg[r + it0], h = v.fvh[r + it0];
+            if (it1 >= 0 && !(xs >= kVSmall) && !(xs < -kVSmall)) {
+                g += v.fvg[r + it1];
+                h += v.fvh[r + it1];
             }
+            v.fg[idx] = g;
+            v.fh[idx] = h;
             return;
         }
         const int b = f - v.nIF, ow = v.own[f];
         if (xs > 0) {
-            v.fg[idx] = recon(v, v.gbp[cb + ow], v.Gg, n, cb + ow, f, ow, xi);
-            v.fh[idx] = recon(v, v.hbp[cb + ow], v.Gh, n, cb + ow, f, ow, xi);
+            v.fg[idx] = v.fvg[r + it0];
+            v.fh[idx] = v.fvh[r + it0];
         } else if (v.btype[b] == 2) {
             const double Tb = v.bT[b];
             const double gi = v.brho[b] * eq_by_rho(v, xi, v.cm + 9 * static_cast<size_t>(ow) + 1, Tb);
@@ -1038,8 +985,7 @@ struct RInBy {
 template <class Ex>
 int record_step(Ex& ex, const View& v) {
     int st;
-    if ((st = ex.run(static_cast<int64_t>(v.nchC) * v.nC, FHalf{v}))) return st;
-    if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nC, FGrad{v}))) return st;
+    if ((st = ex.pass_a(v))) return st;
     if ((st = ex.run(static_cast<int64_t>(v.nv) * v.nF, FFace{v}))) return st;
     if (v.nBF > 0) {
         if ((st = ex.run(static_cast<int64_t>(v.nchF) * v.nBF, FWallOut{v}))) return st;

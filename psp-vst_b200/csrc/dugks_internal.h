@@ -239,4 +239,7 @@ void build_tiling(dugks_handle* h, int tile_cells);
 int set_error(dugks_handle* h, int code, const std::string& msg);
 // ABI helper (dugks_abi.cpp): cell records and tables from ds.cm
 int rebuild_cell_records(dugks_handle* h);
+// pass A of a step of size dt from the current state: the face-value buffer
+// then holds the step's upwind face values at the half step
+int record_face_values(dugks_handle* h, double dt);
 }  // namespace dugks
