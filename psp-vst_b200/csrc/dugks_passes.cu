@@ -1356,6 +1356,23 @@ int row_waste(int n1d, int nb) { return (n1d + nb - 1) / nb * nb - n1d; }
 
 }  // namespace
 
+// every launched layout fits the 227 KB of shared memory a B200 CTA may
+// opt into (cudaFuncAttributeMaxDynamicSharedMemorySize)
+constexpr size_t kSmemMax = 232448;
+template <int D, typename Real>
+constexpr bool fits_d() {
+    return SmemA<D, Real, 8>::bytes() <= kSmemMax && SmemA<D, Real, 8, true>::bytes() <= kSmemMax &&
+           SmemB<Real, 8>::bytes() <= kSmemMax && SmemB<Real, 8, true>::bytes() <= kSmemMax &&
+           SmemA<3, Real, 16, true>::bytes() <= kSmemMax && SmemA<3, Real, 10, true>::bytes() <= kSmemMax &&
+           SmemB<Real, 10, true>::bytes() <= kSmemMax && SmemAG<D, Real, kNbGen>::bytes() <= kSmemMax &&
+           SmemBG<Real, kNbGen>::bytes() <= kSmemMax;
+}
+static_assert(fits_d<2, double>() && fits_d<3, double>() && fits_d<2, float>() && fits_d<3, float>(),
+              "a pass layout exceeds the shared memory of a CTA");
+static_assert(SmemB<float, 16, true>::bytes() <= kSmemMax && SmemA<3, float, 20, true>::bytes() <= kSmemMax &&
+                  SmemB<float, 20, true>::bytes() <= kSmemMax,
+              "a wide FP32 pass layout exceeds the shared memory of a CTA");
+
 cudaError_t launch_pass(const StepArgs& a, int precision, bool pass_b, cudaStream_t s) {
     if (a.dm.general_dv) {
         if (precision == DUGKS_FP64)
