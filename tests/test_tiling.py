@@ -45,3 +45,12 @@ def test_greedy_tiles_fit_and_are_fewer(which):
     tu, nu = _layout(c, 128)
     assert 0 < tg <= 128 and 0 < tu <= 128
     assert ng * 128 >= c.n_cells and ng <= nu
+
+
+@pytest.mark.parametrize("tile_cells", [0, 16])
+def test_octagon_cells_tile(tile_cells):
+    # cells with ten faces (a 2:1 refined cavity): the stencil and flux lists
+    # outgrow the passes' register copies; the tiles still fit their limits
+    c = cs.refined_cavity_case(10, 6)
+    t, n = _layout(c, tile_cells)
+    assert 0 < t <= (tile_cells or 128) and n * t >= c.n_cells
