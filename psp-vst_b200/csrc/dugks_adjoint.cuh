@@ -867,17 +867,17 @@ struct RHalf {
         int nf = 0;
         while (e0 + nf < e1 && (ro(v.cf_ent + e0 + nf) >> 1) < v.nIF) ++nf;
         const bool reg = nf <= kRegF;
-        int rf[kRegF], ro_[kRegF];
+        int rf[kRegF], oc[kRegF];
         unsigned rn = 0;
 #pragma unroll
         for (int q = 0; q < kRegF; ++q) {
             rf[q] = 0;
-            ro_[q] = 0;
+            oc[q] = 0;
             if (reg && q < nf) {
                 const int ent = ro(v.cf_ent + e0 + q);
                 rf[q] = ent >> 1;
                 if (ent & 1) rn |= 1u << q;
-                ro_[q] = (ent & 1) ? ro(v.own + rf[q]) : ro(v.nei + rf[q]);  // the other cell of the face
+                oc[q] = (ent & 1) ? ro(v.own + rf[q]) : ro(v.nei + rf[q]);  // the other cell of the face
             }
         }
         double s[9] = {0};
@@ -889,7 +889,7 @@ struct RHalf {
             if (reg) {
 #pragma unroll
                 for (int q = 0; q < kRegF; ++q)
-                    if (q < nf) face_add(cb, n, rf[q], ro_[q], (rn >> q) & 1u, gc, hc, abg, abh);
+                    if (q < nf) face_add(cb, n, rf[q], oc[q], (rn >> q) & 1u, gc, hc, abg, abh);
             } else {
                 for (int en = e0; en < e0 + nf; ++en) {
                     const int ent = ro(v.cf_ent + en);
